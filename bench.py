@@ -1,0 +1,308 @@
+"""Benchmark of the CellSim3D timestep on B200 (node-steps/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cs3d|reference]
+                    [--workload packed100k|colony|ensemble256] [--cells C]
+
+Default workload: the packed large system (100,000 non-dividing cells, FCC
+packing at volume fraction 0.5, pressure 200, Gaussian node velocities
+sigma 0.01, seed 123), the configuration the headline target is quoted on.
+One "step" is one full timestep of the reference's loop
+(src/GPUbounce.cu:1055-1338) over every cell.  Inputs are larger than L2
+(positions + velocities of 18M nodes = 576 MB), so no L2 flush is needed.
+
+--impl cs3d (default): the CUDA path through libcs3d.so.  Under torchrun
+each rank steps its own replica (the single-system path does not shard;
+ensembles shard by instance), timed with CUDA events, max over ranks.
+--impl reference: the reference has no CPU implementation; its FP64 CPU
+restatement (the oracle, OpenMP over cells, all host threads) steps a bounded
+sample of the same workload on rank 0.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NODE_BYTES = 48  # algorithmic bytes per node-step: float32 x and v, read and written once
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index=0):
+        self.idx = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if parts[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def build_workload(name, cells, seed=123):
+    from cellsim3d_b200 import workloads as W
+    if name == "packed100k":
+        c, vel, L = W.packed_fcc(cells, phi=0.5, seed=seed)
+        p = W.base_params(box_len=(L, L, L), growth_rate=0.0, min_pressure=200.0, max_pressure=200.0,
+                          div_time_steps=5000, rng_ij=seed, rng_kl=100 * seed)
+        return [(p, W.state(c, velocities=vel), cells)]
+    if name == "colony":
+        p, st, cap = W.config2()
+        return [(p, st, cap)]
+    if name == "ensemble256":
+        return [(p, st, 1024) for p, st in W.config4()]
+    raise ValueError(name)
+
+
+def make_topology(insts):
+    import cellsim3d_b200 as cs
+    from cellsim3d_b200 import workloads as W
+    st = insts[0][1]
+    return cs.build_topology(cs.mesh_from_arrays(W.load_mesh()), st["X"][:192], st["Y"][:192], st["Z"][:192])
+
+
+def run_cs3d(args, world, rank, local):
+    import torch
+    import cellsim3d_b200 as cs
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    insts = build_workload(args.workload, args.cells)
+    if args.workload == "ensemble256" and world > 1:
+        # shard instances across ranks by predicted cost (cells), greedy
+        order = sorted(range(len(insts)), key=lambda k: -insts[k][1]["n"])
+        load = [0] * world
+        mine = []
+        for k in order:
+            r = min(range(world), key=lambda q: load[q])
+            load[r] += insts[k][1]["n"]
+            if r == rank:
+                mine.append(k)
+        insts = [insts[k] for k in sorted(mine)]
+    topo = make_topology(insts)
+    ens = cs.Ensemble([p for p, _, _ in insts], topo, [cap for _, _, cap in insts], device=local)
+    for k, (p, st, cap) in enumerate(insts):
+        ens.load_state(k, st["X"], st["Y"], st["Z"], st.get("VX"), st.get("VY"), st.get("VZ"), n_cells=st["n"])
+    n_nodes0 = sum(st["n"] for _, st, _ in insts) * 180
+    ens.step(args.warmup)
+    cells_before = sum(ens.n_cells(k) for k in range(len(insts)))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ens.step(args.steps)
+    torch.cuda.synchronize()
+    ms = ens.last_step_ms()
+    cells_after = sum(ens.n_cells(k) for k in range(len(insts)))
+    node_steps = 0.5 * (cells_before + cells_after) * 180 * args.steps
+    stats = ens.stats()
+    # per-kernel device times (profiling pass after the timed region)
+    prof = ens.profile_step(3)
+    # end to end through the C ABI with host buffers: upload the state, K
+    # synchronous cs3d_step(1) calls (each returns the status word), read the
+    # final state back
+    e2e = None
+    if not args.no_e2e:
+        st0 = ens.state(0)
+        host = {k: torch.from_numpy(st0[k]).pin_memory().numpy() for k in ("X", "Y", "Z", "VX", "VY", "VZ")}
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ens.load_state(0, host["X"], host["Y"], host["Z"], host["VX"], host["VY"], host["VZ"], n_cells=st0["n"])
+        for _ in range(args.steps):
+            ens.step(1)
+        out = ens.state(0)
+        t1 = time.perf_counter()
+        state_bytes = 6 * out["X"].nbytes
+        e2e = {"seconds": t1 - t0, "node_steps": st0["n"] * 180 * args.steps,
+               "h2d": state_bytes / args.steps, "d2h": state_bytes / args.steps + 4 * len(insts)}
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    ns = torch.tensor([node_steps], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(ns, op=dist.ReduceOp.SUM)
+    ms_max = float(t.item())
+    total_node_steps = float(ns.item())
+    result = None
+    if rank == 0:
+        peak, peak_kind = _peaks()
+        value = total_node_steps / (ms_max * 1e-3)
+        top = max(prof, key=lambda kv: kv[1])
+        n_nodes = 0.5 * (cells_before + cells_after) * 180
+        s1 = dict(prof).get("s1_con_dis", top[1])
+        achieved = NODE_BYTES * n_nodes / (s1 * 1e-3) / 1e9
+        step_ms = sum(v for _, v in prof)
+        result = {
+            "metric": "node-steps/s (cells x 180 x steps / s)",
+            "value": value,
+            "unit": "node-steps/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded generator, cellsim3d_b200/workloads.py)",
+            "config": {"workload": args.workload, "cells": cells_before, "nodes": int(n_nodes),
+                       "parallelism": "replicas" if args.workload != "ensemble256" else "instances sharded",
+                       "l2": "inputs larger than L2 (no flush)" if n_nodes * 32 > 126e6 else "L2 resident",
+                       "precision": "FP32 forces/integration, FP64 CoM/volume/division"},
+            "roofline": {"bound": "hbm", "kernel": "s1_con_dis", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "peak_source": peak_kind,
+                         "algorithmic_bytes_per_node": NODE_BYTES},
+            "step_roofline": {"achieved": NODE_BYTES * value / 1e9 / world, "frac": NODE_BYTES * value / 1e9 / world / peak},
+            "kernels_ms": {k: round(v, 4) for k, v in prof},
+            "profiled_step_ms": step_ms,
+            "gpu_launches": int(stats["launches_per_step"]) * args.steps,
+            "nl_rebuilds": stats["rebuilds"],
+            "max_entries": stats["max_entries"],
+            "clocks": clk.summary(),
+        }
+        if e2e:
+            result["e2e"] = {"value": e2e["node_steps"] * world / e2e["seconds"] if world == 1 else
+                             e2e["node_steps"] / e2e["seconds"] * world,
+                             "unit": "node-steps/s", "h2d_bytes_per_step": int(e2e["h2d"]),
+                             "d2h_bytes_per_step": int(e2e["d2h"]),
+                             "how": "cs3d_load_state from pinned host, K x cs3d_step(1) with status read-back, "
+                                    "cs3d_get_state to host"}
+    ens.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
+def cpu_baseline(args, steps=None, cells=None):
+    """The FP64 oracle stepping a bounded sample of the workload on the host."""
+    import oracle
+    from cellsim3d_b200 import workloads as W
+    cells = cells or args.cpu_cells
+    insts = build_workload(args.workload, cells) if args.workload == "packed100k" else \
+        build_workload(args.workload, cells)
+    p, st, cap = insts[0]
+    mesh = W.load_mesh()
+    r0, th = oracle.r0_theta0(st["X"][:192], st["Y"][:192], st["Z"][:192], mesh["nn"])
+    topo = oracle.make_topo(mesh["nn"], mesh["sign"], r0, th, mesh["faces"])
+    S = oracle.System(max(cap, st["n"]), p, topo)
+    S.load(st["X"], st["Y"], st["Z"], st.get("VX"), st.get("VY"), st.get("VZ"), n=st["n"])
+    S.seed(p["rng_ij"], p["rng_kl"])
+    S.init()
+    steps = steps or args.cpu_steps
+    t0 = time.perf_counter()
+    S.step(steps)
+    dt = time.perf_counter() - t0
+    ns = S.n * 180 * steps
+    S.close()
+    return {"value": ns / dt, "unit": "node-steps/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": "%d full timesteps of a %d-cell system of the same generator (FP64 oracle, OpenMP %d threads)"
+                      % (steps, st["n"], os.cpu_count())}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="cs3d", choices=["cs3d", "reference"])
+    ap.add_argument("--workload", default="packed100k", choices=["packed100k", "colony", "ensemble256"])
+    ap.add_argument("--cells", type=int, default=100_000)
+    ap.add_argument("--cpu-cells", type=int, default=10_000)
+    ap.add_argument("--cpu-steps", type=int, default=10)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_env()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        base = cpu_baseline(args, steps=max(1, min(args.steps, args.cpu_steps)))
+        line = {"impl": "reference", "metric": "node-steps/s (cells x 180 x steps / s)", "value": base["value"],
+                "unit": "node-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": {"workload": args.workload, "cells": args.cpu_cells},
+                "cpu_baseline": base,
+                "e2e": {"value": base["value"], "unit": "node-steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+    res = run_cs3d(args, world, rank, local)
+    if rank == 0:
+        if not args.no_cpu and world == 1:
+            res["cpu_baseline"] = cpu_baseline(args)
+        print(json.dumps(res))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,799 @@
+// cs3d_api.cu -- device context of libcs3d.so: allocation, state upload,
+// the initial force evaluation, the per-step launch sequence (captured once
+// per step variant into a CUDA graph) and read-back.  All entry points are
+// extern "C" and return CS3D_* status codes.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "cs3d_kernels.cuh"
+
+using namespace cs3d;
+
+struct cs3d_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int n_inst = 0;
+    int cap_total = 0;
+    int nsm = 148;
+    std::vector<InstParams> hprm;
+    std::vector<int> hn;           // host copy of the loaded cell counts
+    Dev d{};
+    // device allocations to free
+    std::vector<void *> allocs;
+    bool need_init = true;
+    long long host_step = 0;
+    int max_div_steps = 0;
+    bool any_growth = false;
+    float skin = 0.1f;
+    int grid_cells = 0;            // blocks of the per-cell kernels
+    int grid_flat = 0;             // blocks of the per-thread kernels
+    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float last_ms = 0.f;
+    long long launches_per_step = 0;
+    unsigned last_err_bits = 0;
+};
+
+namespace {
+
+#define CK(call)                                         \
+    do {                                                 \
+        cudaError_t e_ = (call);                         \
+        if (e_ != cudaSuccess) {                         \
+            fprintf(stderr, "cs3d: %s failed: %s (%s:%d)\n", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+            return CS3D_E_CUDA;                          \
+        }                                                \
+    } while (0)
+
+template <typename T>
+int dalloc(cs3d_ctx *c, T **p, size_t count)
+{
+    void *q = nullptr;
+    size_t bytes = count * sizeof(T);
+    if (bytes == 0) bytes = 16;
+    if (cudaMalloc(&q, bytes) != cudaSuccess) return CS3D_E_NOMEM;
+    if (cudaMemsetAsync(q, 0, bytes, c->stream) != cudaSuccess) { cudaFree(q); return CS3D_E_CUDA; }
+    c->allocs.push_back(q);
+    *p = (T *)q;
+    return CS3D_OK;
+}
+
+void free_all(cs3d_ctx *c)
+{
+    for (int p = 0; p < 2; ++p)
+        for (int q = 0; q < 2; ++q)
+            if (c->graph[p][q]) cudaGraphExecDestroy(c->graph[p][q]);
+    for (void *q : c->allocs) cudaFree(q);
+    c->allocs.clear();
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+}
+
+// Host-side mesh tables: packed neighbours, R0, theta0 and the arm-end
+// index table that maps node i's six second-neighbour angle terms (the
+// NeighNeighs cases of src/propagate.cu:63-78, theta1 then theta2 per
+// neighbour) onto the arm-force array [(vertex*3 + pair)*2 + end].
+int upload_topology(cs3d_ctx *c, const cs3d_topology *t)
+{
+    std::vector<uint32_t> nnp(SLOTS, 0);
+    std::vector<float4> r0(SLOTS), th(SLOTS);
+    std::vector<uint4> arm(SLOTS);
+    std::vector<uint8_t> faces(CS3D_FACES * 7);
+    for (int i = 0; i < SLOTS; ++i) {
+        r0[i] = make_float4(0, 0, 0, 0);
+        th[i] = make_float4(0, 0, 0, 0);
+        arm[i] = make_uint4(0, 0, 0, 0);
+    }
+    for (int i = 0; i < NODES; ++i) {
+        int a = t->nn[i], b = t->nn[192 + i], cc = t->nn[384 + i];
+        if (a < 0 || a >= NODES || b < 0 || b >= NODES || cc < 0 || cc >= NODES) return CS3D_E_ARG;
+        nnp[i] = (uint32_t)a | ((uint32_t)b << 8) | ((uint32_t)cc << 16) | ((uint32_t)(uint8_t)(int8_t)t->sign[i] << 24);
+        r0[i] = make_float4(t->r0[i], t->r0[192 + i], t->r0[384 + i], 0.f);
+        th[i] = make_float4(t->theta0[3 * i], t->theta0[3 * i + 1], t->theta0[3 * i + 2], 0.f);
+    }
+    for (int i = 0; i < NODES; ++i) {
+        unsigned idx[6];
+        for (int q = 0; q < 3; ++q) {
+            int n = t->nn[q * 192 + i];
+            int na = t->nn[n], nb = t->nn[192 + n], nc = t->nn[384 + n];
+            unsigned base = (unsigned)n * 6;
+            if (na == i) { idx[2 * q] = base + 0 * 2 + 0; idx[2 * q + 1] = base + 2 * 2 + 0; }
+            else if (nb == i) { idx[2 * q] = base + 0 * 2 + 1; idx[2 * q + 1] = base + 1 * 2 + 0; }
+            else if (nc == i) { idx[2 * q] = base + 2 * 2 + 1; idx[2 * q + 1] = base + 1 * 2 + 1; }
+            else return CS3D_E_ARG;  // neighbour table not symmetric
+        }
+        arm[i] = make_uint4(idx[0] | (idx[1] << 16), idx[2] | (idx[3] << 16), idx[4] | (idx[5] << 16), 0u);
+    }
+    for (int f = 0; f < CS3D_FACES * 7; ++f) {
+        if (t->faces[f] < 0 || t->faces[f] >= NODES) return CS3D_E_ARG;
+        faces[f] = (uint8_t)t->faces[f];
+    }
+    int rc;
+    if ((rc = dalloc(c, &c->d.topo.nnpack, SLOTS))) return rc;
+    if ((rc = dalloc(c, &c->d.topo.r0, SLOTS))) return rc;
+    if ((rc = dalloc(c, &c->d.topo.th0, SLOTS))) return rc;
+    if ((rc = dalloc(c, &c->d.topo.arm, SLOTS))) return rc;
+    if ((rc = dalloc(c, &c->d.topo.faces, CS3D_FACES * 7))) return rc;
+    CK(cudaMemcpyAsync(c->d.topo.nnpack, nnp.data(), SLOTS * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d.topo.r0, r0.data(), SLOTS * 16, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d.topo.th0, th.data(), SLOTS * 16, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d.topo.arm, arm.data(), SLOTS * 16, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d.topo.faces, faces.data(), CS3D_FACES * 7, cudaMemcpyHostToDevice, c->stream));
+    return CS3D_OK;
+}
+
+InstParams make_inst(const cs3d_params &p, int base, int cap, float skin)
+{
+    InstParams q{};
+    q.mass = p.particle_mass;
+    q.rr = p.repulsion_range;
+    q.ra = p.attraction_range;
+    q.rs = p.repulsion_strength;
+    q.as = p.attraction_strength;
+    q.E = p.youngs_mod;
+    q.stiff1 = p.stiffness1;
+    q.gint = p.internal_damping;
+    q.gext = p.viscotic_damping;
+    q.go = p.gamma_visc;
+    q.divvol = p.division_vol;
+    q.dt = p.time_interval;
+    q.maxp = p.max_pressure;
+    q.minp = p.min_pressure;
+    q.growth = p.growth_rate;
+    q.thresh = p.thresh_dist;
+    for (int k = 0; k < 3; ++k) q.box[k] = p.box_len[k];
+    volatile float ra = p.attraction_range;  // float products, no contraction
+    q.ra2 = ra * ra;
+    volatile float as = p.attraction_strength, E = p.youngs_mod, rs = p.repulsion_strength;
+    q.asE = as * E;
+    q.rsE = rs * E;
+    q.wallk = 100.0f * E;
+    q.skin = skin;
+    q.rlist = p.attraction_range + skin;
+    q.check_sph = p.check_sphericity;
+    q.angles = p.constrain_angles;
+    q.rigid = p.use_rigid_box;
+    q.daught_same = p.daught_same_stiffness;
+    q.div_steps = p.div_time_steps;
+    q.base = base;
+    q.cap = cap;
+    return q;
+}
+
+int check_params(const cs3d_params &p)
+{
+    if (!(p.particle_mass > 0) || !(p.time_interval > 0) || !(p.attraction_range > 0) ||
+        !(p.repulsion_range >= 0))
+        return CS3D_E_CONFIG;
+    return CS3D_OK;
+}
+
+// Rebuild the active-cell work table from the device cell counts.
+__global__ void k_build_work(Dev d)
+{
+    __shared__ int off;
+    if (threadIdx.x == 0) off = 0;
+    __syncthreads();
+    for (int k = 0; k < d.n_inst; ++k) {
+        int n = d.st[k].n, base = d.prm[k].base;
+        for (int c = threadIdx.x; c < n; c += blockDim.x) d.work[off + c] = base + c;
+        __syncthreads();
+        if (threadIdx.x == 0) off += n;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *d.work_n = off;
+}
+
+// Optional per-launch event recording (profiling pass of cs3d_profile_step).
+struct Prof {
+    std::vector<cudaEvent_t> *ev = nullptr;
+    std::vector<const char *> *names = nullptr;
+    void mark(cudaStream_t s, const char *name) const {
+        if (!ev) return;
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, s);
+        ev->push_back(e);
+        names->push_back(name);
+    }
+};
+
+int launch_nl_build(cs3d_ctx *c, const Prof &pf = Prof())
+{
+    const Dev &d = c->d;
+    cudaStream_t s = c->stream;
+    k_nl_boxes<<<c->grid_cells, SLOTS, 0, s>>>(d); pf.mark(s, "nl_boxes");
+    k_nl_grid<<<1, 32, 0, s>>>(d); pf.mark(s, "nl_grid");
+    k_nl_zero<<<c->grid_flat, 256, 0, s>>>(d); pf.mark(s, "nl_zero");
+    k_nl_count<<<c->grid_flat, 256, 0, s>>>(d); pf.mark(s, "nl_count");
+    k_nl_scan<<<1, 1024, 0, s>>>(d); pf.mark(s, "nl_scan");
+    k_nl_fill<<<c->grid_flat, 256, 0, s>>>(d); pf.mark(s, "nl_fill");
+    k_nl_build<<<c->grid_cells, SLOTS, 0, s>>>(d); pf.mark(s, "nl_build");
+    CK(cudaGetLastError());
+    return CS3D_OK;
+}
+
+int run_init(cs3d_ctx *c)
+{
+    const Dev &d = c->d;
+    cudaStream_t s = c->stream;
+    k_build_work<<<1, 256, 0, s>>>(d);
+    k_init_begin<<<1, 256, 0, s>>>(d);
+    k_geom<<<c->grid_cells, SLOTS, 0, s>>>(d, 0);
+    CK(cudaGetLastError());
+    int rc = launch_nl_build(c);
+    if (rc) return rc;
+    k_s1<true><<<c->grid_cells, SLOTS, 0, s>>>(d, 0);
+    CK(cudaGetLastError());
+    c->host_step = 0;
+    c->need_init = false;
+    return CS3D_OK;
+}
+
+// One timestep, src/GPUbounce.cu:1055-1338, as a fixed launch sequence.
+int launch_step(cs3d_ctx *c, int par, bool div, const Prof &pf = Prof())
+{
+    const Dev &d = c->d;
+    cudaStream_t s = c->stream;
+    int n = 0;
+    k_integrate<<<c->grid_cells, SLOTS, 0, s>>>(d); ++n; pf.mark(s, "integrate");
+    k_step_begin<<<1, 256, 0, s>>>(d, par ^ 1); ++n; pf.mark(s, "step_begin");
+    int rc = launch_nl_build(c, pf);
+    if (rc) return rc;
+    n += 7;
+    k_s1<false><<<c->grid_cells, SLOTS, 0, s>>>(d, par); ++n; pf.mark(s, "s1_con_dis");
+    k_s2<<<c->grid_cells, SLOTS, 0, s>>>(d, par); ++n; pf.mark(s, "s2_dis_geom");
+    if (div) {
+        k_div_select<<<c->n_inst, 256, 0, s>>>(d, par); ++n; pf.mark(s, "div_select");
+        k_div_apply<<<c->grid_cells, SLOTS, 0, s>>>(d, par); ++n; pf.mark(s, "div_apply");
+        k_grid_fix<<<c->grid_flat, 256, 0, s>>>(d, par); ++n; pf.mark(s, "grid_fix");
+    }
+    CK(cudaGetLastError());
+    c->launches_per_step = n;
+    return CS3D_OK;
+}
+
+int get_graph(cs3d_ctx *c, int par, bool div, cudaGraphExec_t *out)
+{
+    cudaGraphExec_t &g = c->graph[par][div ? 1 : 0];
+    if (!g) {
+        cudaGraph_t graph;
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = launch_step(c, par, div);
+        cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+        if (rc) { if (e == cudaSuccess) cudaGraphDestroy(graph); return rc; }
+        CK(e);
+        e = cudaGraphInstantiate(&g, graph, 0);
+        cudaGraphDestroy(graph);
+        CK(e);
+    }
+    *out = g;
+    return CS3D_OK;
+}
+
+int ensure_init(cs3d_ctx *c)
+{
+    if (!c->need_init) return CS3D_OK;
+    return run_init(c);
+}
+
+int read_errors(cs3d_ctx *c, unsigned *any)
+{
+    std::vector<InstState> st(c->n_inst);
+    CK(cudaMemcpyAsync(st.data(), c->d.st, sizeof(InstState) * c->n_inst, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    unsigned bits = 0;
+    for (auto &q : st) bits |= q.err;
+    *any = bits;
+    c->last_err_bits = bits;
+    return CS3D_OK;
+}
+
+void to_soa(const std::vector<float4> &src, int n, float *X, float *Y, float *Z)
+{
+    for (int c = 0; c < n; ++c)
+        for (int i = 0; i < SLOTS; ++i) {
+            const float4 &v = src[(size_t)c * SLOTS + i];
+            if (X) X[(size_t)c * SLOTS + i] = v.x;
+            if (Y) Y[(size_t)c * SLOTS + i] = v.y;
+            if (Z) Z[(size_t)c * SLOTS + i] = v.z;
+        }
+}
+
+int inst_count(cs3d_ctx *c, int inst, int *n)
+{
+    int v = 0;
+    CK(cudaMemcpyAsync(&v, &c->d.st[inst].n, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    *n = v;
+    return CS3D_OK;
+}
+
+int fetch4(cs3d_ctx *c, const float4 *src, int inst, int n, std::vector<float4> &out)
+{
+    out.resize((size_t)n * SLOTS);
+    if (n == 0) return CS3D_OK;
+    CK(cudaMemcpyAsync(out.data(), src + (size_t)c->hprm[inst].base * SLOTS, sizeof(float4) * out.size(),
+                       cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return CS3D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topology *topo,
+                         const int *capacity, int device, void *stream, cs3d_ctx **out)
+{
+    if (!out || !params || !topo || !capacity || n_inst <= 0) return CS3D_E_ARG;
+    *out = nullptr;
+    long long total = 0;
+    for (int k = 0; k < n_inst; ++k) {
+        if (capacity[k] <= 0) return CS3D_E_ARG;
+        if (check_params(params[k])) return CS3D_E_CONFIG;
+        total += capacity[k];
+    }
+    if (total > (1 << 23)) return CS3D_E_ARG;  // cell ids are packed in 24 bits for pair records
+    cs3d_ctx *c = new (std::nothrow) cs3d_ctx();
+    if (!c) return CS3D_E_NOMEM;
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) { delete c; return CS3D_E_CUDA; }
+    if (stream) c->stream = (cudaStream_t)stream;
+    else {
+        if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return CS3D_E_CUDA; }
+        c->own_stream = true;
+    }
+    cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device);
+    c->n_inst = n_inst;
+    c->cap_total = (int)total;
+    c->hn.assign(n_inst, 0);
+    int base = 0;
+    for (int k = 0; k < n_inst; ++k) {
+        c->hprm.push_back(make_inst(params[k], base, capacity[k], c->skin));
+        base += capacity[k];
+        if (params[k].growth_rate > 0) c->any_growth = true;
+        c->max_div_steps = std::max(c->max_div_steps, params[k].div_time_steps);
+    }
+    Dev &d = c->d;
+    d.n_inst = n_inst;
+    d.cap_total = c->cap_total;
+    const size_t nodes = (size_t)c->cap_total * SLOTS;
+    int rc = CS3D_OK;
+#define AL(ptr, cnt) if (!rc) rc = dalloc(c, &(ptr), (cnt))
+    AL(d.prm, n_inst);
+    AL(d.st, n_inst);
+    AL(d.X, nodes); AL(d.V, nodes); AL(d.Vb, nodes); AL(d.FC, nodes); AL(d.FD, nodes);
+    AL(d.CM, c->cap_total);
+    AL(d.press, c->cap_total); AL(d.E, c->cap_total); AL(d.vol, c->cap_total); AL(d.area, c->cap_total);
+    AL(d.divflag, c->cap_total);
+    AL(d.aabb[0], 2 * (size_t)c->cap_total); AL(d.aabb[1], 2 * (size_t)c->cap_total);
+    AL(d.aabb_cur, 2 * (size_t)c->cap_total);
+    AL(d.cell_inst, c->cap_total);
+    AL(d.work, c->cap_total); AL(d.work_n, 1);
+    AL(d.cand, (size_t)c->cap_total * MAXC); AL(d.ncand, c->cap_total);
+    AL(d.ent, (size_t)c->cap_total * MAXE * SLOTS); AL(d.nent, nodes);
+    d.bin_cap = 8 * c->cap_total + 65536;
+    AL(d.bin_count, (size_t)d.bin_cap + 1); AL(d.bin_start, (size_t)d.bin_cap + 1);
+    AL(d.bin_cells, c->cap_total); AL(d.cell_bin, c->cap_total); AL(d.cell_rank, c->cap_total);
+    AL(d.total_bins, 1);
+    AL(d.divtab, c->cap_total); AL(d.div_total, 1);
+    d.ev_cap = std::max(1 << 16, 2 * c->cap_total);
+    AL(d.events, d.ev_cap); AL(d.n_events, 1);
+    AL(d.flags, 4);
+    d.pair_cap = 1;
+    AL(d.pairs, 1); AL(d.n_pairs, 1);
+#undef AL
+    if (!rc) rc = upload_topology(c, topo);
+    if (rc) { free_all(c); delete c; return rc; }
+    // instance parameters, RANMAR streams and slot ownership
+    std::vector<InstState> st(n_inst);
+    std::vector<int> owner(c->cap_total);
+    for (int k = 0; k < n_inst; ++k) {
+        memset(&st[k], 0, sizeof(InstState));
+        cs3d_rng r;
+        if (cs3d_rng_init(&r, params[k].rng_ij, params[k].rng_kl) != CS3D_OK) {
+            free_all(c); delete c; return CS3D_E_CONFIG;
+        }
+        memcpy(st[k].u, r.u, sizeof r.u);
+        st[k].rc = r.c; st[k].rcd = r.cd; st[k].rcm = r.cm; st[k].i97 = r.i97; st[k].j97 = r.j97;
+        for (int q = 0; q < capacity[k]; ++q) owner[c->hprm[k].base + q] = k;
+    }
+    if (cudaMemcpyAsync(d.prm, c->hprm.data(), sizeof(InstParams) * n_inst, cudaMemcpyHostToDevice, c->stream) ||
+        cudaMemcpyAsync(d.st, st.data(), sizeof(InstState) * n_inst, cudaMemcpyHostToDevice, c->stream) ||
+        cudaMemcpyAsync(d.cell_inst, owner.data(), sizeof(int) * owner.size(), cudaMemcpyHostToDevice, c->stream) ||
+        cudaEventCreate(&c->ev0) || cudaEventCreate(&c->ev1) || cudaStreamSynchronize(c->stream)) {
+        free_all(c); delete c; return CS3D_E_CUDA;
+    }
+    int occ = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_s1<false>, SLOTS, 0);
+    c->grid_cells = std::max(1, std::min(c->cap_total, c->nsm * std::max(occ, 1)));
+    c->grid_flat = std::max(1, std::min((c->cap_total + 255) / 256 + 1, c->nsm * 8));
+    *out = c;
+    return CS3D_OK;
+}
+
+int cs3d_create(const cs3d_params *params, const cs3d_topology *topo, int capacity_cells, int device,
+                void *stream, cs3d_ctx **out)
+{
+    return cs3d_create_ensemble(1, params, topo, &capacity_cells, device, stream, out);
+}
+
+int cs3d_destroy(cs3d_ctx *c)
+{
+    if (!c) return CS3D_E_ARG;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    free_all(c);
+    delete c;
+    return CS3D_OK;
+}
+
+int cs3d_set_option(cs3d_ctx *c, int option, long long value)
+{
+    if (!c) return CS3D_E_ARG;
+    cudaSetDevice(c->device);
+    switch (option) {
+    case CS3D_OPT_RECORD_PAIRS:
+        c->d.record_pairs = value ? 1 : 0;
+        break;
+    case CS3D_OPT_PAIR_CAPACITY: {
+        if (value < 1) return CS3D_E_ARG;
+        int4 *p = nullptr;
+        if (cudaMalloc(&p, sizeof(int4) * (size_t)value) != cudaSuccess) return CS3D_E_NOMEM;
+        c->allocs.push_back(p);
+        c->d.pairs = p;
+        c->d.pair_cap = value;
+        break;
+    }
+    case CS3D_OPT_SKIN: {
+        float s = (float)value * 1e-6f;
+        if (!(s > 0.002f) || s > 1.0f) return CS3D_E_ARG;
+        c->skin = s;
+        for (auto &q : c->hprm) { q.skin = s; q.rlist = q.ra + s; }
+        CK(cudaMemcpyAsync(c->d.prm, c->hprm.data(), sizeof(InstParams) * c->n_inst, cudaMemcpyHostToDevice, c->stream));
+        c->need_init = true;
+        break;
+    }
+    default:
+        return CS3D_E_ARG;
+    }
+    // launch parameters are baked into captured graphs: drop them
+    for (int p = 0; p < 2; ++p)
+        for (int q = 0; q < 2; ++q)
+            if (c->graph[p][q]) { cudaGraphExecDestroy(c->graph[p][q]); c->graph[p][q] = nullptr; }
+    return CS3D_OK;
+}
+
+int cs3d_load_state(cs3d_ctx *c, int inst, int n, const float *X, const float *Y, const float *Z,
+                    const float *VX, const float *VY, const float *VZ, const float *pressure,
+                    const float *youngs)
+{
+    if (!c || inst < 0 || inst >= c->n_inst || n < 0 || (n > 0 && (!X || !Y || !Z))) return CS3D_E_ARG;
+    const InstParams &P = c->hprm[inst];
+    if (n > P.cap) return CS3D_E_CAPACITY;
+    cudaSetDevice(c->device);
+    const size_t slots = (size_t)P.cap * SLOTS;
+    std::vector<float4> x(slots, make_float4(0, 0, 0, 0)), v(slots, make_float4(0, 0, 0, 0));
+    for (size_t g = 0; g < (size_t)n * SLOTS; ++g) {
+        int node = (int)(g % SLOTS);
+        if (node >= NODES) continue;
+        x[g] = make_float4(X[g], Y[g], Z[g], 0.f);
+        if (VX && VY && VZ) v[g] = make_float4(VX[g], VY[g], VZ[g], 0.f);
+    }
+    std::vector<float> p(P.cap, 0.f), e(P.cap, 0.f);
+    for (int k = 0; k < n; ++k) {
+        p[k] = pressure ? pressure[k] : P.minp;
+        e[k] = youngs ? youngs[k] : P.stiff1;
+    }
+    const size_t off = (size_t)P.base * SLOTS;
+    const Dev &d = c->d;
+    CK(cudaMemcpyAsync(d.X + off, x.data(), sizeof(float4) * slots, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(d.V + off, v.data(), sizeof(float4) * slots, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(d.Vb + off, 0, sizeof(float4) * slots, c->stream));
+    CK(cudaMemsetAsync(d.FC + off, 0, sizeof(float4) * slots, c->stream));
+    CK(cudaMemsetAsync(d.FD + off, 0, sizeof(float4) * slots, c->stream));
+    CK(cudaMemsetAsync(d.CM + P.base, 0, sizeof(float4) * P.cap, c->stream));
+    CK(cudaMemsetAsync(d.vol + P.base, 0, sizeof(float) * P.cap, c->stream));
+    CK(cudaMemsetAsync(d.area + P.base, 0, sizeof(float) * P.cap, c->stream));
+    CK(cudaMemsetAsync(d.divflag + P.base, 0, P.cap, c->stream));
+    CK(cudaMemcpyAsync(d.press + P.base, p.data(), sizeof(float) * P.cap, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(d.E + P.base, e.data(), sizeof(float) * P.cap, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(&d.st[inst].n, &n, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    int zero = 0;
+    CK(cudaMemcpyAsync(&d.st[inst].step, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(&d.st[inst].err, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->hn[inst] = n;
+    c->need_init = true;
+    return CS3D_OK;
+}
+
+int cs3d_set_rng(cs3d_ctx *c, int inst, const cs3d_rng *r)
+{
+    if (!c || !r || inst < 0 || inst >= c->n_inst || !r->ok) return CS3D_E_ARG;
+    cudaSetDevice(c->device);
+    InstState st;
+    CK(cudaMemcpyAsync(&st, &c->d.st[inst], sizeof st, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    memcpy(st.u, r->u, sizeof st.u);
+    st.rc = r->c; st.rcd = r->cd; st.rcm = r->cm; st.i97 = r->i97; st.j97 = r->j97;
+    CK(cudaMemcpyAsync(&c->d.st[inst], &st, sizeof st, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return CS3D_OK;
+}
+
+int cs3d_step(cs3d_ctx *c, int n_steps)
+{
+    if (!c || n_steps < 0) return CS3D_E_ARG;
+    cudaSetDevice(c->device);
+    int rc = ensure_init(c);
+    if (rc) return rc;
+    CK(cudaEventRecord(c->ev0, c->stream));
+    for (int k = 0; k < n_steps; ++k) {
+        long long s = c->host_step + 1;
+        int par = (int)((s - 1) & 1);
+        bool div = c->any_growth && s <= c->max_div_steps;
+        cudaGraphExec_t g;
+        if ((rc = get_graph(c, par, div, &g))) return rc;
+        CK(cudaGraphLaunch(g, c->stream));
+        c->host_step = s;
+    }
+    CK(cudaEventRecord(c->ev1, c->stream));
+    CK(cudaEventSynchronize(c->ev1));
+    CK(cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1));
+    unsigned bits = 0;
+    if ((rc = read_errors(c, &bits))) return rc;
+    if (bits & CS3D_ERRBIT_CAPACITY) return CS3D_E_CAPACITY;
+    if (bits) return CS3D_E_DEVICE_FLAGS;
+    return CS3D_OK;
+}
+
+int cs3d_profile_step(cs3d_ctx *c, int n_steps, float *kernel_ms, char *names, int names_len,
+                      int max_kernels, int *n_kernels)
+{
+    if (!c || n_steps <= 0 || !n_kernels) return CS3D_E_ARG;
+    cudaSetDevice(c->device);
+    int rc = ensure_init(c);
+    if (rc) return rc;
+    std::vector<double> acc;
+    std::vector<const char *> first_names;
+    for (int k = 0; k < n_steps; ++k) {
+        long long st = c->host_step + 1;
+        int par = (int)((st - 1) & 1);
+        bool div = c->any_growth && st <= c->max_div_steps;
+        std::vector<cudaEvent_t> ev;
+        std::vector<const char *> nm;
+        Prof pf;
+        pf.ev = &ev;
+        pf.names = &nm;
+        cudaEvent_t e0;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventRecord(e0, c->stream));
+        if ((rc = launch_step(c, par, div, pf))) return rc;
+        c->host_step = st;
+        CK(cudaEventSynchronize(ev.empty() ? e0 : ev.back()));
+        if (acc.size() < ev.size()) { acc.resize(ev.size(), 0.0); first_names = nm; }
+        cudaEvent_t prev = e0;
+        for (size_t q = 0; q < ev.size(); ++q) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, prev, ev[q]);
+            acc[q] += ms;
+            prev = ev[q];
+        }
+        cudaEventDestroy(e0);
+        for (auto e : ev) cudaEventDestroy(e);
+    }
+    int nk = (int)acc.size();
+    *n_kernels = nk;
+    std::string all;
+    for (int q = 0; q < nk; ++q) {
+        if (kernel_ms && q < max_kernels) kernel_ms[q] = (float)(acc[q] / n_steps);
+        if (q) all += ",";
+        all += first_names[q];
+    }
+    if (names && names_len > 0) snprintf(names, (size_t)names_len, "%s", all.c_str());
+    unsigned bits = 0;
+    if ((rc = read_errors(c, &bits))) return rc;
+    return bits ? CS3D_E_DEVICE_FLAGS : CS3D_OK;
+}
+
+int cs3d_last_step_ms(cs3d_ctx *c, float *ms)
+{
+    if (!c || !ms) return CS3D_E_ARG;
+    *ms = c->last_ms;
+    return CS3D_OK;
+}
+
+int cs3d_get_state(cs3d_ctx *c, int inst, int *n_cells, float *X, float *Y, float *Z, float *VX, float *VY,
+                   float *VZ, float *pressure, float *youngs)
+{
+    if (!c || inst < 0 || inst >= c->n_inst) return CS3D_E_ARG;
+    cudaSetDevice(c->device);
+    int rc = ensure_init(c);
+    if (rc) return rc;
+    int n = 0;
+    if ((rc = inst_count(c, inst, &n))) return rc;
+    if (n_cells) *n_cells = n;
+    std::vector<float4> buf;
+    if (X || Y || Z) {
+        if ((rc = fetch4(c, c->d.X, inst, n, buf))) return rc;
+        to_soa(buf, n, X, Y, Z);
+    }
+    if (VX || VY || VZ) {
+        if ((rc = fetch4(c, c->d.V, inst, n, buf))) return rc;
+        to_soa(buf, n, VX, VY, VZ);
+    }
+    const int base = c->hprm[inst].base;
+    if (pressure && n) CK(cudaMemcpyAsync(pressure, c->d.press + base, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
+    if (youngs && n) CK(cudaMemcpyAsync(youngs, c->d.E + base, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return CS3D_OK;
+}
+
+int cs3d_get_forces(cs3d_ctx *c, int inst, float *FCX, float *FCY, float *FCZ, float *FDX, float *FDY, float *FDZ)
+{
+    if (!c || inst < 0 || inst >= c->n_inst) return CS3D_E_ARG;
+    cudaSetDevice(c->device);
+    int rc = ensure_init(c);
+    if (rc) return rc;
+    int n = 0;
+    if ((rc = inst_count(c, inst, &n))) return rc;
+    std::vector<float4> buf;
+    if (FCX || FCY || FCZ) {
+        if ((rc = fetch4(c, c->d.FC, inst, n, buf))) return rc;
+        to_soa(buf, n, FCX, FCY, FCZ);
+    }
+    if (FDX || FDY || FDZ) {
+        if ((rc = fetch4(c, c->d.FD, inst, n, buf))) return rc;
+        to_soa(buf, n, FDX, FDY, FDZ);
+    }
+    return CS3D_OK;
+}
+
+int cs3d_get_cells(cs3d_ctx *c, int inst, float *cm, float *volume, float *area, float *aabb)
+{
+    if (!c || inst < 0 || inst >= c->n_inst) return CS3D_E_ARG;
+    cudaSetDevice(c->device);
+    int rc = ensure_init(c);
+    if (rc) return rc;
+    int n = 0;
+    if ((rc = inst_count(c, inst, &n))) return rc;
+    const int base = c->hprm[inst].base;
+    if (cm && n) {
+        std::vector<float4> b(n);
+        CK(cudaMemcpyAsync(b.data(), c->d.CM + base, sizeof(float4) * n, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for (int k = 0; k < n; ++k) { cm[3 * k] = b[k].x; cm[3 * k + 1] = b[k].y; cm[3 * k + 2] = b[k].z; }
+    }
+    if (volume && n) CK(cudaMemcpyAsync(volume, c->d.vol + base, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
+    if (area && n) CK(cudaMemcpyAsync(area, c->d.area + base, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
+    if (aabb && n) {
+        std::vector<float4> b(2 * (size_t)n);
+        int par = (int)(c->host_step & 1);
+        CK(cudaMemcpyAsync(b.data(), c->d.aabb[par] + 2 * (size_t)base, sizeof(float4) * 2 * n, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for (int k = 0; k < n; ++k) {
+            const float4 lo = b[2 * k], hi = b[2 * k + 1];
+            float *o = aabb + 6 * k;
+            o[0] = lo.x; o[1] = hi.x; o[2] = lo.y; o[3] = hi.y; o[4] = lo.z; o[5] = hi.z;
+        }
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return CS3D_OK;
+}
+
+int cs3d_get_grid(cs3d_ctx *c, int inst, float minmax[6], int divs[3])
+{
+    if (!c || inst < 0 || inst >= c->n_inst) return CS3D_E_ARG;
+    cudaSetDevice(c->device);
+    int rc = ensure_init(c);
+    if (rc) return rc;
+    InstState st;
+    CK(cudaMemcpyAsync(&st, &c->d.st[inst], sizeof st, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    int par = (int)(c->host_step & 1);
+    for (int q = 0; q < 3; ++q) {
+        auto dec = [](int i) { int b = i >= 0 ? i : i ^ 0x7fffffff; float f; memcpy(&f, &b, 4); return f; };
+        float mn = std::min(dec(st.mm[par][2 * q]), 1.0e8f);
+        float mx = std::max(dec(st.mm[par][2 * q + 1]), -1.0e8f);
+        if (minmax) { minmax[2 * q] = mn; minmax[2 * q + 1] = mx; }
+        volatile float ext = mx - mn;
+        volatile float r = ext / DL;
+        if (divs) divs[q] = (int)(r + 1.0f);
+    }
+    return CS3D_OK;
+}
+
+int cs3d_get_pairs(cs3d_ctx *c, int inst, int kind, int32_t *out, long long max_pairs, long long *count)
+{
+    if (!c || inst < 0 || inst >= c->n_inst || kind < 0 || kind > 1 || !count) return CS3D_E_ARG;
+    cudaSetDevice(c->device);
+    int rc = ensure_init(c);
+    if (rc) return rc;
+    unsigned long long np = 0;
+    CK(cudaMemcpyAsync(&np, c->d.n_pairs, sizeof np, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if ((long long)np > c->d.pair_cap) return CS3D_E_CAPACITY;
+    std::vector<int4> buf(np);
+    if (np) CK(cudaMemcpyAsync(buf.data(), c->d.pairs, sizeof(int4) * np, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const int base = c->hprm[inst].base, cap = c->hprm[inst].cap;
+    long long k = 0;
+    for (const int4 &p : buf) {
+        int a = p.x >> 8, i = p.x & 255, b = p.y >> 8, j = p.y & 255;
+        if (a < base || a >= base + cap) continue;
+        bool keep = kind == 0 ? (p.z & 1) : 1;
+        if (!keep) continue;
+        if (out && k < max_pairs) {
+            out[4 * k] = a - base; out[4 * k + 1] = i; out[4 * k + 2] = b - base; out[4 * k + 3] = j;
+        }
+        ++k;
+    }
+    *count = k;
+    return CS3D_OK;
+}
+
+int cs3d_get_events(cs3d_ctx *c, int inst, int32_t *out, int max_events, int *count)
+{
+    if (!c || inst < 0 || inst >= c->n_inst || !count) return CS3D_E_ARG;
+    cudaSetDevice(c->device);
+    int ne = 0;
+    CK(cudaMemcpyAsync(&ne, c->d.n_events, sizeof ne, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    ne = std::min(ne, c->d.ev_cap);
+    std::vector<int4> buf(ne);
+    if (ne) CK(cudaMemcpyAsync(buf.data(), c->d.events, sizeof(int4) * ne, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::vector<int4> mine;
+    for (auto &e : buf) if (e.x == inst) mine.push_back(e);
+    std::sort(mine.begin(), mine.end(), [](const int4 &a, const int4 &b) {
+        return a.y != b.y ? a.y < b.y : a.z < b.z;
+    });
+    int k = 0;
+    for (auto &e : mine) {
+        if (out && k < max_events) { out[3 * k] = e.y; out[3 * k + 1] = e.z; out[3 * k + 2] = e.w; }
+        ++k;
+    }
+    *count = k;
+    return CS3D_OK;
+}
+
+int cs3d_last_error(cs3d_ctx *c, int inst, uint32_t *bits)
+{
+    if (!c || !bits || inst < -1 || inst >= c->n_inst) return CS3D_E_ARG;
+    cudaSetDevice(c->device);
+    std::vector<InstState> st(c->n_inst);
+    CK(cudaMemcpyAsync(st.data(), c->d.st, sizeof(InstState) * c->n_inst, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    unsigned b = 0;
+    for (int k = 0; k < c->n_inst; ++k)
+        if (inst < 0 || k == inst) b |= st[k].err;
+    *bits = b;
+    return CS3D_OK;
+}
+
+int cs3d_get_stats(cs3d_ctx *c, long long *stats, int n)
+{
+    if (!c || !stats || n <= 0) return CS3D_E_ARG;
+    cudaSetDevice(c->device);
+    std::vector<InstState> st(c->n_inst);
+    CK(cudaMemcpyAsync(st.data(), c->d.st, sizeof(InstState) * c->n_inst, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    long long v[8] = {c->host_step, 0, 0, 0, c->launches_per_step, 0, 0, 0};
+    for (auto &q : st) {
+        v[1] += q.rebuilds;
+        v[2] = std::max<long long>(v[2], q.max_entries);
+        v[3] = std::max<long long>(v[3], q.max_cand);
+    }
+    for (int k = 0; k < n && k < 8; ++k) stats[k] = v[k];
+    return CS3D_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,159 @@
+// cs3d_dev.cuh -- device-side data structures and helpers shared by the
+// kernels of libcs3d.so.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/cs3d.h"
+
+namespace cs3d {
+
+constexpr int SLOTS = CS3D_SLOTS;      // node slots per cell (reference padding)
+constexpr int NODES = CS3D_NODES;      // real nodes per cell
+constexpr int MAXC = CS3D_MAX_CAND;    // contact-candidate cells per cell
+constexpr int MAXE = CS3D_MAX_ENTRIES; // contact-candidate nodes per node
+constexpr float DL = 2.9f;             // reference grid spacing, src/GPUbounce.cu:756
+constexpr int NARM = NODES * 3 * 2;    // arm-end forces of the 540 angles
+
+// Per-instance constants (uploaded once).
+struct InstParams {
+    float mass, rr, ra, rs, as, E, stiff1, gint, gext, go, divvol, dt, maxp, minp, growth, thresh;
+    float box[3];
+    float ra2;      // fl(ra*ra), the reference's float cut-off
+    float asE;      // fl(as*E), attraction coefficient
+    float rsE;      // fl(rs*E), repulsion coefficient
+    float wallk;    // fl(100*E), rigid-box wall stiffness, src/propagate.cu:481
+    float rlist;    // neighbour-list radius (ra + skin)
+    float skin;
+    int check_sph, angles, rigid, daught_same, div_steps;
+    int base, cap;
+};
+
+// Per-instance mutable state (device resident).
+struct InstState {
+    int n;                 // current cell count
+    int step;              // number of the step in progress / last finished
+    unsigned err;          // CS3D_ERRBIT_*
+    int rebuild;           // neighbour list must be rebuilt before the next sweep
+    int mm[2][6];          // grid extents (ordered-int min/max) by step parity
+    float disp_acc;        // displacement bound accumulated since the last rebuild
+    unsigned disp_step;    // max node displacement of the current step (float bits)
+    int div_count;         // divisions in the current step
+    int force_rebuild;
+    int bmm[6];            // build-grid extents (ordered ints)
+    unsigned maxext;       // largest cell extent (float bits)
+    float borg[3];         // build-grid origin
+    float bh;              // build-grid bin size
+    int bdim[3];
+    int boff;              // first bin of this instance in the global bin array
+    int max_entries, max_cand;
+    int rebuilds;
+    // RANMAR, src/marsaglia.h:50-52
+    float u[98];
+    float rc, rcd, rcm;
+    int i97, j97;
+};
+
+struct DivEntry {
+    int parent, daughter, inst, pad;
+    float n[4];
+};
+
+// Static mesh tables in global memory (7 KB, L1/L2 resident).
+struct Topo {
+    uint32_t *nnpack;   // [192] nn0 | nn1<<8 | nn2<<16 | (sign&0xff)<<24
+    float4 *r0;         // [192] equilibrium lengths to nn0..2
+    float4 *th0;        // [192] aij, ajk, aik
+    uint4 *arm;         // [192] six uint16 indices into the arm-force array
+    uint8_t *faces;     // [92*7]
+};
+
+// Pointers of a context (passed by value to every kernel).
+struct Dev {
+    int n_inst;
+    int cap_total;
+    InstParams *prm;
+    InstState *st;
+    Topo topo;
+    float4 *X;          // positions (x, y, z, 0), [cell*192 + node]
+    float4 *V;          // velocities (state)
+    float4 *Vb;         // velocities after the half kicks (v3), read by neighbours
+    float4 *FC, *FD;    // forces
+    float4 *CM;         // centre of mass
+    float *press, *E, *vol, *area;
+    uint8_t *divflag;
+    float4 *aabb[2];    // [2*cell] lo, hi  (stale boxes by parity)
+    float4 *aabb_cur;   // boxes at neighbour-list build
+    int *cell_inst;
+    int *work;          // active cells
+    int *work_n;
+    int *cand;          // [cell*MAXC]
+    int *ncand;         // [cell]
+    uint16_t *ent;      // [(cell*MAXE + k)*192 + node]
+    uint8_t *nent;      // [cell*192 + node]
+    int *bin_count, *bin_start, *bin_cells, *cell_bin, *cell_rank;
+    int bin_cap;
+    int *total_bins;
+    DivEntry *divtab;
+    int *div_total;
+    int4 *events;       // (inst, step, parent, daughter)
+    int *n_events;
+    int ev_cap;
+    int *flags;         // [0] any rebuild, [1] any division
+    int4 *pairs;        // (cell_a<<8 | node_i, cell_b<<8 | node_j, kind, 0)
+    unsigned long long *n_pairs;
+    long long pair_cap;
+    int record_pairs;
+};
+
+__device__ __forceinline__ int f2o(float f)
+{
+    int i = __float_as_int(f);
+    return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__device__ __forceinline__ float o2f(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff); }
+
+// Reference float arithmetic without FMA contraction (pair and box tests).
+__device__ __forceinline__ float r2_nc(float dx, float dy, float dz)
+{
+    return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+}
+
+// Grid divisions, src/GPUbounce.cu:1332-1334.
+__device__ __forceinline__ int grid_div(float mn, float mx)
+{
+    return (int)__fadd_rn(__fdiv_rn(__fsub_rn(mx, mn), DL), 1.0f);
+}
+
+// Node bin along one axis, src/propagate.cu:360-370.
+__device__ __forceinline__ int node_bin_axis(float x, float mn, int div)
+{
+    int s = (int)__fdiv_rn(__fsub_rn(x, mn), DL);
+    if (s < 0) s = 0;
+    if (s >= div) s = div - 1;
+    return s;
+}
+
+// makeNNlist insertion range along one axis, src/propagatebound.cu:224-241.
+__device__ __forceinline__ void bin_range_axis(float lo, float hi, float attrac, float mn, int div,
+                                               int &st, int &en)
+{
+    st = (int)__fdiv_rn(__fsub_rn(__fsub_rn(lo, attrac), mn), DL);
+    if (st < 0) st = 0;
+    en = (int)__fdiv_rn(__fsub_rn(__fadd_rn(hi, attrac), mn), DL);
+    if (en >= div) en = div - 1;
+}
+
+// Bounding-box filter, src/propagate.cu:382-392.  True if the cell is kept.
+__device__ __forceinline__ bool aabb_keep(float4 lo, float4 hi, float X, float Y, float Z, float ra2)
+{
+    float a = __fsub_rn(X, hi.x), b = __fsub_rn(lo.x, X);
+    float dx = __fadd_rn(__fmul_rn((float)(a > 0.0f), a), __fmul_rn((float)(b > 0.0f), b));
+    a = __fsub_rn(Y, hi.y); b = __fsub_rn(lo.y, Y);
+    float dy = __fadd_rn(__fmul_rn((float)(a > 0.0f), a), __fmul_rn((float)(b > 0.0f), b));
+    a = __fsub_rn(Z, hi.z); b = __fsub_rn(lo.z, Z);
+    float dz = __fadd_rn(__fmul_rn((float)(a > 0.0f), a), __fmul_rn((float)(b > 0.0f), b));
+    return !(r2_nc(dx, dy, dz) > ra2);
+}
+
+}  // namespace cs3d

@@ -1,0 +1,286 @@
+/*
+ * cs3d.h -- C ABI of libcs3d.so, the B200-native timestep of CellSim3D.
+ *
+ * Every function returns an int status: 0 = success, negative = CS3D_E_*.
+ * No C++ exceptions and no torch types cross this boundary; all buffers are
+ * plain pointers with explicit sizes.  Host arrays are caller-owned and are
+ * copied synchronously on the context's stream.  A context owns all of its
+ * device memory and is used by one host thread at a time.
+ *
+ * Layout conventions follow the reference (SoftSimu/CellSim3D):
+ *   - per-node arrays are SoA float, indexed cell*192 + node for nodes
+ *     0..179 (slots 180..191 are padding), src/GPUbounce.cu:365-373;
+ *   - per-cell arrays are indexed by cell;
+ *   - neighbour tables are [k*192 + node], src/GPUbounce.cu:1829-1832.
+ */
+#ifndef CS3D_H
+#define CS3D_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CS3D_SLOTS 192
+#define CS3D_NODES 180
+#define CS3D_FACES 92
+
+/* ---- status codes ----------------------------------------------------- */
+#define CS3D_OK                 0
+#define CS3D_E_ARG             -1   /* invalid argument / size */
+#define CS3D_E_CUDA            -2   /* a CUDA runtime call failed */
+#define CS3D_E_NOMEM           -3   /* device or host allocation failed */
+#define CS3D_E_IO              -4   /* file could not be opened / read */
+#define CS3D_E_PARSE           -5   /* inp.json malformed or missing section */
+#define CS3D_E_CONFIG          -6   /* parameter validation failed */
+#define CS3D_E_DEVICE_FLAGS    -7   /* a kernel raised an error bit, see cs3d_last_error */
+#define CS3D_E_CAPACITY       -69   /* population exceeded capacity, src/GPUbounce.cu:1265-1270 */
+#define CS3D_E_UNSUPPORTED     -8   /* feature of the reference outside this build */
+
+/* ---- device error bits (cs3d_last_error) ------------------------------ */
+#define CS3D_ERRBIT_NAN            0x001u  /* NaN position, src/propagate.cu:241-248 */
+#define CS3D_ERRBIT_CAPACITY       0x002u  /* division past capacity */
+#define CS3D_ERRBIT_CAND_OVERFLOW  0x004u  /* > CS3D_MAX_CAND contact cells for one cell */
+#define CS3D_ERRBIT_ENTRY_OVERFLOW 0x008u  /* > CS3D_MAX_ENTRIES contact nodes for one node */
+#define CS3D_ERRBIT_NONFINITE_VOL  0x010u  /* src/volume.cu:134-139 */
+#define CS3D_ERRBIT_BAD_NORMAL     0x020u  /* |n| != 1, src/postscriptinit.cu:215-219 */
+#define CS3D_ERRBIT_GRID_OVERFLOW  0x040u  /* rebuild grid larger than its buffer */
+#define CS3D_ERRBIT_PAIR_OVERFLOW  0x080u  /* pair-recording buffer full */
+
+#define CS3D_MAX_CAND      32   /* contact-candidate cells per cell */
+#define CS3D_MAX_ENTRIES   48   /* contact-candidate nodes per node */
+
+/* ---- parameters of the hot path (one simulation instance) ------------- */
+/* Field meaning and units are the reference's inp.json keys.              */
+typedef struct cs3d_params {
+    float particle_mass;        /* core.particle_mass */
+    float repulsion_range;      /* core.repulsion_range */
+    float attraction_range;     /* core.attraction_range */
+    float repulsion_strength;   /* core.repulsion_strength (x Youngs_mod) */
+    float attraction_strength;  /* core.attraction_strength (x Youngs_mod) */
+    float youngs_mod;           /* core.Youngs_mod */
+    float stiffness1;           /* core.stiffFactor1 * Youngs_mod, src/GPUbounce.cu:1953 */
+    float internal_damping;     /* core.internal_damping (gamma_int) */
+    float viscotic_damping;     /* core.viscotic_damping (gamma_ext) */
+    float gamma_visc;           /* core.gamma_visc (gamma_o) */
+    float division_vol;         /* core.division_Vol */
+    float time_interval;        /* core.time_interval */
+    float max_pressure;         /* core.maxPressure */
+    float min_pressure;         /* core.minPressure */
+    float growth_rate;          /* core.growth_rate (rMax; no population model) */
+    float thresh_dist;          /* walls.threshDist */
+    float box_len[3];           /* boxParams.box_len_{x,y,z} = boxMax */
+    int32_t check_sphericity;   /* core.checkSphericity */
+    int32_t constrain_angles;   /* core.constrainAngles */
+    int32_t use_rigid_box;      /* boxParams.useRigidSimulationBox */
+    int32_t daught_same_stiffness; /* stiffnessParams.daughtSameStiffness */
+    int32_t div_time_steps;     /* core.div_time_steps */
+    int32_t rng_ij, rng_kl;     /* RANMAR seeds (see cs3d_seed_map) */
+} cs3d_params;
+
+/* ---- static mesh data ------------------------------------------------- */
+typedef struct cs3d_topology {
+    int32_t nn[3 * CS3D_SLOTS];     /* 0-based neighbours, [k*192 + node] */
+    int32_t sign[CS3D_NODES];       /* orientation sign per node */
+    float r0[3 * CS3D_SLOTS];       /* equilibrium bond lengths, [k*192 + node] */
+    float theta0[3 * CS3D_SLOTS];   /* [node*3 + {aij, ajk, aik}] */
+    int32_t faces[CS3D_FACES * 7];  /* C180_56 layout */
+} cs3d_topology;
+
+typedef struct cs3d_mesh {
+    float xyz[CS3D_NODES * 3];      /* C180 file, row-major */
+    int32_t nn[3 * CS3D_SLOTS];
+    int32_t sign[CS3D_NODES];
+    int32_t bonds[270 * 2];         /* C180C, 0-based */
+    int32_t faces[CS3D_FACES * 7];
+} cs3d_mesh;
+
+/* RANMAR generator state, src/marsaglia.h:50-52 */
+typedef struct cs3d_rng {
+    float u[98];
+    float c, cd, cm;
+    int32_t i97, j97;
+    int32_t ok;
+} cs3d_rng;
+
+/* Full inp.json contents, src/GPUbounce.cu:1914-2247 (all eight sections). */
+typedef struct cs3d_config {
+    /* core */
+    int32_t max_cells;              /* MaxNoofC180s */
+    float particle_mass, repulsion_range, attraction_range;
+    float repulsion_strength, attraction_strength, youngs_mod, stiff_factor1;
+    float viscotic_damping, internal_damping, gamma_visc, division_vol;
+    int32_t random_z_offset; float z_offset;
+    int32_t div_time_steps; float time_interval; int32_t restart;
+    int32_t traj_write_int; int32_t non_div_time_steps;
+    char traj_file_name[256]; int32_t binary_output;
+    float max_pressure, min_pressure, growth_rate;
+    int32_t check_sphericity, constrain_angles, do_adaptive_dt;
+    float dt_max, dt_tol; int32_t phase_count; int32_t write_cont_force;
+    char forces_file[256]; int32_t correct_com;
+    /* counting */
+    char mit_index_file[256]; int32_t count_only_internal; float radius_cutoff;
+    int32_t overwrite_mit_ind; int32_t cell_count_int;
+    /* population */
+    int32_t do_pop_model; float total_food, regular_consumption, division_consumption;
+    float death_release_food; int32_t cell_life_time; float max_pop;
+    /* walls */
+    int32_t use_walls; char perp_axis[8]; float d_axis, wall_len, wall_width, thresh_dist;
+    /* divParams */
+    int32_t use_div_plane_basis; float div_plane_basis[3];
+    /* stiffnessParams */
+    int32_t use_different_stiffnesses; float soft_stiff_factor; int32_t number_of_softer_cells;
+    float fraction_of_softer_cells; int32_t during_growth, daught_same_stiffness;
+    float closeness_to_center; int32_t start_at_pop, choose_random_cell_indices, recalc_r0;
+    /* boxParams */
+    int32_t use_rigid_box, use_pbcs; float box_length; float box_len[3];
+    int32_t flatbox, rand_pos;
+    /* rand_params */
+    int32_t add_rands, rand_seed, rand_dist; float rand_scale_factor;
+} cs3d_config;
+
+typedef struct cs3d_ctx cs3d_ctx;
+
+/* ---- host utilities (no GPU needed) ----------------------------------- */
+
+/* Library version (major*10000 + minor*100 + patch). */
+int cs3d_version(void);
+
+/* Message for a status code. */
+const char *cs3d_strerror(int status);
+
+/* Parse inp.json (// and C comments allowed) and apply the reference's
+ * validation.  Replaces read_json_params, src/GPUbounce.cu:1914-2247. */
+int cs3d_config_read_json(const char *path, cs3d_config *out, char *errbuf, int errlen);
+
+/* Hot-path parameters from a parsed config.  Seeds: cs3d_seed_map. */
+int cs3d_config_to_params(const cs3d_config *cfg, cs3d_params *out);
+
+/* Read C180, C180NN, C180C, C180_pentahexa from a directory.  Replaces the
+ * file readers of initialize_C180s and read_fullerene_nn,
+ * src/GPUbounce.cu:1616-1627 and :1814-1888. */
+int cs3d_mesh_read(const char *dir, cs3d_mesh *out);
+
+/* Equilibrium bond lengths and angles from cell 0's initial positions
+ * (192-stride arrays), host float arithmetic as src/GPUbounce.cu:1890-1908
+ * (R0) and :909-938 (theta0). */
+int cs3d_topology_build(const cs3d_mesh *mesh, const float *x0, const float *y0,
+                        const float *z0, cs3d_topology *out);
+
+/* RANMAR seeding, src/marsaglia.h:54-113.  Returns CS3D_E_ARG outside the
+ * legal seed range (the reference exits). */
+int cs3d_rng_init(cs3d_rng *rng, int ij, int kl);
+/* RANMAR draws, src/marsaglia.h:115-144. */
+int cs3d_rng_draw(cs3d_rng *rng, float *out, int len);
+/* Marsaglia sphere point, src/RandomVector.h:8-24. */
+int cs3d_rng_random_vector(cs3d_rng *rng, float n[3]);
+/* rand_seed -> (ij, kl): (seed, 100*seed) as src/GPUbounce.cu:1796-1799 for
+ * 0 <= seed <= 300; larger seeds fold into the legal range
+ * (seed mod 31329, 100*seed mod 30082). */
+int cs3d_seed_map(int seed, int *ij, int *kl);
+
+/* Initial cell placement, src/GPUbounce.cu:1598-1774 (lattice or random
+ * insertion with RANMAR draws).  X/Y/Z have capacity n_cells*192. */
+int cs3d_init_positions(const cs3d_config *cfg, const cs3d_mesh *mesh, int n_cells,
+                        cs3d_rng *rng, float *X, float *Y, float *Z);
+
+/* Binary trajectory writer, src/GPUbounce.cu:1007-1018 (header),
+ * :2446-2477 (frames), :1508-1511 (final cell count).  Read by
+ * scripts/celldiv.py. */
+typedef struct cs3d_traj cs3d_traj;
+int cs3d_traj_open(const char *path, int max_cells, int variable_stiffness, int max_frames,
+                   cs3d_traj **out);
+int cs3d_traj_write_frame(cs3d_traj *t, int step, int frame, int n_cells, const float *X,
+                          const float *Y, const float *Z, const int32_t *types);
+int cs3d_traj_close(cs3d_traj *t, int final_cells);
+
+/* ---- device context --------------------------------------------------- */
+
+/* One simulation with room for capacity_cells cells.  stream may be NULL
+ * (the context creates its own).  Replaces the allocation block of main,
+ * src/GPUbounce.cu:358-527. */
+int cs3d_create(const cs3d_params *params, const cs3d_topology *topo, int capacity_cells,
+                int device, void *stream, cs3d_ctx **out);
+
+/* A batch of n_inst independent simulations stepped together (per-instance
+ * parameters, seeds, boxes and capacities).  No counterpart in the
+ * reference, which runs one simulation per process. */
+int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topology *topo,
+                         const int *capacity_cells, int device, void *stream, cs3d_ctx **out);
+
+/* Load the state of instance inst: n_cells cells, 192-stride SoA.
+ * V*, pressure and youngs may be NULL (zeros, min_pressure, stiffness1 --
+ * the reference's defaults, src/GPUbounce.cu:449-451, :867-871, :617-620).
+ * The initial centre of mass, grid and first force evaluation
+ * (src/GPUbounce.cu:739-763, :978-1004) run before the next step or read. */
+int cs3d_load_state(cs3d_ctx *ctx, int inst, int n_cells, const float *X, const float *Y,
+                    const float *Z, const float *VX, const float *VY, const float *VZ,
+                    const float *pressure, const float *youngs);
+
+/* Replace the RANMAR state of instance inst (e.g. after host-side draws
+ * for random placement). */
+int cs3d_set_rng(cs3d_ctx *ctx, int inst, const cs3d_rng *rng);
+
+/* Advance every instance by n_steps timesteps of src/GPUbounce.cu:1055-1338.
+ * Returns CS3D_E_DEVICE_FLAGS or CS3D_E_CAPACITY if a kernel raised an
+ * error bit (see cs3d_last_error). */
+int cs3d_step(cs3d_ctx *ctx, int n_steps);
+
+/* Read back instance inst.  Any output pointer may be NULL. */
+int cs3d_get_state(cs3d_ctx *ctx, int inst, int *n_cells, float *X, float *Y, float *Z,
+                   float *VX, float *VY, float *VZ, float *pressure, float *youngs);
+
+/* Conservative (fConList) and dissipative (fDisList) forces of the last
+ * evaluation, 192-stride SoA. */
+int cs3d_get_forces(cs3d_ctx *ctx, int inst, float *FCX, float *FCY, float *FCZ,
+                    float *FDX, float *FDY, float *FDZ);
+
+/* Per-cell centre of mass (3*n), volume, area and bounding box (6*n:
+ * minx maxx miny maxy minz maxz) as of the last step. */
+int cs3d_get_cells(cs3d_ctx *ctx, int inst, float *cm, float *volume, float *area,
+                   float *aabb);
+
+/* The neighbour-grid extents (Minx[0..5]) and divisions used by the next
+ * force evaluation. */
+int cs3d_get_grid(cs3d_ctx *ctx, int inst, float minmax[6], int divs[3]);
+
+/* Options. */
+#define CS3D_OPT_RECORD_PAIRS  1   /* value 0/1: record the contact pairs used */
+#define CS3D_OPT_SKIN          2   /* value = skin length in units of 1e-6 */
+#define CS3D_OPT_PAIR_CAPACITY 3   /* value = max recorded pairs */
+int cs3d_set_option(cs3d_ctx *ctx, int option, long long value);
+
+/* Contact pairs recorded during the last force evaluation (requires
+ * CS3D_OPT_RECORD_PAIRS).  kind 0: conservative (strict cut-off,
+ * src/propagate.cu:421); kind 1: dissipative (src/propagate.cu:641).
+ * out receives (cell_a, node_i, cell_b, node_j) quadruples. */
+int cs3d_get_pairs(cs3d_ctx *ctx, int inst, int kind, int32_t *out, long long max_pairs,
+                   long long *count);
+
+/* Division events (step, parent, daughter) since creation. */
+int cs3d_get_events(cs3d_ctx *ctx, int inst, int32_t *out, int max_events, int *count);
+
+/* Error bits raised on the device for instance inst (OR of CS3D_ERRBIT_*). */
+int cs3d_last_error(cs3d_ctx *ctx, int inst, uint32_t *bits);
+
+/* Counters: [0] steps, [1] neighbour-list rebuilds, [2] max entries per node
+ * seen, [3] max candidate cells per cell seen, [4] kernel launches per step. */
+int cs3d_get_stats(cs3d_ctx *ctx, long long *stats, int n);
+
+/* Profiling pass: n_steps steps launched kernel by kernel (not as a graph)
+ * with a CUDA event after each launch on the context's stream; kernel_ms
+ * receives the average time of each launch slot of a step, names a
+ * comma-separated list of their names.  No counterpart in the reference. */
+int cs3d_profile_step(cs3d_ctx *ctx, int n_steps, float *kernel_ms, char *names, int names_len,
+                      int max_kernels, int *n_kernels);
+
+/* Device time of the last cs3d_step call (ms, CUDA events). */
+int cs3d_last_step_ms(cs3d_ctx *ctx, float *ms);
+
+int cs3d_destroy(cs3d_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CS3D_H */
