@@ -226,6 +226,8 @@ def run_cs3d(args, world, rank, local):
             "gpu_launches": int(stats["launches_per_step"]) * args.steps,
             "nl_rebuilds": stats["rebuilds"],
             "max_entries": stats["max_entries"],
+            "max_cand": stats["max_cand"],
+            "max_halo": stats["max_halo"],
             "clocks": clk.summary(),
         }
         if e2e:

@@ -192,6 +192,12 @@ class Ensemble:
     def set_rng(self, inst, rng):
         _lib.check(_lib.lib().cs3d_set_rng(self.h, inst, C.byref(rng.state)), "cs3d_set_rng")
 
+    def get_rng(self, inst=0):
+        r = Ranmar.__new__(Ranmar)
+        r.state = Rng()
+        _lib.check(_lib.lib().cs3d_get_rng(self.h, inst, C.byref(r.state)), "cs3d_get_rng")
+        return r
+
     def set_option(self, option, value):
         _lib.check(_lib.lib().cs3d_set_option(self.h, option, int(value)), "cs3d_set_option")
 
@@ -284,7 +290,8 @@ class Ensemble:
     def stats(self):
         s = (C.c_longlong * 8)()
         _lib.check(_lib.lib().cs3d_get_stats(self.h, s, 8), "cs3d_get_stats")
-        return {"steps": s[0], "rebuilds": s[1], "max_entries": s[2], "max_cand": s[3], "launches_per_step": s[4]}
+        return {"steps": s[0], "rebuilds": s[1], "max_entries": s[2], "max_cand": s[3], "launches_per_step": s[4],
+                "max_halo": s[5]}
 
 
 class Simulation(Ensemble):

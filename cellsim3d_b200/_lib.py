@@ -75,7 +75,7 @@ EXPORTS = [
     "cs3d_version", "cs3d_strerror", "cs3d_config_read_json", "cs3d_config_to_params", "cs3d_mesh_read",
     "cs3d_topology_build", "cs3d_rng_init", "cs3d_rng_draw", "cs3d_rng_random_vector", "cs3d_seed_map",
     "cs3d_init_positions", "cs3d_traj_open", "cs3d_traj_write_frame", "cs3d_traj_close", "cs3d_create",
-    "cs3d_create_ensemble", "cs3d_load_state", "cs3d_set_rng", "cs3d_step", "cs3d_get_state",
+    "cs3d_create_ensemble", "cs3d_load_state", "cs3d_set_rng", "cs3d_get_rng", "cs3d_step", "cs3d_get_state",
     "cs3d_get_forces", "cs3d_get_cells", "cs3d_get_grid", "cs3d_set_option", "cs3d_get_pairs",
     "cs3d_get_events", "cs3d_last_error", "cs3d_get_stats", "cs3d_profile_step", "cs3d_last_step_ms",
     "cs3d_destroy",
@@ -126,6 +126,7 @@ def lib():
                                        C.POINTER(P)]
     L.cs3d_load_state.argtypes = [P, C.c_int, C.c_int, fp, fp, fp, fp, fp, fp, fp, fp]
     L.cs3d_set_rng.argtypes = [P, C.c_int, C.POINTER(Rng)]
+    L.cs3d_get_rng.argtypes = [P, C.c_int, C.POINTER(Rng)]
     L.cs3d_step.argtypes = [P, C.c_int]
     L.cs3d_get_state.argtypes = [P, C.c_int, ip, fp, fp, fp, fp, fp, fp, fp, fp]
     L.cs3d_get_forces.argtypes = [P, C.c_int, fp, fp, fp, fp, fp, fp]

@@ -114,7 +114,15 @@ int upload_topology(cs3d_ctx *c, const cs3d_topology *t)
         if (t->faces[f] < 0 || t->faces[f] >= NODES) return CS3D_E_ARG;
         faces[f] = (uint8_t)t->faces[f];
     }
+    std::vector<double2> cs0(3 * SLOTS, make_double2(1.0, 0.0));
+    for (int i = 0; i < NODES; ++i)
+        for (int k = 0; k < 3; ++k) {
+            const double th = (double)t->theta0[3 * i + k];
+            cs0[3 * i + k] = make_double2(cos(th), sin(th));
+        }
     int rc;
+    if ((rc = dalloc(c, &c->d.topo.cs0, 3 * SLOTS))) return rc;
+    CK(cudaMemcpyAsync(c->d.topo.cs0, cs0.data(), sizeof(double2) * 3 * SLOTS, cudaMemcpyHostToDevice, c->stream));
     if ((rc = dalloc(c, &c->d.topo.nnpack, SLOTS))) return rc;
     if ((rc = dalloc(c, &c->d.topo.r0, SLOTS))) return rc;
     if ((rc = dalloc(c, &c->d.topo.th0, SLOTS))) return rc;
@@ -229,7 +237,7 @@ int run_init(cs3d_ctx *c)
     CK(cudaGetLastError());
     int rc = launch_nl_build(c);
     if (rc) return rc;
-    k_s1<true><<<c->grid_cells, SLOTS, 0, s>>>(d, 0);
+    k_s1<true><<<c->grid_cells, SLOTS, sizeof(S1Smem), s>>>(d, 0);
     CK(cudaGetLastError());
     c->host_step = 0;
     c->need_init = false;
@@ -247,8 +255,10 @@ int launch_step(cs3d_ctx *c, int par, bool div, const Prof &pf = Prof())
     int rc = launch_nl_build(c, pf);
     if (rc) return rc;
     n += 7;
-    k_s1<false><<<c->grid_cells, SLOTS, 0, s>>>(d, par); ++n; pf.mark(s, "s1_con_dis");
-    k_s2<<<c->grid_cells, SLOTS, 0, s>>>(d, par); ++n; pf.mark(s, "s2_dis_geom");
+    k_s1<false><<<c->grid_cells, SLOTS, sizeof(S1Smem), s>>>(d, par); ++n; pf.mark(s, "s1_con_dis");
+    if (div) k_s2<true><<<c->grid_cells, SLOTS, 0, s>>>(d, par);
+    else k_s2<false><<<c->grid_cells, SLOTS, 0, s>>>(d, par);
+    ++n; pf.mark(s, "s2_dis_geom");
     if (div) {
         k_div_select<<<c->n_inst, 256, 0, s>>>(d, par); ++n; pf.mark(s, "div_select");
         k_div_apply<<<c->grid_cells, SLOTS, 0, s>>>(d, par); ++n; pf.mark(s, "div_apply");
@@ -363,6 +373,7 @@ int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topol
     }
     Dev &d = c->d;
     d.n_inst = n_inst;
+    d.single = n_inst == 1 ? 1 : 0;
     d.cap_total = c->cap_total;
     const size_t nodes = (size_t)c->cap_total * SLOTS;
     int rc = CS3D_OK;
@@ -378,6 +389,9 @@ int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topol
     AL(d.cell_inst, c->cap_total);
     AL(d.work, c->cap_total); AL(d.work_n, 1);
     AL(d.cand, (size_t)c->cap_total * MAXC); AL(d.ncand, c->cap_total);
+    AL(d.halo, (size_t)c->cap_total * HMAX); AL(d.halo_n, c->cap_total);
+    AL(d.halo_slot, (size_t)c->cap_total * HMAX);
+    AL(d.Xb, nodes);
     AL(d.ent, (size_t)c->cap_total * MAXE * SLOTS); AL(d.nent, nodes);
     d.bin_cap = 8 * c->cap_total + 65536;
     AL(d.bin_count, (size_t)d.bin_cap + 1); AL(d.bin_start, (size_t)d.bin_cap + 1);
@@ -412,7 +426,11 @@ int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topol
         free_all(c); delete c; return CS3D_E_CUDA;
     }
     int occ = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_s1<false>, SLOTS, 0);
+    if (cudaFuncSetAttribute(k_s1<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(S1Smem)) ||
+        cudaFuncSetAttribute(k_s1<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(S1Smem))) {
+        free_all(c); delete c; return CS3D_E_CUDA;
+    }
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_s1<false>, SLOTS, sizeof(S1Smem));
     c->grid_cells = std::max(1, std::min(c->cap_total, c->nsm * std::max(occ, 1)));
     c->grid_flat = std::max(1, std::min((c->cap_total + 255) / 256 + 1, c->nsm * 8));
     *out = c;
@@ -526,6 +544,20 @@ int cs3d_set_rng(cs3d_ctx *c, int inst, const cs3d_rng *r)
     st.rc = r->c; st.rcd = r->cd; st.rcm = r->cm; st.i97 = r->i97; st.j97 = r->j97;
     CK(cudaMemcpyAsync(&c->d.st[inst], &st, sizeof st, cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    return CS3D_OK;
+}
+
+int cs3d_get_rng(cs3d_ctx *c, int inst, cs3d_rng *r)
+{
+    if (!c || !r || inst < 0 || inst >= c->n_inst) return CS3D_E_ARG;
+    cudaSetDevice(c->device);
+    InstState st;
+    CK(cudaMemcpyAsync(&st, &c->d.st[inst], sizeof st, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    memset(r, 0, sizeof *r);
+    memcpy(r->u, st.u, sizeof r->u);
+    r->c = st.rc; r->cd = st.rcd; r->cm = st.rcm; r->i97 = st.i97; r->j97 = st.j97;
+    r->ok = 1;
     return CS3D_OK;
 }
 
@@ -787,6 +819,7 @@ int cs3d_get_stats(cs3d_ctx *c, long long *stats, int n)
     CK(cudaMemcpyAsync(st.data(), c->d.st, sizeof(InstState) * c->n_inst, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     long long v[8] = {c->host_step, 0, 0, 0, c->launches_per_step, 0, 0, 0};
+    for (auto &q : st) v[5] = std::max<long long>(v[5], q.max_halo);
     for (auto &q : st) {
         v[1] += q.rebuilds;
         v[2] = std::max<long long>(v[2], q.max_entries);

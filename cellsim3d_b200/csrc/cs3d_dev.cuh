@@ -12,6 +12,7 @@ constexpr int SLOTS = CS3D_SLOTS;      // node slots per cell (reference padding
 constexpr int NODES = CS3D_NODES;      // real nodes per cell
 constexpr int MAXC = CS3D_MAX_CAND;    // contact-candidate cells per cell
 constexpr int MAXE = CS3D_MAX_ENTRIES; // contact-candidate nodes per node
+constexpr int HMAX = CS3D_MAX_HALO;    // distinct contact-candidate nodes per cell
 constexpr float DL = 2.9f;             // reference grid spacing, src/GPUbounce.cu:756
 constexpr int NARM = NODES * 3 * 2;    // arm-end forces of the 540 angles
 
@@ -46,7 +47,7 @@ struct InstState {
     float bh;              // build-grid bin size
     int bdim[3];
     int boff;              // first bin of this instance in the global bin array
-    int max_entries, max_cand;
+    int max_entries, max_cand, max_halo;
     int rebuilds;
     // RANMAR, src/marsaglia.h:50-52
     float u[98];
@@ -64,6 +65,7 @@ struct Topo {
     uint32_t *nnpack;   // [192] nn0 | nn1<<8 | nn2<<16 | (sign&0xff)<<24
     float4 *r0;         // [192] equilibrium lengths to nn0..2
     float4 *th0;        // [192] aij, ajk, aik
+    double2 *cs0;       // [192*3] (cos, sin) of aij, ajk, aik in FP64
     uint4 *arm;         // [192] six uint16 indices into the arm-force array
     uint8_t *faces;     // [92*7]
 };
@@ -87,9 +89,14 @@ struct Dev {
     int *cell_inst;
     int *work;          // active cells
     int *work_n;
+    int single;         // one instance with base 0: the work table is the identity
     int *cand;          // [cell*MAXC]
     int *ncand;         // [cell]
-    uint16_t *ent;      // [(cell*MAXE + k)*192 + node]
+    int *halo;          // [cell*HMAX] global node index (cell*192 + node) of the contact candidates
+    uint8_t *halo_slot; // [cell*HMAX] candidate-cell slot of each halo node
+    int *halo_n;        // [cell]
+    float4 *Xb;         // positions at the last neighbour-list build
+    uint16_t *ent;      // [(cell*MAXE + k)*192 + node] halo index
     uint8_t *nent;      // [cell*192 + node]
     int *bin_count, *bin_start, *bin_cells, *cell_bin, *cell_rank;
     int bin_cap;

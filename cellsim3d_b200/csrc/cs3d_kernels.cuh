@@ -1,16 +1,21 @@
 // cs3d_kernels.cuh -- the per-timestep kernels of libcs3d.so (sm_100a).
 //
 // One CTA of 192 threads (six warps) owns one cell at a time and walks the
-// active-cell work table grid-stride; thread i owns node i.  The cell's 180
-// positions and velocities are staged in shared memory; the 540 bond angles
-// are evaluated once each (the reference evaluates each twice, once from the
-// vertex and once from the arm end) and their arm-end forces are gathered
-// from shared memory in the reference's summation order.  Inter-cell contact
-// candidates come from a per-node neighbour list built on the device and
-// reused while the accumulated displacement stays inside the skin; the exact
-// reference predicates (stale bounding box, stale grid bin, strict and
-// non-strict cut-offs) are re-evaluated on every candidate every step, so the
-// pair sets are exactly the reference's.
+// active cells grid-stride; thread i owns node i.  The cell's 180 positions
+// and velocities are staged in shared memory together with its "halo": the
+// nodes of neighbouring cells that lie within the neighbour-list radius of
+// any of its nodes, gathered in one round trip per step.  The 540 bond
+// angles are evaluated once each (the reference evaluates every angle twice,
+// from the vertex and from the arm end) and their arm-end forces are
+// gathered from shared memory in the reference's summation order.
+//
+// The neighbour list (per cell: candidate cells, halo, per-node halo
+// indices) is rebuilt on the device whenever the accumulated displacement
+// bound reaches the skin, or after a division.  Every step the reference's
+// own contact predicates -- stale grid bin of the node, stale bounding box of
+// the neighbour cell, strict (conservative) and non-strict (dissipative)
+// cut-offs in float -- are evaluated on every list entry, so the contact
+// pairs are exactly the reference's.
 #pragma once
 #include "cs3d_dev.cuh"
 
@@ -32,6 +37,11 @@ __device__ __forceinline__ T warp_sum(T v)
 
 __device__ __forceinline__ void atomic_or_err(InstState *st, unsigned bits) { atomicOr(&st->err, bits); }
 
+// Active cells: the identity for a single instance, else the work table.
+__device__ __forceinline__ int n_work(const Dev &d) { return d.single ? d.st[0].n : *d.work_n; }
+__device__ __forceinline__ int cell_of(const Dev &d, int w) { return d.single ? w : d.work[w]; }
+__device__ __forceinline__ int inst_of(const Dev &d, int a) { return d.single ? 0 : d.cell_inst[a]; }
+
 // Kick of the split velocity Verlet with the reference's mixed precision:
 // the float sum is scaled by the double literal 0.5 and divided by the mass
 // in double, then stored as float (src/propagate.cu:698-705, 721-723, 732-734).
@@ -40,55 +50,76 @@ __device__ __forceinline__ float kick(float v, float fsum, double m)
     return (float)((double)v + 0.5 * (double)fsum / m);
 }
 
-// Bond-angle term for one angle at a vertex with arms P (to the p-end node)
-// and Q (to the q-end node); Fp/Fq are GetAngleForce(P, Q) and
-// GetAngleForce(Q, P) of src/propagate.cu:26-60 (k = 1000, :335).
-__device__ __forceinline__ void angle_pair(float3 P, float3 Q, float th0, float3 &Fp, float3 &Fq)
+// sqrt(x) and 1/x of positive doubles: float hardware seeds refined by one
+// Newton step in FP64 (relative error ~1e-14, far below what the forces need,
+// and much cheaper than the correctly rounded FP64 sequences).
+__device__ __forceinline__ double sqrt_nr(double x)
 {
-#ifdef CS3D_ANGLE_F64
-    double px = P.x, py = P.y, pz = P.z, qx = Q.x, qy = Q.y, qz = Q.z;
-    double idk = px * qx + py * qy + pz * qz;
-    double rp2 = px * px + py * py + pz * pz;
-    double rq2 = qx * qx + qy * qy + qz * qz;
-    double c1 = -1.0 / sqrt(rp2 * rq2 - idk * idk + 1e-3);
-    double th = acos(idk / (sqrt(rp2) * sqrt(rq2) + 1e-3));
-    double f = -1000.0 * c1 * (th - (double)th0);
-    double cp = idk / rp2, cq = idk / rq2;
-    Fp = make_float3((float)(f * (qx - cp * px)), (float)(f * (qy - cp * py)), (float)(f * (qz - cp * pz)));
-    Fq = make_float3((float)(f * (px - cq * qx)), (float)(f * (py - cq * qy)), (float)(f * (pz - cq * qz)));
-#else
-    float idk = dot3(P, Q);
-    float rp2 = dot3(P, P);
-    float rq2 = dot3(Q, Q);
-    float c1 = -1.0f / sqrtf((float)((double)(rp2 * rq2 - idk * idk) + 1e-3));
-    float th = (float)acos((double)idk / ((double)(sqrtf(rp2) * sqrtf(rq2)) + 1e-3));
-    float f = -1000.0f * c1 * (th - th0);
-    float cp = idk / rp2, cq = idk / rq2;
-    Fp = make_float3(f * (Q.x - cp * P.x), f * (Q.y - cp * P.y), f * (Q.z - cp * P.z));
-    Fq = make_float3(f * (P.x - cq * Q.x), f * (P.y - cq * Q.y), f * (P.z - cq * Q.z));
-#endif
+    double y = (double)rsqrtf((float)x);
+    y = y * (1.5 - 0.5 * x * y * y);
+    return x * y;
+}
+__device__ __forceinline__ double rcp_nr(double x)
+{
+    double r = (double)__frcp_rn((float)x);
+    return r * (2.0 - x * r);
 }
 
-// Shared per-CTA data of the contact sweep: the candidate cells of the
-// current cell with their stale boxes and stale insertion bin ranges.
+// Bond-angle term for one angle at a vertex with arms P (to the p-end node)
+// and Q (to the q-end node); Fp/Fq are GetAngleForce(P, Q) and
+// GetAngleForce(Q, P) of src/propagate.cu:26-60 (k = 1000, :335), with the
+// same 1e-3 regularisers.  The force is proportional to theta - theta0, a
+// difference of two angles near 2 rad whose float rounding alone (1.2e-7)
+// would exceed the 1e-5 relative force bar, so it is formed without
+// rounding theta.  With u = cos(theta) (the reference's regularised ratio)
+// and s = sin(theta) = sqrt(1 - u^2) in FP64, and cos/sin of theta0 in FP64,
+//   theta - theta0 = atan2(s cos0 - u sin0, u cos0 + s sin0)
+// is a single well-conditioned FP64 arctangent instead of an arccosine of a
+// ratio followed by a cancelling subtraction.
+__device__ __forceinline__ void angle_pair(float3 P, float3 Q, double c0, double s0, double3 &Fp, double3 &Fq)
+{
+    const double px = P.x, py = P.y, pz = P.z, qx = Q.x, qy = Q.y, qz = Q.z;
+    const double idk = px * qx + py * qy + pz * qz;
+    const double rp2 = px * px + py * py + pz * pz;
+    const double rq2 = qx * qx + qy * qy + qz * qz;
+    const double w2 = rp2 * rq2;
+    const double u = idk * rcp_nr(sqrt_nr(w2) + 1e-3);
+    const double s = sqrt_nr(fmax(1.0 - u * u, 1e-30));
+    const double dth = atan2(s * c0 - u * s0, u * c0 + s * s0);
+    const double c1 = -rcp_nr(sqrt_nr(w2 - idk * idk + 1e-3));
+    const double f = -1000.0 * c1 * dth;
+    const double cp = idk * rcp_nr(rp2), cq = idk * rcp_nr(rq2);
+    Fp = make_double3(f * (qx - cp * px), f * (qy - cp * py), f * (qz - cp * pz));
+    Fq = make_double3(f * (px - cq * qx), f * (py - cq * qy), f * (pz - cq * qz));
+}
+
+// Shared per-CTA data of the contact sweep: candidate cells with their stale
+// boxes and stale insertion bin ranges, and the gathered halo.
 struct SlotData {
     int cell[MAXC];
     float4 lo[MAXC], hi[MAXC];
     int rlo[MAXC][3], rhi[MAXC][3];
-    int ncand;
     float mn[3];
     int div[3];
 };
 
-// Fill SlotData for cell a (threads 0..MAXC-1).  Must be followed by a
-// __syncthreads().
-__device__ __forceinline__ void load_slots(const Dev &d, int a, const InstParams &P, const InstState *st,
-                                           int par, SlotData &sd)
+struct Halo {
+    float4 x[HMAX];
+    float4 v[HMAX];
+    uint8_t s[HMAX];
+};
+
+// Phase A of a cell: candidate cells, stale grid, the halo's node ids (into
+// registers) and slots.  Independent loads only, so they overlap with the
+// caller's own-node loads; the caller then calls __syncthreads().
+constexpr int HREG = (HMAX + SLOTS - 1) / SLOTS;
+
+__device__ __forceinline__ void slots_phase_a(const Dev &d, int a, const InstState *st, int par, SlotData &sd,
+                                              Halo &hl, int nc, int nh, int (&hid)[HREG])
 {
     int t = threadIdx.x;
-    int nc = d.ncand[a];
+    if (t < MAXC) sd.cell[t] = t < nc ? d.cand[a * MAXC + t] : 0;
     if (t == 0) {
-        sd.ncand = nc;
         const int *mm = st->mm[par];
         for (int q = 0; q < 3; ++q) {
             float mn = fminf(o2f(mm[2 * q]), 1.0e8f);
@@ -97,10 +128,23 @@ __device__ __forceinline__ void load_slots(const Dev &d, int a, const InstParams
             sd.div[q] = grid_div(mn, mx);
         }
     }
-    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < HREG; ++q) {
+        const int h = t + q * SLOTS;
+        hid[q] = h < nh ? d.halo[(size_t)a * HMAX + h] : -1;
+        if (h < nh) hl.s[h] = d.halo_slot[(size_t)a * HMAX + h];
+    }
+}
+
+// Phase B: stale boxes / insertion ranges of the candidates and the halo
+// gather (positions from X, velocities from Vsrc).  Needs phase A to be
+// visible (__syncthreads() before), and a __syncthreads() after.
+__device__ __forceinline__ void slots_phase_b(const Dev &d, const InstParams &P, int par, SlotData &sd, Halo &hl,
+                                              int nc, const int (&hid)[HREG], const float4 *__restrict__ Vsrc)
+{
+    int t = threadIdx.x;
     if (t < nc) {
-        int c = d.cand[a * MAXC + t];
-        sd.cell[t] = c;
+        int c = sd.cell[t];
         float4 lo = d.aabb[par][2 * c], hi = d.aabb[par][2 * c + 1];
         sd.lo[t] = lo;
         sd.hi[t] = hi;
@@ -108,63 +152,107 @@ __device__ __forceinline__ void load_slots(const Dev &d, int a, const InstParams
         bin_range_axis(lo.y, hi.y, P.ra, sd.mn[1], sd.div[1], sd.rlo[t][1], sd.rhi[t][1]);
         bin_range_axis(lo.z, hi.z, P.ra, sd.mn[2], sd.div[2], sd.rlo[t][2], sd.rhi[t][2]);
     }
+#pragma unroll
+    for (int q = 0; q < HREG; ++q) {
+        if (hid[q] < 0) break;
+        hl.x[t + q * SLOTS] = __ldg(&d.X[hid[q]]);
+        hl.v[t + q * SLOTS] = __ldg(&Vsrc[hid[q]]);
+    }
 }
 
 // ---------------------------------------------------------------------------
-// Contact sweep of one node over its neighbour-list entries.
+// Contact sweep of one node over its neighbour-list entries (halo indices).
 // MODE 0: conservative + dissipative (S1); MODE 1: dissipative only (S2).
 // ---------------------------------------------------------------------------
 template <int MODE>
-__device__ __forceinline__ void contact_sweep(const Dev &d, const InstParams &P, const SlotData &sd,
-                                              int a, int i, float3 x, float3 v, float3 nrm,
-                                              const float4 *__restrict__ Vsrc, float3 &cf, float3 &vt)
+__device__ __forceinline__ void contact_sweep(const Dev &d, const InstParams &P, const SlotData &sd, const Halo &hl,
+                                              int a, int i, float3 x, float3 v, float3 nrm, double3 &cf, double3 &vt)
 {
-    int nb[3] = {node_bin_axis(x.x, sd.mn[0], sd.div[0]), node_bin_axis(x.y, sd.mn[1], sd.div[1]),
-                 node_bin_axis(x.z, sd.mn[2], sd.div[2])};
-    int ne = d.nent[a * SLOTS + i];
+    const int nb0 = node_bin_axis(x.x, sd.mn[0], sd.div[0]);
+    const int nb1 = node_bin_axis(x.y, sd.mn[1], sd.div[1]);
+    const int nb2 = node_bin_axis(x.z, sd.mn[2], sd.div[2]);
+    const int ne = d.nent[(size_t)a * SLOTS + i];
+    const uint16_t *ep = d.ent + (size_t)a * MAXE * SLOTS + i;
     int cur = -1;
     bool ok = false;
-    int c = 0;
-    for (int k = 0; k < ne; ++k) {
-        unsigned e = d.ent[((size_t)a * MAXE + k) * SLOTS + i];
-        int s = (int)(e >> 8), j = (int)(e & 255u);
-        if (s != cur) {
-            cur = s;
-            c = sd.cell[s];
-            ok = nb[0] >= sd.rlo[s][0] && nb[0] <= sd.rhi[s][0] && nb[1] >= sd.rlo[s][1] &&
-                 nb[1] <= sd.rhi[s][1] && nb[2] >= sd.rlo[s][2] && nb[2] <= sd.rhi[s][2] &&
-                 aabb_keep(sd.lo[s], sd.hi[s], x.x, x.y, x.z, P.ra2);
-        }
-        if (!ok) continue;
-        size_t gj = (size_t)c * SLOTS + j;
-        float4 xj = __ldg(&d.X[gj]);
-        float dx = __fsub_rn(x.x, xj.x), dy = __fsub_rn(x.y, xj.y), dz = __fsub_rn(x.z, xj.z);
-        float r2 = r2_nc(dx, dy, dz);
-        if (r2 > P.ra2) continue;
-        // dissipative pair (non-strict cut-off, src/propagate.cu:641)
-        float4 vj = __ldg(&Vsrc[gj]);
-        float3 vij = make_float3(v.x - vj.x, v.y - vj.y, v.z - vj.z);
-        float dn = dot3(vij, nrm);
-        vt.x += vij.x - dn * nrm.x;
-        vt.y += vij.y - dn * nrm.y;
-        vt.z += vij.z - dn * nrm.z;
-        if (MODE == 0) {
-            if (d.record_pairs) {
-                unsigned long long slot = atomicAdd(d.n_pairs, 1ull);
-                if ((long long)slot < d.pair_cap)
-                    d.pairs[slot] = make_int4((a << 8) | i, (c << 8) | j, r2 < P.ra2 ? 3 : 2, 0);
+    for (int k0 = 0; k0 < ne; k0 += 4) {
+        int hh[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) hh[q] = (k0 + q < ne) ? (int)ep[(k0 + q) * SLOTS] : -1;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int h = hh[q];
+            if (h < 0) break;
+            const int s = hl.s[h];
+            if (s != cur) {
+                cur = s;
+                ok = nb0 >= sd.rlo[s][0] && nb0 <= sd.rhi[s][0] && nb1 >= sd.rlo[s][1] && nb1 <= sd.rhi[s][1] &&
+                     nb2 >= sd.rlo[s][2] && nb2 <= sd.rhi[s][2] &&
+                     aabb_keep(sd.lo[s], sd.hi[s], x.x, x.y, x.z, P.ra2);
             }
-            if (r2 < P.ra2) {  // conservative pair (strict cut-off, src/propagate.cu:421)
-                float R = sqrtf(r2);
-                float k = 0.0f;
-                if (R < P.ra) k += -P.asE * (P.ra - R) / R;
-                if (R <= P.rr) k += P.rsE * (P.rr - R) / R;
-                cf.x += k * dx;
-                cf.y += k * dy;
-                cf.z += k * dz;
+            if (!ok) continue;
+            const float4 xj = hl.x[h];
+            const float dx = __fsub_rn(x.x, xj.x), dy = __fsub_rn(x.y, xj.y), dz = __fsub_rn(x.z, xj.z);
+            const float r2 = r2_nc(dx, dy, dz);
+            if (r2 > P.ra2) continue;
+            // dissipative pair (non-strict cut-off, src/propagate.cu:641);
+            // velocity differences of floats are exact in FP64
+            const float4 vj = hl.v[h];
+            const double vx = (double)v.x - vj.x, vy = (double)v.y - vj.y, vz = (double)v.z - vj.z;
+            const double dn = vx * nrm.x + vy * nrm.y + vz * nrm.z;
+            vt.x += vx - dn * nrm.x;
+            vt.y += vy - dn * nrm.y;
+            vt.z += vz - dn * nrm.z;
+            if (MODE == 0) {
+                if (d.record_pairs) {
+                    unsigned long long slot = atomicAdd(d.n_pairs, 1ull);
+                    const int gj = d.halo[(size_t)a * HMAX + h];
+                    if ((long long)slot < d.pair_cap)
+                        d.pairs[slot] = make_int4((a << 8) | i, ((gj / SLOTS) << 8) | (gj % SLOTS), r2 < P.ra2 ? 3 : 2, 0);
+                }
+                if (r2 < P.ra2) {  // conservative pair (strict cut-off, src/propagate.cu:421)
+                    // distance in FP64: (rr - R) cancels for stiff repulsion
+                    const double R = sqrt_nr((double)dx * dx + (double)dy * dy + (double)dz * dz);
+                    const double iR = rcp_nr(R);
+                    double k = 0.0;
+                    if (R < (double)P.ra) k += -(double)P.asE * ((double)P.ra - R) * iR;
+                    if (R <= (double)P.rr) k += (double)P.rsE * ((double)P.rr - R) * iR;
+                    cf.x += k * dx;
+                    cf.y += k * dy;
+                    cf.z += k * dz;
+                }
             }
         }
     }
+}
+
+// Unit surface normal of node i for the tangential friction,
+// src/propagate.cu:558-572.
+__device__ __forceinline__ float3 node_normal(const float4 *xs, int n0, int n1, int n2, float sgn)
+{
+    float3 A = sub3(f3(xs[n1]), f3(xs[n0]));
+    float3 B = sub3(f3(xs[n2]), f3(xs[n0]));
+    float3 nrm = make_float3(A.y * B.z - A.z * B.y, A.z * B.x - A.x * B.z, A.x * B.y - A.y * B.x);
+    float nin = 1.0f / sqrtf(nrm.x * nrm.x + nrm.y * nrm.y + nrm.z * nrm.z);
+    return make_float3(sgn * (nin * nrm.x), sgn * (nin * nrm.y), sgn * (nin * nrm.z));
+}
+
+// Dissipative force, src/propagate.cu:546-658: bond damping with the three
+// neighbours, tangential friction sum vt, viscous drag.  FP64: the damping
+// term is a sum of velocity differences that can cancel.
+__device__ __forceinline__ float3 dis_force(const InstParams &P, const float4 *vs, int n0, int n1, int n2, float3 v,
+                                           double3 vt)
+{
+    double dx = 0.0, dy = 0.0, dz = 0.0;
+    const int nbr[3] = {n0, n1, n2};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float4 vn = vs[nbr[k]];
+        dx += (double)v.x - vn.x; dy += (double)v.y - vn.y; dz += (double)v.z - vn.z;
+    }
+    const double gi = P.gint, ge = P.gext, go = P.go;
+    return make_float3((float)(-gi * dx - ge * vt.x - go * v.x), (float)(-gi * dy - ge * vt.y - go * v.y),
+                       (float)(-gi * dz - ge * vt.z - go * v.z));
 }
 
 // ---------------------------------------------------------------------------
@@ -173,11 +261,11 @@ __device__ __forceinline__ void contact_sweep(const Dev &d, const InstParams &P,
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(SLOTS) k_integrate(Dev d)
 {
-    const int W = *d.work_n;
+    const int W = n_work(d);
     __shared__ float smax[SLOTS / 32];
     for (int w = blockIdx.x; w < W; w += gridDim.x) {
-        int a = d.work[w];
-        int inst = d.cell_inst[a];
+        int a = cell_of(d, w);
+        int inst = inst_of(d, a);
         const InstParams &P = d.prm[inst];
         int i = threadIdx.x;
         float disp = 0.0f;
@@ -190,7 +278,9 @@ __global__ void __launch_bounds__(SLOTS) k_integrate(Dev d)
             v.y = kick(v.y, __fadd_rn(__fmul_rn(dt, fc.y), __fmul_rn(dt, fd.y)), m);
             v.z = kick(v.z, __fadd_rn(__fmul_rn(dt, fc.z), __fmul_rn(dt, fd.z)), m);
             float4 xn = make_float4(__fmaf_rn(v.x, dt, x.x), __fmaf_rn(v.y, dt, x.y), __fmaf_rn(v.z, dt, x.z), 0.0f);
-            float ddx = xn.x - x.x, ddy = xn.y - x.y, ddz = xn.z - x.z;
+            // displacement since the last neighbour-list build
+            const float4 xb = d.Xb[g];
+            float ddx = xn.x - xb.x, ddy = xn.y - xb.y, ddz = xn.z - xb.z;
             disp = sqrtf(ddx * ddx + ddy * ddy + ddz * ddz);
             d.X[g] = xn;
             d.V[g] = v;
@@ -221,15 +311,16 @@ __global__ void k_step_begin(Dev d, int par_next)
         InstState *st = &d.st[k];
         const InstParams &P = d.prm[k];
         st->step += 1;
+        // ds: the largest distance of any node from its position at the
+        // last build.  While 2*ds stays below the skin, every pair within
+        // the contact cut-off now was within the list radius then; the
+        // 1e-3 slack covers float rounding of the distances.
         float ds = __uint_as_float(st->disp_step);
         st->disp_step = 0u;
-        // every node moved at most ds this step, so no pair distance changed
-        // by more than 2*ds; a margin of 1e-3 covers float rounding
-        float acc = st->disp_acc + ds * 1.0001f + 1e-6f;
-        bool need = st->force_rebuild || 2.0f * acc + 1e-3f >= P.skin;
+        bool need = st->force_rebuild || !(2.0f * ds + 1e-3f < P.skin);
         st->rebuild = need ? 1 : 0;
         st->force_rebuild = 0;
-        st->disp_acc = need ? 0.0f : acc;
+        st->disp_acc = ds;
         st->div_count = 0;
         if (need) st->rebuilds += 1;
         for (int q = 0; q < 3; ++q) {
@@ -245,7 +336,7 @@ __global__ void k_step_begin(Dev d, int par_next)
     if (threadIdx.x == 0) { d.flags[0] = any; *d.n_pairs = 0ull; }
 }
 
-// Init variant: rebuild everything, reset parity-0 grid accumulators.
+// Init variant: rebuild everything, reset the grid accumulators.
 __global__ void k_init_begin(Dev d)
 {
     for (int k = threadIdx.x; k < d.n_inst; k += blockDim.x) {
@@ -317,8 +408,8 @@ __device__ __forceinline__ void cell_geom(const float4 *xs, GeomScratch &gs, flo
 }
 
 // Volume, area and the division test, src/volume.cu:5-163, in FP64.
-__device__ __forceinline__ void cell_volume(const Dev &d, const float4 *xs, float3 cm, GeomScratch &gs,
-                                            bool sph, double &vol, double &area)
+__device__ __noinline__ void cell_volume(const Dev &d, const float4 *xs, float3 cm, GeomScratch &gs, bool sph,
+                                         double &vol, double &area)
 {
     int t = threadIdx.x, w = t >> 5, l = t & 31;
     double tv = 0, fa = 0;
@@ -368,129 +459,130 @@ __device__ __forceinline__ void cell_volume(const Dev &d, const float4 *xs, floa
 struct S1Smem {
     float4 xs[SLOTS];
     float4 vs[SLOTS];
-    float armx[NARM], army[NARM], armz[NARM];
+    double armx[NARM], army[NARM], armz[NARM];
     SlotData sd;
+    Halo hl;
 };
 
 template <bool INIT>
 __global__ void __launch_bounds__(SLOTS) k_s1(Dev d, int par)
 {
-    __shared__ S1Smem sm;
-    const int W = *d.work_n;
+    extern __shared__ __align__(16) unsigned char s1_raw[];  // sizeof(S1Smem), > 48 KB
+    S1Smem &sm = *reinterpret_cast<S1Smem *>(s1_raw);
+    const int W = n_work(d);
     const int i = threadIdx.x;
     const uint32_t nnp = (i < NODES) ? __ldg(&d.topo.nnpack[i]) : 0u;
     const int n0 = nnp & 255, n1 = (nnp >> 8) & 255, n2 = (nnp >> 16) & 255;
     const float sgn = (float)(int8_t)(nnp >> 24);
     for (int w = blockIdx.x; w < W; w += gridDim.x) {
-        const int a = d.work[w];
-        const int inst = d.cell_inst[a];
+        const int a = cell_of(d, w);
+        const int inst = inst_of(d, a);
         const InstParams &P = d.prm[inst];
         const size_t g = (size_t)a * SLOTS + i;
+        const int nc = d.ncand[a];
+        const int nh = d.halo_n[a];
         float4 x4 = make_float4(0, 0, 0, 0), v4 = make_float4(0, 0, 0, 0);
         if (i < NODES) { x4 = d.X[g]; v4 = d.V[g]; }
         sm.xs[i] = x4;
         sm.vs[i] = v4;
-        load_slots(d, a, P, &d.st[inst], par, sm.sd);
+        int hid[HREG];
+        slots_phase_a(d, a, &d.st[inst], par, sm.sd, sm.hl, nc, nh, hid);
         __syncthreads();
+        slots_phase_b(d, P, par, sm.sd, sm.hl, nc, hid, d.V);
         const float3 x = f3(x4);
         const float3 v = f3(v4);
         // bond angles: thread = vertex, three angles each
         if (P.angles && i < NODES) {
             float3 pa = sub3(f3(sm.xs[n0]), x), pb = sub3(f3(sm.xs[n1]), x), pc = sub3(f3(sm.xs[n2]), x);
-            float4 th = __ldg(&d.topo.th0[i]);
-            float3 Fp, Fq;
-            angle_pair(pa, pb, th.x, Fp, Fq);
+            const double2 *cs0 = d.topo.cs0 + 3 * i;
+            double3 Fp, Fq;
             int o = i * 6;
+            double2 t0 = __ldg(&cs0[0]);
+            angle_pair(pa, pb, t0.x, t0.y, Fp, Fq);
             sm.armx[o] = Fp.x; sm.army[o] = Fp.y; sm.armz[o] = Fp.z;
             sm.armx[o + 1] = Fq.x; sm.army[o + 1] = Fq.y; sm.armz[o + 1] = Fq.z;
-            angle_pair(pb, pc, th.y, Fp, Fq);
+            t0 = __ldg(&cs0[1]);
+            angle_pair(pb, pc, t0.x, t0.y, Fp, Fq);
             sm.armx[o + 2] = Fp.x; sm.army[o + 2] = Fp.y; sm.armz[o + 2] = Fp.z;
             sm.armx[o + 3] = Fq.x; sm.army[o + 3] = Fq.y; sm.armz[o + 3] = Fq.z;
-            angle_pair(pa, pc, th.z, Fp, Fq);
+            t0 = __ldg(&cs0[2]);
+            angle_pair(pa, pc, t0.x, t0.y, Fp, Fq);
             sm.armx[o + 4] = Fp.x; sm.army[o + 4] = Fp.y; sm.armz[o + 4] = Fp.z;
             sm.armx[o + 5] = Fq.x; sm.army[o + 5] = Fq.y; sm.armz[o + 5] = Fq.z;
         }
         __syncthreads();
         if (i < NODES) {
             if (isnan(x.x) || isnan(x.y) || isnan(x.z)) atomic_or_err(&d.st[inst], CS3D_ERRBIT_NAN);
-            float FX = 0.f, FY = 0.f, FZ = 0.f;
+            // The node force is accumulated in FP64: its terms (pressure up
+            // to ~1e3, stiff contact repulsion up to ~1e4) can cancel to a
+            // net force orders of magnitude smaller, and the sum is rounded
+            // to float once, as the reference stores it.
+            double FX = 0.0, FY = 0.0, FZ = 0.0;
             // springs, src/propagate.cu:298-314
-            const float stiff = d.E[a];
+            const double stiff = d.E[a];
             const float4 r0 = __ldg(&d.topo.r0[i]);
             const int nbr[3] = {n0, n1, n2};
             const float r0v[3] = {r0.x, r0.y, r0.z};
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                float3 dd = sub3(f3(sm.xs[nbr[k]]), x);
-                float R = sqrtf(dd.x * dd.x + dd.y * dd.y + dd.z * dd.z);
-                float c = stiff * (R - r0v[k]) / r0v[k] / R;
+                const float3 dd = sub3(f3(sm.xs[nbr[k]]), x);
+                const double R = sqrt_nr((double)dd.x * dd.x + (double)dd.y * dd.y + (double)dd.z * dd.z);
+                const double c = stiff * (R - (double)r0v[k]) * rcp_nr((double)r0v[k] * R);
                 FX += c * dd.x; FY += c * dd.y; FZ += c * dd.z;
             }
             // internal pressure, src/propagate.cu:318-330 (CM of the previous step)
             {
-                float4 cm = d.CM[a];
-                float3 r = make_float3(x.x - cm.x, x.y - cm.y, x.z - cm.z);
-                float inv = 1.0f / sqrtf(r.x * r.x + r.y * r.y + r.z * r.z);
-                float pr = 3.0f * d.press[a];
-                FX += pr * (inv * r.x); FY += pr * (inv * r.y); FZ += pr * (inv * r.z);
+                const float4 cm = d.CM[a];
+                const float3 r = make_float3(x.x - cm.x, x.y - cm.y, x.z - cm.z);
+                const double c = 3.0 * (double)d.press[a] *
+                                 rcp_nr(sqrt_nr((double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z));
+                FX += c * r.x; FY += c * r.y; FZ += c * r.z;
             }
             // bond angles, src/propagate.cu:81-181 (vertex terms then arm terms)
             if (P.angles) {
-                float ax = 0.f, ay = 0.f, az = 0.f;
-                int o = i * 6;
+                double ax = 0.0, ay = 0.0, az = 0.0;
+                const int o = i * 6;
 #pragma unroll
                 for (int q = 0; q < 3; ++q) {
                     ax -= sm.armx[o + 2 * q] + sm.armx[o + 2 * q + 1];
                     ay -= sm.army[o + 2 * q] + sm.army[o + 2 * q + 1];
                     az -= sm.armz[o + 2 * q] + sm.armz[o + 2 * q + 1];
                 }
-                uint4 am = __ldg(&d.topo.arm[i]);
-                unsigned idx[6] = {am.x & 0xffffu, am.x >> 16, am.y & 0xffffu, am.y >> 16, am.z & 0xffffu, am.z >> 16};
+                const uint4 am = __ldg(&d.topo.arm[i]);
+                const unsigned idx[6] = {am.x & 0xffffu, am.x >> 16, am.y & 0xffffu, am.y >> 16, am.z & 0xffffu, am.z >> 16};
 #pragma unroll
                 for (int q = 0; q < 6; ++q) { ax += sm.armx[idx[q]]; ay += sm.army[idx[q]]; az += sm.armz[idx[q]]; }
                 FX += ax; FY += ay; FZ += az;
             }
-            // surface normal for the tangential friction, src/propagate.cu:558-572
-            float3 A = sub3(f3(sm.xs[n1]), f3(sm.xs[n0]));
-            float3 B = sub3(f3(sm.xs[n2]), f3(sm.xs[n0]));
-            float3 nrm = make_float3(A.y * B.z - A.z * B.y, A.z * B.x - A.x * B.z, A.x * B.y - A.y * B.x);
-            float nin = 1.0f / sqrtf(nrm.x * nrm.x + nrm.y * nrm.y + nrm.z * nrm.z);
-            nrm = make_float3(sgn * (nin * nrm.x), sgn * (nin * nrm.y), sgn * (nin * nrm.z));
-            // contacts
-            float3 cf = make_float3(0.f, 0.f, 0.f), vt = make_float3(0.f, 0.f, 0.f);
-            contact_sweep<0>(d, P, sm.sd, a, i, x, v, nrm, d.V, cf, vt);
+            const float3 nrm = node_normal(sm.xs, n0, n1, n2, sgn);
+            double3 cf = make_double3(0.0, 0.0, 0.0);
+            double3 vt = make_double3(0.0, 0.0, 0.0);
+            contact_sweep<0>(d, P, sm.sd, sm.hl, a, i, x, v, nrm, cf, vt);
             FX += cf.x; FY += cf.y; FZ += cf.z;
-            // rigid box walls, src/propagate.cu:474-510
+            // rigid box walls, src/propagate.cu:474-510 (float gap tests)
             if (P.rigid) {
+                const double wk = P.wallk, th = P.thresh;
                 float g1 = x.x, g2 = __fsub_rn(P.box[0], x.x);
-                if (g1 < P.thresh) FX += -P.wallk * (g1 - P.thresh);
-                if (g2 < P.thresh) FX += P.wallk * (g2 - P.thresh);
+                if (g1 < P.thresh) FX += -wk * ((double)g1 - th);
+                if (g2 < P.thresh) FX += wk * ((double)g2 - th);
                 g1 = x.y; g2 = __fsub_rn(P.box[1], x.y);
-                if (g1 < P.thresh) FY += -P.wallk * (g1 - P.thresh);
-                if (g2 < P.thresh) FY += P.wallk * (g2 - P.thresh);
+                if (g1 < P.thresh) FY += -wk * ((double)g1 - th);
+                if (g2 < P.thresh) FY += wk * ((double)g2 - th);
                 g1 = x.z; g2 = __fsub_rn(P.box[2], x.z);
-                if (g1 < P.thresh) FZ += -P.wallk * (g1 - P.thresh);
-                if (g2 < P.thresh) FZ += P.wallk * (g2 - P.thresh);
+                if (g1 < P.thresh) FZ += -wk * ((double)g1 - th);
+                if (g2 < P.thresh) FZ += wk * ((double)g2 - th);
             }
-            // dissipative force with v after Integrate
-            float3 dv = make_float3(0.f, 0.f, 0.f);
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                float4 vn = sm.vs[nbr[k]];
-                dv.x += v.x - vn.x; dv.y += v.y - vn.y; dv.z += v.z - vn.z;
-            }
-            float3 fd = make_float3(-P.gint * dv.x - P.gext * vt.x - P.go * v.x,
-                                    -P.gint * dv.y - P.gext * vt.y - P.go * v.y,
-                                    -P.gint * dv.z - P.gext * vt.z - P.go * v.z);
-            d.FC[g] = make_float4(FX, FY, FZ, 0.f);
+            const float3 fd = dis_force(P, sm.vs, n0, n1, n2, v, vt);
+            d.FC[g] = make_float4((float)FX, (float)FY, (float)FZ, 0.f);
             if (INIT) {
                 d.FD[g] = make_float4(fd.x, fd.y, fd.z, 0.f);
             } else {
                 const double m = P.mass;
                 const float dt = P.dt;
-                float vx = kick(v.x, __fmul_rn(dt, FX), m);
-                float vy = kick(v.y, __fmul_rn(dt, FY), m);
-                float vz = kick(v.z, __fmul_rn(dt, FZ), m);
+                // VelocityUpdateA reads the stored (float) conservative force
+                float vx = kick(v.x, __fmul_rn(dt, (float)FX), m);
+                float vy = kick(v.y, __fmul_rn(dt, (float)FY), m);
+                float vz = kick(v.z, __fmul_rn(dt, (float)FZ), m);
                 const double hdt = 0.5 * (double)dt;
                 vx = (float)((double)vx + hdt * (double)fd.x / m);
                 vy = (float)((double)vy + hdt * (double)fd.y / m);
@@ -505,80 +597,84 @@ __global__ void __launch_bounds__(SLOTS) k_s1(Dev d, int par)
 // ---------------------------------------------------------------------------
 // S2: second dissipative force with the updated velocities
 // (src/GPUbounce.cu:1151), centre of mass (:1164), volumes and division
-// flags (:1172), bounding boxes and grid extents for the next step (:1312-1334).
+// flags (:1172, DIV only), bounding boxes and grid extents for the next step
+// (:1312-1334).
 // ---------------------------------------------------------------------------
 struct S2Smem {
     float4 xs[SLOTS];
     float4 vs[SLOTS];
     SlotData sd;
+    Halo hl;
     GeomScratch gs;
 };
 
+__device__ __forceinline__ void flush_mm(Dev &d, int inst, int pn, const float *acc)
+{
+    int *mm = d.st[inst].mm[pn];
+    for (int q = 0; q < 3; ++q) {
+        atomicMin(&mm[2 * q], f2o(acc[2 * q]));
+        atomicMax(&mm[2 * q + 1], f2o(acc[2 * q + 1]));
+    }
+}
+
+template <bool DIV>
 __global__ void __launch_bounds__(SLOTS) k_s2(Dev d, int par)
 {
     __shared__ S2Smem sm;
-    const int W = *d.work_n;
+    const int W = n_work(d);
     const int i = threadIdx.x;
     const int pn = par ^ 1;
     const uint32_t nnp = (i < NODES) ? __ldg(&d.topo.nnpack[i]) : 0u;
     const int n0 = nnp & 255, n1 = (nnp >> 8) & 255, n2 = (nnp >> 16) & 255;
     const float sgn = (float)(int8_t)(nnp >> 24);
-    // per-CTA running grid extents (flushed when the instance changes)
     int acc_inst = -1;
     float acc[6];
     for (int w = blockIdx.x; w < W; w += gridDim.x) {
-        const int a = d.work[w];
-        const int inst = d.cell_inst[a];
+        const int a = cell_of(d, w);
+        const int inst = inst_of(d, a);
         const InstParams &P = d.prm[inst];
         InstState *st = &d.st[inst];
         const size_t g = (size_t)a * SLOTS + i;
+        const int nc = d.ncand[a];
+        const int nh = d.halo_n[a];
         float4 x4 = make_float4(0, 0, 0, 0), v4 = make_float4(0, 0, 0, 0);
         if (i < NODES) { x4 = d.X[g]; v4 = d.Vb[g]; }
         sm.xs[i] = x4;
         sm.vs[i] = v4;
-        load_slots(d, a, P, st, par, sm.sd);
+        int hid[HREG];
+        slots_phase_a(d, a, st, par, sm.sd, sm.hl, nc, nh, hid);
+        __syncthreads();
+        slots_phase_b(d, P, par, sm.sd, sm.hl, nc, hid, d.Vb);
         __syncthreads();
         const float3 x = f3(x4), v = f3(v4);
         if (i < NODES) {
-            float3 A = sub3(f3(sm.xs[n1]), f3(sm.xs[n0]));
-            float3 B = sub3(f3(sm.xs[n2]), f3(sm.xs[n0]));
-            float3 nrm = make_float3(A.y * B.z - A.z * B.y, A.z * B.x - A.x * B.z, A.x * B.y - A.y * B.x);
-            float nin = 1.0f / sqrtf(nrm.x * nrm.x + nrm.y * nrm.y + nrm.z * nrm.z);
-            nrm = make_float3(sgn * (nin * nrm.x), sgn * (nin * nrm.y), sgn * (nin * nrm.z));
-            float3 cf = make_float3(0.f, 0.f, 0.f), vt = make_float3(0.f, 0.f, 0.f);
-            contact_sweep<1>(d, P, sm.sd, a, i, x, v, nrm, d.Vb, cf, vt);
-            float3 dv = make_float3(0.f, 0.f, 0.f);
-            const int nbr[3] = {n0, n1, n2};
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                float4 vn = sm.vs[nbr[k]];
-                dv.x += v.x - vn.x; dv.y += v.y - vn.y; dv.z += v.z - vn.z;
-            }
-            float3 fd = make_float3(-P.gint * dv.x - P.gext * vt.x - P.go * v.x,
-                                    -P.gint * dv.y - P.gext * vt.y - P.go * v.y,
-                                    -P.gint * dv.z - P.gext * vt.z - P.go * v.z);
+            const float3 nrm = node_normal(sm.xs, n0, n1, n2, sgn);
+            double3 cf = make_double3(0.0, 0.0, 0.0);
+            double3 vt = make_double3(0.0, 0.0, 0.0);
+            contact_sweep<1>(d, P, sm.sd, sm.hl, a, i, x, v, nrm, cf, vt);
+            const float3 fd = dis_force(P, sm.vs, n0, n1, n2, v, vt);
             d.FD[g] = make_float4(fd.x, fd.y, fd.z, 0.f);
             d.V[g] = v4;
         }
-        // centre of mass and bounding box of the post-step positions
         float3 cm;
         float4 lo, hi;
         cell_geom(sm.xs, sm.gs, cm, lo, hi);
-        const bool divide_on = st->step <= P.div_steps && P.growth > 0.0f;
-        if (divide_on) {
-            double vol, area;
-            cell_volume(d, sm.xs, cm, sm.gs, P.check_sph != 0, vol, area);
-            if (i == 0) {
-                d.vol[a] = (float)vol;
-                if (!isfinite(vol)) { atomic_or_err(st, CS3D_ERRBIT_NONFINITE_VOL); vol = 1.0; }
-                int flag = vol > (double)P.divvol;
-                if (P.check_sph) {
-                    d.area[a] = (float)area;
-                    double cb = cbrt(vol);
-                    double psi = 4.835975862049408 * cb * cb / area;
-                    if (fabs(1.0 - psi) > 0.05) flag = 0;
+        if (DIV) {
+            if (st->step <= P.div_steps && P.growth > 0.0f) {
+                double vol, area;
+                cell_volume(d, sm.xs, cm, sm.gs, P.check_sph != 0, vol, area);
+                if (i == 0) {
+                    d.vol[a] = (float)vol;
+                    if (!isfinite(vol)) { atomic_or_err(st, CS3D_ERRBIT_NONFINITE_VOL); vol = 1.0; }
+                    int flag = vol > (double)P.divvol;
+                    if (P.check_sph) {
+                        d.area[a] = (float)area;
+                        double cb = cbrt(vol);
+                        double psi = 4.835975862049408 * cb * cb / area;
+                        if (fabs(1.0 - psi) > 0.05) flag = 0;
+                    }
+                    d.divflag[a] = (uint8_t)flag;
                 }
-                d.divflag[a] = (uint8_t)flag;
             }
         }
         if (i == 0) {
@@ -586,13 +682,7 @@ __global__ void __launch_bounds__(SLOTS) k_s2(Dev d, int par)
             d.aabb[pn][2 * a] = lo;
             d.aabb[pn][2 * a + 1] = hi;
             if (inst != acc_inst) {
-                if (acc_inst >= 0) {
-                    int *mm = d.st[acc_inst].mm[pn];
-                    for (int q = 0; q < 3; ++q) {
-                        atomicMin(&mm[2 * q], f2o(acc[2 * q]));
-                        atomicMax(&mm[2 * q + 1], f2o(acc[2 * q + 1]));
-                    }
-                }
+                if (acc_inst >= 0) flush_mm(d, acc_inst, pn, acc);
                 acc_inst = inst;
                 acc[0] = lo.x; acc[1] = hi.x; acc[2] = lo.y; acc[3] = hi.y; acc[4] = lo.z; acc[5] = hi.z;
             } else {
@@ -603,13 +693,7 @@ __global__ void __launch_bounds__(SLOTS) k_s2(Dev d, int par)
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0 && acc_inst >= 0) {
-        int *mm = d.st[acc_inst].mm[pn];
-        for (int q = 0; q < 3; ++q) {
-            atomicMin(&mm[2 * q], f2o(acc[2 * q]));
-            atomicMax(&mm[2 * q + 1], f2o(acc[2 * q + 1]));
-        }
-    }
+    if (threadIdx.x == 0 && acc_inst >= 0) flush_mm(d, acc_inst, pn, acc);
 }
 
 // Centre of mass, bounding boxes and grid extents only (initialisation,
@@ -618,11 +702,11 @@ __global__ void __launch_bounds__(SLOTS) k_geom(Dev d, int par)
 {
     __shared__ float4 xs[SLOTS];
     __shared__ GeomScratch gs;
-    const int W = *d.work_n;
+    const int W = n_work(d);
     const int i = threadIdx.x;
     for (int w = blockIdx.x; w < W; w += gridDim.x) {
-        const int a = d.work[w];
-        const int inst = d.cell_inst[a];
+        const int a = cell_of(d, w);
+        const int inst = inst_of(d, a);
         xs[i] = (i < NODES) ? d.X[(size_t)a * SLOTS + i] : make_float4(0, 0, 0, 0);
         __syncthreads();
         float3 cm;
@@ -691,16 +775,15 @@ __global__ void __launch_bounds__(256) k_div_select(Dev d, int par)
     const int n0 = st->n;
     if (threadIdx.x == 0) cnt = 0;
     __syncthreads();
-    // count dividers
     int mine = 0;
     for (int c = threadIdx.x; c < n0; c += blockDim.x) mine += d.divflag[P.base + c] ? 1 : 0;
     mine = warp_sum(mine);
     if ((threadIdx.x & 31) == 0) atomicAdd(&cnt, mine);
     __syncthreads();
-    int total = cnt;
+    const int total = cnt;
     if (total == 0) return;
-    int room = P.cap - n0;
-    int ndiv = total < room ? total : room;
+    const int room = P.cap - n0;
+    const int ndiv = total < room ? total : room;
     if (threadIdx.x == 0) {
         if (total > room) atomicOr(&st->err, CS3D_ERRBIT_CAPACITY);
         base_slot = atomicAdd(d.div_total, ndiv);
@@ -732,7 +815,7 @@ __global__ void __launch_bounds__(256) k_div_select(Dev d, int par)
         done += tot;
         __syncthreads();
     }
-    // normals in ascending order (serial RNG stream)
+    // normals in ascending order (one serial RNG stream per instance)
     if (threadIdx.x == 0) {
         int ev0 = atomicAdd(d.n_events, ndiv);
         for (int q = 0; q < ndiv; ++q) {
@@ -743,9 +826,9 @@ __global__ void __launch_bounds__(256) k_div_select(Dev d, int par)
             float nn = sqrtf(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
             if (fabsf(nn - 1.0f) > 1e-3f) atomicOr(&st->err, CS3D_ERRBIT_BAD_NORMAL);
             if (ev0 + q < d.ev_cap) d.events[ev0 + q] = make_int4(k, st->step, e.parent - P.base, e.daughter - P.base);
+            if (!d.single) d.work[atomicAdd(d.work_n, 1)] = e.daughter;
         }
         st->n = n0 + ndiv;
-        // grid extents of this step are recomputed after the daughters exist
         for (int q = 0; q < 3; ++q) {
             st->mm[par ^ 1][2 * q] = f2o(1.0e30f);
             st->mm[par ^ 1][2 * q + 1] = f2o(-1.0e30f);
@@ -774,14 +857,21 @@ __global__ void __launch_bounds__(SLOTS) k_div_apply(Dev d, int par)
         if (i < NODES) {
             float4 x = d.X[(size_t)a * SLOTS + i];
             double px[3] = {x.x, x.y, x.z};
+            // separate roundings (no DFMA) so the result is bit-identical to
+            // the oracle's FP64 restatement of CalcAndUpdateDaughtPos
             for (int s = 0; s < 2; ++s) {
                 double sg = s == 0 ? 1.0 : -1.0;
                 double n[3] = {sg * e.n[0], sg * e.n[1], sg * e.n[2]};
-                double o[3] = {cm[0] + half * n[0], cm[1] + half * n[1], cm[2] + half * n[2]};
-                double y[3] = {px[0] - o[0], px[1] - o[1], px[2] - o[2]};
-                double dn = y[0] * n[0] + y[1] * n[1] + y[2] * n[2];
-                if (dn <= 0.0) { y[0] -= dn * n[0]; y[1] -= dn * n[1]; y[2] -= dn * n[2]; }
-                float4 r = make_float4((float)(y[0] + o[0]), (float)(y[1] + o[1]), (float)(y[2] + o[2]), 0.f);
+                double o[3], y[3];
+                for (int q = 0; q < 3; ++q) {
+                    o[q] = __dadd_rn(cm[q], __dmul_rn(half, n[q]));
+                    y[q] = __dsub_rn(px[q], o[q]);
+                }
+                double dn = __dadd_rn(__dadd_rn(__dmul_rn(y[0], n[0]), __dmul_rn(y[1], n[1])), __dmul_rn(y[2], n[2]));
+                if (dn <= 0.0)
+                    for (int q = 0; q < 3; ++q) y[q] = __dsub_rn(y[q], __dmul_rn(dn, n[q]));
+                float4 r = make_float4((float)__dadd_rn(y[0], o[0]), (float)__dadd_rn(y[1], o[1]),
+                                       (float)__dadd_rn(y[2], o[2]), 0.f);
                 if (s == 0) xa = r; else xb = r;
             }
         }
@@ -803,8 +893,6 @@ __global__ void __launch_bounds__(SLOTS) k_div_apply(Dev d, int par)
             d.press[b] = P.minp;
             d.E[b] = P.daught_same ? d.E[a] : P.stiff1;
             d.cell_inst[b] = e.inst;
-            int wslot = atomicAdd(d.work_n, 1);
-            d.work[wslot] = b;
         }
         if (i < NODES) {
             size_t ga = (size_t)a * SLOTS + i, gb = (size_t)b * SLOTS + i;
@@ -822,10 +910,10 @@ __global__ void __launch_bounds__(SLOTS) k_div_apply(Dev d, int par)
 __global__ void k_grid_fix(Dev d, int par)
 {
     const int pn = par ^ 1;
-    const int W = *d.work_n;
+    const int W = n_work(d);
     for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < W; w += gridDim.x * blockDim.x) {
-        int a = d.work[w];
-        int inst = d.cell_inst[a];
+        int a = cell_of(d, w);
+        int inst = inst_of(d, a);
         if (d.st[inst].div_count == 0) continue;
         float4 lo = d.aabb[pn][2 * a], hi = d.aabb[pn][2 * a + 1];
         int *mm = d.st[inst].mm[pn];
@@ -836,19 +924,19 @@ __global__ void k_grid_fix(Dev d, int par)
 }
 
 // ---------------------------------------------------------------------------
-// Neighbour-list build (only when an instance's displacement bound reaches
-// the skin, or after a division).  R1: current boxes and build extents.
+// Neighbour-list build (only for instances whose displacement bound reached
+// the skin, or that divided).  R1: current boxes and build extents.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(SLOTS) k_nl_boxes(Dev d)
 {
     if (!d.flags[0]) return;
     __shared__ float4 xs[SLOTS];
     __shared__ GeomScratch gs;
-    const int W = *d.work_n;
+    const int W = n_work(d);
     const int i = threadIdx.x;
     for (int w = blockIdx.x; w < W; w += gridDim.x) {
-        const int a = d.work[w];
-        const int inst = d.cell_inst[a];
+        const int a = cell_of(d, w);
+        const int inst = inst_of(d, a);
         if (!d.st[inst].rebuild) continue;  // uniform across the block
         xs[i] = (i < NODES) ? d.X[(size_t)a * SLOTS + i] : make_float4(0, 0, 0, 0);
         __syncthreads();
@@ -869,7 +957,7 @@ __global__ void __launch_bounds__(SLOTS) k_nl_boxes(Dev d)
     }
 }
 
-// R2: build-grid geometry per instance and global bin offsets (one block).
+// R2: build-grid geometry per instance and global bin offsets (one thread).
 __global__ void k_nl_grid(Dev d)
 {
     if (!d.flags[0]) return;
@@ -889,6 +977,7 @@ __global__ void k_nl_grid(Dev d)
         for (int q = 0; q < 3; ++q) {
             float mn = o2f(st->bmm[2 * q]), mx = o2f(st->bmm[2 * q + 1]);
             int dim = (int)((mx - mn) / h) + 1;
+            if (dim < 1) dim = 1;
             st->bdim[q] = dim;
             st->borg[q] = mn;
             nb *= dim;
@@ -928,10 +1017,10 @@ __device__ __forceinline__ int build_bin(const InstState *st, float4 lo, float4 
 __global__ void k_nl_count(Dev d)
 {
     if (!d.flags[0]) return;
-    const int W = *d.work_n;
+    const int W = n_work(d);
     for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < W; w += gridDim.x * blockDim.x) {
-        int a = d.work[w];
-        const InstState *st = &d.st[d.cell_inst[a]];
+        int a = cell_of(d, w);
+        const InstState *st = &d.st[inst_of(d, a)];
         if (!st->rebuild) continue;
         int b3[3];
         int bin = build_bin(st, d.aabb_cur[2 * a], d.aabb_cur[2 * a + 1], b3);
@@ -981,36 +1070,63 @@ __global__ void __launch_bounds__(1024) k_nl_scan(Dev d)
 __global__ void k_nl_fill(Dev d)
 {
     if (!d.flags[0]) return;
-    const int W = *d.work_n;
+    const int W = n_work(d);
     for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < W; w += gridDim.x * blockDim.x) {
-        int a = d.work[w];
-        if (!d.st[d.cell_inst[a]].rebuild) continue;
+        int a = cell_of(d, w);
+        if (!d.st[inst_of(d, a)].rebuild) continue;
         d.bin_cells[d.bin_start[d.cell_bin[a]] + d.cell_rank[a]] = a;
     }
 }
 
-// R7: contact-candidate cells of each cell (boxes within rlist) and the
-// per-node candidate lists (nodes within rlist), deterministic order.
+// Block-wide ordered compaction of flags (192 threads): returns the rank of
+// this thread's element among the set flags and the total.
+__device__ __forceinline__ int block_rank(int flag, int *wcnt, int &total)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    unsigned b = __ballot_sync(0xffffffffu, flag);
+    if (lane == 0) wcnt[wid] = __popc(b);
+    __syncthreads();
+    int off = 0, tot = 0;
+    for (int q = 0; q < SLOTS / 32; ++q) {
+        if (q < wid) off += wcnt[q];
+        tot += wcnt[q];
+    }
+    total = tot;
+    return off + __popc(b & ((1u << lane) - 1u));
+}
+
+// R7: per cell, the candidate cells (boxes within rlist, ascending id), the
+// halo (nodes of candidate cells within rlist of some node of the cell,
+// ordered by slot then node) and each node's halo indices (ascending).
+struct BuildSmem {
+    float4 xs[SLOTS];
+    float4 cs[SLOTS];
+    int cand[MAXC];
+    float4 clo[MAXC], chi[MAXC];
+    uint8_t near[SLOTS];     // compacted nodes of the candidate near the cell
+    uint8_t mark[SLOTS];
+    uint16_t hmap[SLOTS];
+    int wcnt[SLOTS / 32];
+    int ncand;
+};
+
 __global__ void __launch_bounds__(SLOTS) k_nl_build(Dev d)
 {
     if (!d.flags[0]) return;
-    __shared__ float4 xs[SLOTS];
-    __shared__ float4 cs[SLOTS];
-    __shared__ int cand[MAXC];
-    __shared__ float4 clo[MAXC], chi[MAXC];
-    __shared__ int ncand;
-    const int W = *d.work_n;
+    __shared__ BuildSmem sm;
+    const int W = n_work(d);
     const int i = threadIdx.x;
     for (int w = blockIdx.x; w < W; w += gridDim.x) {
-        const int a = d.work[w];
-        const int inst = d.cell_inst[a];
+        const int a = cell_of(d, w);
+        const int inst = inst_of(d, a);
         InstState *st = &d.st[inst];
-        if (!st->rebuild) continue;
+        if (!st->rebuild) continue;  // uniform across the block
         const InstParams &P = d.prm[inst];
         const float rl = P.rlist + 1e-4f;
         const float rl2 = rl * rl;
-        if (i == 0) ncand = 0;
-        xs[i] = (i < NODES) ? d.X[(size_t)a * SLOTS + i] : make_float4(0, 0, 0, 0);
+        if (i == 0) sm.ncand = 0;
+        sm.xs[i] = (i < NODES) ? d.X[(size_t)a * SLOTS + i] : make_float4(0, 0, 0, 0);
+        sm.mark[i] = 0;
         __syncthreads();
         const float4 alo = d.aabb_cur[2 * a], ahi = d.aabb_cur[2 * a + 1];
         if (i < 27) {
@@ -1027,62 +1143,100 @@ __global__ void __launch_bounds__(SLOTS) k_nl_build(Dev d)
                     float gy = fmaxf(0.f, fmaxf(lo.y - ahi.y, alo.y - hi.y));
                     float gz = fmaxf(0.f, fmaxf(lo.z - ahi.z, alo.z - hi.z));
                     if (gx * gx + gy * gy + gz * gz >= rl2) continue;
-                    int s = atomicAdd(&ncand, 1);
-                    if (s < MAXC) cand[s] = c;
+                    int s = atomicAdd(&sm.ncand, 1);
+                    if (s < MAXC) sm.cand[s] = c;
                 }
             }
         }
         __syncthreads();
-        int nc = ncand;
+        int nc = sm.ncand;
         if (nc > MAXC) {
             if (i == 0) atomicOr(&st->err, CS3D_ERRBIT_CAND_OVERFLOW);
             nc = MAXC;
         }
         if (i == 0) {
-            // ascending cell order (insertion sort, nc <= 32)
-            for (int p = 1; p < nc; ++p) {
-                int v = cand[p], q = p - 1;
-                while (q >= 0 && cand[q] > v) { cand[q + 1] = cand[q]; --q; }
-                cand[q + 1] = v;
+            for (int p = 1; p < nc; ++p) {  // ascending cell order, nc <= 32
+                int v = sm.cand[p], q = p - 1;
+                while (q >= 0 && sm.cand[q] > v) { sm.cand[q + 1] = sm.cand[q]; --q; }
+                sm.cand[q + 1] = v;
             }
             d.ncand[a] = nc;
-            atomicMax(&st->max_cand, ncand);
+            atomicMax(&st->max_cand, sm.ncand);
         }
         __syncthreads();
         if (i < nc) {
-            d.cand[a * MAXC + i] = cand[i];
-            clo[i] = d.aabb_cur[2 * cand[i]];
-            chi[i] = d.aabb_cur[2 * cand[i] + 1];
+            d.cand[a * MAXC + i] = sm.cand[i];
+            sm.clo[i] = d.aabb_cur[2 * sm.cand[i]];
+            sm.chi[i] = d.aabb_cur[2 * sm.cand[i] + 1];
         }
         __syncthreads();
-        const float3 x = f3(xs[i]);
-        int cnt = 0;
+        const float3 x = f3(sm.xs[i]);
+        uint16_t *ep = d.ent + (size_t)a * MAXE * SLOTS + i;
+        int cnt = 0, hbase = 0;
+        bool hover = false;
         for (int s = 0; s < nc; ++s) {
-            const int c = cand[s];
-            cs[i] = (i < NODES) ? d.X[(size_t)c * SLOTS + i] : make_float4(0, 0, 0, 0);
+            const int c = sm.cand[s];
+            const float4 y4 = (i < NODES) ? d.X[(size_t)c * SLOTS + i] : make_float4(0, 0, 0, 0);
+            sm.cs[i] = y4;
+            // nodes of c within rlist of this cell's box, in ascending order
+            float gx = fmaxf(0.f, fmaxf(alo.x - y4.x, y4.x - ahi.x));
+            float gy = fmaxf(0.f, fmaxf(alo.y - y4.y, y4.y - ahi.y));
+            float gz = fmaxf(0.f, fmaxf(alo.z - y4.z, y4.z - ahi.z));
+            int fl = (i < NODES) && (gx * gx + gy * gy + gz * gz < rl2);
+            int nnear;
+            int r = block_rank(fl, sm.wcnt, nnear);
+            if (fl) sm.near[r] = (uint8_t)i;
             __syncthreads();
+            const int k_first = cnt;
             if (i < NODES) {
-                float4 lo = clo[s], hi = chi[s];
-                float gx = fmaxf(0.f, fmaxf(lo.x - x.x, x.x - hi.x));
-                float gy = fmaxf(0.f, fmaxf(lo.y - x.y, x.y - hi.y));
-                float gz = fmaxf(0.f, fmaxf(lo.z - x.z, x.z - hi.z));
-                if (gx * gx + gy * gy + gz * gz < rl2) {
-                    for (int j = 0; j < NODES; ++j) {
-                        float4 y = cs[j];
-                        float dx = x.x - y.x, dy = x.y - y.y, dz = x.z - y.z;
+                const float4 lo = sm.clo[s], hi = sm.chi[s];
+                float hx = fmaxf(0.f, fmaxf(lo.x - x.x, x.x - hi.x));
+                float hy = fmaxf(0.f, fmaxf(lo.y - x.y, x.y - hi.y));
+                float hz = fmaxf(0.f, fmaxf(lo.z - x.z, x.z - hi.z));
+                if (hx * hx + hy * hy + hz * hz < rl2) {
+                    for (int q = 0; q < nnear; ++q) {
+                        const int j = sm.near[q];
+                        const float4 yj = sm.cs[j];
+                        const float dx = x.x - yj.x, dy = x.y - yj.y, dz = x.z - yj.z;
                         if (dx * dx + dy * dy + dz * dz < rl2) {
-                            if (cnt < MAXE)
-                                d.ent[((size_t)a * MAXE + cnt) * SLOTS + i] = (uint16_t)((s << 8) | j);
+                            if (cnt < MAXE) ep[(size_t)cnt * SLOTS] = (uint16_t)j;
                             ++cnt;
+                            sm.mark[j] = 1;
                         }
                     }
                 }
             }
             __syncthreads();
+            // halo entries of this slot: marked nodes, ascending
+            const int mk = sm.mark[i];
+            int nmk;
+            const int hr = block_rank(mk, sm.wcnt, nmk);
+            if (mk) {
+                const int h = hbase + hr;
+                sm.hmap[i] = (uint16_t)h;
+                if (h < HMAX) {
+                    d.halo[(size_t)a * HMAX + h] = c * SLOTS + i;
+                    d.halo_slot[(size_t)a * HMAX + h] = (uint8_t)s;
+                }
+            }
+            __syncthreads();
+            for (int k = k_first; k < cnt && k < MAXE; ++k) ep[(size_t)k * SLOTS] = sm.hmap[ep[(size_t)k * SLOTS]];
+            hbase += nmk;
+            if (hbase > HMAX) hover = true;
+            sm.mark[i] = 0;
+            __syncthreads();
         }
         if (i < NODES) {
-            if (cnt > MAXE) { atomicOr(&st->err, CS3D_ERRBIT_ENTRY_OVERFLOW); }
-            d.nent[(size_t)a * SLOTS + i] = (uint8_t)(cnt < MAXE ? cnt : MAXE);
+            if (cnt > MAXE) atomicOr(&st->err, CS3D_ERRBIT_ENTRY_OVERFLOW);
+            // a halo overflow leaves the cell without contacts (and the error
+            // bit set): its entries would index past the shared halo
+            d.nent[(size_t)a * SLOTS + i] = hover ? (uint8_t)0 : (uint8_t)(cnt < MAXE ? cnt : MAXE);
+            d.Xb[(size_t)a * SLOTS + i] = sm.xs[i];  // reference for the displacement test
+        }
+        if (i == 0) {
+            if (hover) atomicOr(&st->err, CS3D_ERRBIT_HALO_OVERFLOW);
+            d.halo_n[a] = hbase < HMAX ? hbase : HMAX;
+            atomicMax(&st->max_halo, hbase);
         }
         int wm = cnt;
         for (int o = 16; o > 0; o >>= 1) wm = max(wm, __shfl_xor_sync(0xffffffffu, wm, o));

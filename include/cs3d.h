@@ -47,9 +47,11 @@ extern "C" {
 #define CS3D_ERRBIT_BAD_NORMAL     0x020u  /* |n| != 1, src/postscriptinit.cu:215-219 */
 #define CS3D_ERRBIT_GRID_OVERFLOW  0x040u  /* rebuild grid larger than its buffer */
 #define CS3D_ERRBIT_PAIR_OVERFLOW  0x080u  /* pair-recording buffer full */
+#define CS3D_ERRBIT_HALO_OVERFLOW  0x100u  /* > CS3D_MAX_HALO contact nodes for one cell */
 
-#define CS3D_MAX_CAND      32   /* contact-candidate cells per cell */
-#define CS3D_MAX_ENTRIES   48   /* contact-candidate nodes per node */
+#define CS3D_MAX_CAND      64   /* contact-candidate cells per cell */
+#define CS3D_MAX_ENTRIES   32   /* contact-candidate nodes per node */
+#define CS3D_MAX_HALO     512   /* distinct contact-candidate nodes per cell */
 
 /* ---- parameters of the hot path (one simulation instance) ------------- */
 /* Field meaning and units are the reference's inp.json keys.              */
@@ -221,6 +223,8 @@ int cs3d_load_state(cs3d_ctx *ctx, int inst, int n_cells, const float *X, const 
 /* Replace the RANMAR state of instance inst (e.g. after host-side draws
  * for random placement). */
 int cs3d_set_rng(cs3d_ctx *ctx, int inst, const cs3d_rng *rng);
+/* Current RANMAR state of instance inst (the stream the divisions draw from). */
+int cs3d_get_rng(cs3d_ctx *ctx, int inst, cs3d_rng *rng);
 
 /* Advance every instance by n_steps timesteps of src/GPUbounce.cu:1055-1338.
  * Returns CS3D_E_DEVICE_FLAGS or CS3D_E_CAPACITY if a kernel raised an
@@ -265,7 +269,8 @@ int cs3d_get_events(cs3d_ctx *ctx, int inst, int32_t *out, int max_events, int *
 int cs3d_last_error(cs3d_ctx *ctx, int inst, uint32_t *bits);
 
 /* Counters: [0] steps, [1] neighbour-list rebuilds, [2] max entries per node
- * seen, [3] max candidate cells per cell seen, [4] kernel launches per step. */
+ * seen, [3] max candidate cells per cell seen, [4] kernel launches per step,
+ * [5] max halo nodes per cell seen. */
 int cs3d_get_stats(cs3d_ctx *ctx, long long *stats, int n);
 
 /* Profiling pass: n_steps steps launched kernel by kernel (not as a graph)

@@ -242,6 +242,22 @@ class System:
         self.FD[:] = 0
         self._n[0] = n
 
+    def set_step(self, step):
+        self._step[0] = int(step)
+
+    def load_forces(self, FCX, FCY, FCZ, FDX, FDY, FDZ):
+        """Forces of the previous evaluation (float arrays from the CUDA path)."""
+        n = len(FCX)
+        for q, a in enumerate((FCX, FCY, FCZ)):
+            self.FC[q, :n] = a
+        for q, a in enumerate((FDX, FDY, FDZ)):
+            self.FD[q, :n] = a
+
+    def load_cm(self, cm):
+        """Per-cell centres of mass (n, 3) as the stale values of the next step."""
+        n = len(cm)
+        self.CM[:, :n] = np.asarray(cm, dtype=np.float32).T
+
     def seed(self, ij, kl):
         if lib().orc_rmarin(lib().orc_rng(self.h), ij, kl) != 0:
             raise ValueError("seed out of range")
@@ -290,3 +306,24 @@ class System:
 
     def compute_cm(self):
         lib().orc_center_of_mass(self.h)
+
+
+def _attach_force_methods():
+    def con_force(self):
+        """Conservative force at the current state with the current grid."""
+        lib().orc_con_force(self.h)
+
+    def dis_force(self):
+        """Dissipative force at the current state with the current grid."""
+        lib().orc_dis_force(self.h)
+
+    def set_rng_from(self, rng_struct):
+        """RANMAR state from a cs3d_rng-layout ctypes structure."""
+        C.memmove(lib().orc_rng(self.h), C.byref(rng_struct), C.sizeof(OrcRanmar))
+
+    System.con_force = con_force
+    System.dis_force = dis_force
+    System.set_rng_from = set_rng_from
+
+
+_attach_force_methods()

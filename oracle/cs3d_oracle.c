@@ -266,6 +266,7 @@ int *orc_ptr_i(orc_sys *s, int which)
     case 0: return &s->n; case 1: return &s->step; case 2: return &s->xdiv;
     case 3: return &s->nev; case 4: return s->ev;
     case 5: return &s->max_bin_count; case 6: return &s->max_local_nn;
+    case 7: return &s->ydiv; case 8: return &s->zdiv;
     default: return NULL;
     }
 }
@@ -275,11 +276,33 @@ orc_ranmar *orc_rng(orc_sys *s) { return &s->rng; }
 /* ------------------------------------------------------------------------ */
 /* Centre of mass, src/centermass.cu:8-50.  FP64 sum, stored float.          */
 /* ------------------------------------------------------------------------ */
+/* FP64 sum of the 180 node values in a fixed association order: six groups
+ * of 32 slots (slots 180..191 are zero), each reduced pairwise
+ * (w[l] + w[l ^ o] for o = 16, 8, 4, 2, 1), then the six group sums added in
+ * order.  This is the order of the CUDA path's warp reduction, so both give
+ * the same double before rounding to float. */
+static double sum192(const float *v)
+{
+    double tot = 0.0;
+    for (int g = 0; g < 6; ++g) {
+        double w[32];
+        for (int l = 0; l < 32; ++l) {
+            int i = 32 * g + l;
+            w[l] = i < 180 ? (double)v[i] : 0.0;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            double t[32];
+            for (int l = 0; l < 32; ++l) t[l] = w[l] + w[l ^ o];
+            for (int l = 0; l < 32; ++l) w[l] = t[l];
+        }
+        tot += w[0];
+    }
+    return tot;
+}
+
 static void cm_cell(orc_sys *s, int c)
 {
-    double sx = 0, sy = 0, sz = 0;
-    const float *X = s->X + c * 192, *Y = s->Y + c * 192, *Z = s->Z + c * 192;
-    for (int i = 0; i < 180; ++i) { sx += X[i]; sy += Y[i]; sz += Z[i]; }
+    double sx = sum192(s->X + c * 192), sy = sum192(s->Y + c * 192), sz = sum192(s->Z + c * 192);
     s->CM[c] = (float)(sx / 180.0);
     s->CM[s->cap + c] = (float)(sy / 180.0);
     s->CM[2 * s->cap + c] = (float)(sz / 180.0);
@@ -838,10 +861,15 @@ void orc_step(orc_sys *s)
 {
     const orc_params *P = &s->P;
     const int cap192 = s->cap * 192;
-    const double dt = P->dt, m = P->mass;
+    const double m = P->mass;
     int step = ++s->step;
     const int N = s->n;
-    /* Integrate + ForwardTime, src/propagate.cu:681-763 */
+    /* Integrate + ForwardTime, src/propagate.cu:681-763.  The reference keeps
+     * forces in float arrays between kernels and evaluates the kick as a float
+     * sum scaled in double ("0.5" is a double literal); the drift X + v*dt is
+     * one float multiply-add.  Transcribed exactly, so that from the same float
+     * state the oracle's positions after the drift are the reference's. */
+    const float dtf = P->dt;
     #pragma omp parallel for schedule(static)
     for (int c = 0; c < N; ++c)
         for (int i = 0; i < 180; ++i) {
@@ -849,9 +877,10 @@ void orc_step(orc_sys *s)
             float *V[3] = {s->VX, s->VY, s->VZ};
             float *X[3] = {s->X, s->Y, s->Z};
             for (int q = 0; q < 3; ++q) {
-                double v = (double)V[q][g] + 0.5 * (dt * s->FC[q * cap192 + g] + dt * s->FD[q * cap192 + g]) / m;
-                V[q][g] = (float)v;
-                X[q][g] = (float)((double)X[q][g] + (double)V[q][g] * dt);
+                float fc = (float)s->FC[q * cap192 + g], fd = (float)s->FD[q * cap192 + g];
+                float sum = dtf * fc + dtf * fd;
+                V[q][g] = (float)((double)V[q][g] + 0.5 * (double)sum / m);
+                X[q][g] = fmaf(V[q][g], dtf, X[q][g]);
             }
         }
     /* PressureUpdate, src/PressureKernels.cu:35-39 */
@@ -860,15 +889,16 @@ void orc_step(orc_sys *s)
     record_pairs(s);
     orc_con_force(s);
     orc_dis_force(s);
-    /* VelocityUpdateA/B, src/propagate.cu:714-736 */
+    /* VelocityUpdateA/B, src/propagate.cu:714-736 (float forces, double scale) */
     #pragma omp parallel for schedule(static)
     for (int c = 0; c < N; ++c)
         for (int i = 0; i < 180; ++i) {
             int g = c * 192 + i;
             float *V[3] = {s->VX, s->VY, s->VZ};
             for (int q = 0; q < 3; ++q) {
-                V[q][g] = (float)((double)V[q][g] + 0.5 * (dt * s->FC[q * cap192 + g]) / m);
-                V[q][g] = (float)((double)V[q][g] + 0.5 * dt * s->FD[q * cap192 + g] / m);
+                float fc = (float)s->FC[q * cap192 + g], fd = (float)s->FD[q * cap192 + g];
+                V[q][g] = (float)((double)V[q][g] + 0.5 * (double)(dtf * fc) / m);
+                V[q][g] = (float)((double)V[q][g] + 0.5 * (double)dtf * (double)fd / m);
             }
         }
     orc_dis_force(s);

@@ -1,7 +1,10 @@
-"""Shared helpers of the parity tests: set up one workload in the CUDA path
-(through the C ABI) and in the oracle from identical float32 inputs, and the
-error metrics of the parity bar (per node: |F - F_ref| / max(|F_ref|,
-1e-3 * median|F_ref|); global: ||dF||_2 / ||F_ref||_2)."""
+"""Shared helpers of the parity tests.
+
+The parity bar is checked on identical inputs: a single step of the CUDA
+path (through the C ABI) and of the FP64 oracle from the same float state,
+taken from the CUDA path itself.  Error metrics: per node
+|F - F_ref| / max(|F_ref|, 1e-3 * median|F_ref|) and globally
+||dF||_2 / ||F_ref||_2."""
 import numpy as np
 
 import cellsim3d_b200 as cs
@@ -21,6 +24,7 @@ def topo_for(st, mesh):
 
 
 def make_pair(p, st, mesh, capacity, record_pairs=True, pair_capacity=1 << 22):
+    """A Simulation and a tracking oracle started from the same initial state."""
     topo, otopo = topo_for(st, mesh)
     sim = cs.Simulation(p, topo, capacity)
     if record_pairs:
@@ -34,20 +38,28 @@ def make_pair(p, st, mesh, capacity, record_pairs=True, pair_capacity=1 << 22):
     orc.seed(p["rng_ij"], p["rng_kl"])
     orc.set_record(record_pairs)
     orc.init()
+    sim.otopo = otopo
+    sim.params = p
+    sim.capacity = capacity
     return sim, orc
 
 
-def node_mask(n):
+def node_mask(n, exclude_cells=()):
     m = np.zeros((n, 192), bool)
     m[:, :180] = True
+    for c in exclude_cells:
+        if c < n:
+            m[c] = False
     return m.reshape(-1)
 
 
-def rel_err(got, ref, n):
-    """(max per-node floor-relative error, global relative error)."""
-    msk = node_mask(n)
-    g = np.stack([a[: n * 192] for a in got], -1)[msk].astype(np.float64)
-    r = np.stack([a[: n * 192] for a in ref], -1)[msk].astype(np.float64)
+def rel_err(got, ref, n, exclude_cells=()):
+    """(max per-node floor-relative error, global relative error, p99)."""
+    msk = node_mask(n, exclude_cells)
+    g = np.stack([np.asarray(a)[: n * 192] for a in got], -1)[msk].astype(np.float64)
+    r = np.stack([np.asarray(a)[: n * 192] for a in ref], -1)[msk].astype(np.float64)
+    if len(r) == 0:
+        return 0.0, 0.0, 0.0
     nr = np.linalg.norm(r, axis=1)
     floor = max(1e-3 * float(np.median(nr)), 1e-30)
     e = np.linalg.norm(g - r, axis=1) / np.maximum(nr, floor)
@@ -55,12 +67,12 @@ def rel_err(got, ref, n):
     return float(e.max()), float(glob), float(np.percentile(e, 99))
 
 
-def force_errors(sim, orc):
+def force_errors(sim, orc, exclude_cells=()):
     n = sim.n_cells()
     f = sim.forces()
     FC, FD = orc.FC, orc.FD
-    ec = rel_err([f["FCX"], f["FCY"], f["FCZ"]], [FC[0], FC[1], FC[2]], n)
-    ed = rel_err([f["FDX"], f["FDY"], f["FDZ"]], [FD[0], FD[1], FD[2]], n)
+    ec = rel_err([f["FCX"], f["FCY"], f["FCZ"]], [FC[0], FC[1], FC[2]], n, exclude_cells)
+    ed = rel_err([f["FDX"], f["FDY"], f["FDZ"]], [FD[0], FD[1], FD[2]], n, exclude_cells)
     return ec, ed
 
 
@@ -70,3 +82,82 @@ def sorted_pairs(a):
         return a.reshape(0, 4)
     key = ((a[:, 0] * 256 + a[:, 1]) * (1 << 24) + a[:, 2]) * 256 + a[:, 3]
     return a[np.argsort(key, kind="stable")]
+
+
+def snapshot(sim):
+    st = sim.state()
+    st.update(sim.forces())
+    st["cm"] = sim.cells()["cm"]
+    st["rng"] = sim.get_rng()
+    st["step"] = sim.stats()["steps"]
+    return st
+
+
+def oracle_from(snap, p, otopo, capacity, record=True):
+    """An oracle holding the CUDA path's state after a step (float inputs)."""
+    O = oracle.System(capacity, p, otopo)
+    n = snap["n"]
+    O.load(snap["X"], snap["Y"], snap["Z"], snap["VX"], snap["VY"], snap["VZ"],
+           pressure=snap["pressure"], youngs=snap["youngs"], n=n)
+    O.load_forces(snap["FCX"], snap["FCY"], snap["FCZ"], snap["FDX"], snap["FDY"], snap["FDZ"])
+    O.load_cm(snap["cm"])
+    O.set_rng_from(snap["rng"].state)
+    O.set_step(snap["step"])
+    O.compute_grid()
+    O.set_record(record)
+    return O
+
+
+def single_step_check(sim, tag="", tol=TOL, check_pairs=True):
+    """Step the CUDA path once and the oracle once from the identical state;
+    returns a dict of the measured errors after asserting the parity bar."""
+    p, otopo, cap = sim.params, sim.otopo, sim.capacity
+    before = snapshot(sim)
+    O = oracle_from(before, p, otopo, cap, record=check_pairs)
+    sim.step(1)
+    O.step(1)
+    after = snapshot(sim)
+    n = after["n"]
+    res = {"tag": tag, "n": n}
+    # discrete results: cell count, division events of this step, pair sets
+    assert n == O.n, (tag, n, O.n)
+    ev_g = sim.events()
+    ev_g = ev_g[ev_g[:, 0] == after["step"]] if len(ev_g) else ev_g
+    ev_o = O.events()
+    assert np.array_equal(ev_g, ev_o), (tag, "division events", ev_g, ev_o)
+    divided = set(ev_g[:, 1].tolist()) | set(ev_g[:, 2].tolist()) if len(ev_g) else set()
+    if check_pairs:
+        for kind in (0, 1):
+            g = sorted_pairs(sim.pairs(kind))
+            r = sorted_pairs(O.recorded_pairs(kind))
+            assert g.shape == r.shape and np.array_equal(g, r), (tag, "pair set", kind, g.shape, r.shape)
+        res["pairs"] = (len(sorted_pairs(sim.pairs(0))), len(sorted_pairs(sim.pairs(1))))
+    # positions after the drift and the division geometry: bit-exact
+    k = n * 192
+    for a, b in (("X", O.X), ("Y", O.Y), ("Z", O.Z)):
+        assert np.array_equal(after[a][:k].view(np.uint32), b[:k].view(np.uint32)), (tag, "positions", a)
+    cm_o = O.CM[:, :n].T
+    ex = [c for c in range(n)]
+    # conservative force (identical inputs)
+    ec = rel_err([after["FCX"], after["FCY"], after["FCZ"]], [O.FC[0], O.FC[1], O.FC[2]], n)
+    # velocities after the step
+    ev = rel_err([after["VX"], after["VY"], after["VZ"]], [O.VX, O.VY, O.VZ], n)
+    # dissipative force on identical inputs: the CUDA path's own v3 and x,
+    # stale grid of the previous step (cells that divided this step excluded:
+    # their positions changed after the force evaluation)
+    O2 = oracle_from(before, p, otopo, cap, record=False)
+    O2.X[:k], O2.Y[:k], O2.Z[:k] = after["X"][:k], after["Y"][:k], after["Z"][:k]
+    O2.VX[:k], O2.VY[:k], O2.VZ[:k] = after["VX"][:k], after["VY"][:k], after["VZ"][:k]
+    O2._n[0] = n
+    O2.dis_force()
+    ed = rel_err([after["FDX"], after["FDY"], after["FDZ"]], [O2.FD[0], O2.FD[1], O2.FD[2]], n,
+                 exclude_cells=sorted(divided))
+    res.update(fc=ec, fd=ed, v=ev, cm_exact=bool(np.array_equal(after["cm"].view(np.uint32), cm_o.view(np.uint32))))
+    print("%-26s n=%5d Fc max %.2e glob %.2e | Fd max %.2e glob %.2e | V max %.2e glob %.2e"
+          % (tag, n, ec[0], ec[1], ed[0], ed[1], ev[0], ev[1]))
+    assert ec[0] < tol and ec[1] < tol, (tag, "Fc", ec)
+    assert ed[0] < tol and ed[1] < tol, (tag, "Fd", ed)
+    assert ev[0] < tol and ev[1] < tol, (tag, "V", ev)
+    O.close()
+    O2.close()
+    return res
