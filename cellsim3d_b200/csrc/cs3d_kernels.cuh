@@ -71,12 +71,23 @@ __device__ __forceinline__ double rcp_nr(double x)
 // same 1e-3 regularisers.  The force is proportional to theta - theta0, a
 // difference of two angles near 2 rad whose float rounding alone (1.2e-7)
 // would exceed the 1e-5 relative force bar, so it is formed without
-// rounding theta.  With u = cos(theta) (the reference's regularised ratio)
-// and s = sin(theta) = sqrt(1 - u^2) in FP64, and cos/sin of theta0 in FP64,
-//   theta - theta0 = atan2(s cos0 - u sin0, u cos0 + s sin0)
-// is a single well-conditioned FP64 arctangent instead of an arccosine of a
-// ratio followed by a cancelling subtraction.
-__device__ __forceinline__ void angle_pair(float3 P, float3 Q, double c0, double s0, double3 &Fp, double3 &Fq)
+// rounding theta.  u = cos(theta) (the reference's regularised ratio) is
+// formed in FP64; with c0, s0 = cos, sin of theta0 in FP64,
+//   sin(dth / 2) = (c0 - u) / (2 sin(theta0 + dth / 2)),   dth = theta - theta0.
+// A float estimate of dth from acosf is refined by one Newton step of this
+// equation in FP64 (sin/cos of dth/2 by their Taylor series, |dth/2| < 0.4
+// for |dth/2| up to ~1.2 rad), which leaves dth accurate to ~1e-13.
+__device__ __forceinline__ void sincos_small(double x, double &s, double &c)
+{
+    const double x2 = x * x;
+    s = x * (1.0 + x2 * (-1.0 / 6 + x2 * (1.0 / 120 + x2 * (-1.0 / 5040 + x2 * (1.0 / 362880 +
+            x2 * (-1.0 / 39916800 + x2 * (1.0 / 6227020800.0 - x2 / 1307674368000.0)))))));
+    c = 1.0 + x2 * (-0.5 + x2 * (1.0 / 24 + x2 * (-1.0 / 720 + x2 * (1.0 / 40320 + x2 * (-1.0 / 3628800 +
+            x2 * (1.0 / 479001600 + x2 * (-1.0 / 87178291200.0 + x2 / 20922789888000.0)))))));
+}
+
+__device__ __forceinline__ void angle_pair(float3 P, float3 Q, float th0f, double c0, double s0, double3 &Fp,
+                                           double3 &Fq)
 {
     const double px = P.x, py = P.y, pz = P.z, qx = Q.x, qy = Q.y, qz = Q.z;
     const double idk = px * qx + py * qy + pz * qz;
@@ -84,8 +95,15 @@ __device__ __forceinline__ void angle_pair(float3 P, float3 Q, double c0, double
     const double rq2 = qx * qx + qy * qy + qz * qz;
     const double w2 = rp2 * rq2;
     const double u = idk * rcp_nr(sqrt_nr(w2) + 1e-3);
-    const double s = sqrt_nr(fmax(1.0 - u * u, 1e-30));
-    const double dth = atan2(s * c0 - u * s0, u * c0 + s * s0);
+    // float estimate, then one Newton step on g(h) = sin(h) sin(theta0 + h) - (c0 - u)/2, h = dth/2
+    double h = 0.5 * (double)(acosf((float)u) - th0f);
+    double sh, ch;
+    sincos_small(h, sh, ch);
+    const double s1 = s0 * ch + c0 * sh, c1t = c0 * ch - s0 * sh;  // sin, cos of theta0 + h
+    const double g = sh * s1 - 0.5 * (c0 - u);
+    const double dg = ch * s1 + sh * c1t;                            // d/dh of sin(h) sin(theta0 + h)
+    h -= g * rcp_nr(dg);
+    const double dth = 2.0 * h;
     const double c1 = -rcp_nr(sqrt_nr(w2 - idk * idk + 1e-3));
     const double f = -1000.0 * c1 * dth;
     const double cp = idk * rcp_nr(rp2), cq = idk * rcp_nr(rq2);
@@ -118,7 +136,9 @@ __device__ __forceinline__ void slots_phase_a(const Dev &d, int a, const InstSta
                                               Halo &hl, int nc, int nh, int (&hid)[HREG])
 {
     int t = threadIdx.x;
-    if (t < MAXC) sd.cell[t] = t < nc ? d.cand[a * MAXC + t] : 0;
+    // the lists are read in full, whatever their counts, so that no load
+    // waits for another (entries past the counts are never used)
+    if (t < MAXC) sd.cell[t] = d.cand[a * MAXC + t];
     if (t == 0) {
         const int *mm = st->mm[par];
         for (int q = 0; q < 3; ++q) {
@@ -131,16 +151,21 @@ __device__ __forceinline__ void slots_phase_a(const Dev &d, int a, const InstSta
 #pragma unroll
     for (int q = 0; q < HREG; ++q) {
         const int h = t + q * SLOTS;
-        hid[q] = h < nh ? d.halo[(size_t)a * HMAX + h] : -1;
-        if (h < nh) hl.s[h] = d.halo_slot[(size_t)a * HMAX + h];
+        if (h < HMAX) {
+            const int id = d.halo[(size_t)a * HMAX + h];
+            const uint8_t sl = d.halo_slot[(size_t)a * HMAX + h];
+            hid[q] = h < nh ? id : -1;
+            hl.s[h] = sl;
+        } else {
+            hid[q] = -1;
+        }
     }
 }
 
-// Phase B: stale boxes / insertion ranges of the candidates and the halo
+// Phase B: stale boxes / insertion ranges of the candidates, then the halo
 // gather (positions from X, velocities from Vsrc).  Needs phase A to be
 // visible (__syncthreads() before), and a __syncthreads() after.
-__device__ __forceinline__ void slots_phase_b(const Dev &d, const InstParams &P, int par, SlotData &sd, Halo &hl,
-                                              int nc, const int (&hid)[HREG], const float4 *__restrict__ Vsrc)
+__device__ __forceinline__ void slots_boxes(const Dev &d, const InstParams &P, int par, SlotData &sd, int nc)
 {
     int t = threadIdx.x;
     if (t < nc) {
@@ -152,6 +177,12 @@ __device__ __forceinline__ void slots_phase_b(const Dev &d, const InstParams &P,
         bin_range_axis(lo.y, hi.y, P.ra, sd.mn[1], sd.div[1], sd.rlo[t][1], sd.rhi[t][1]);
         bin_range_axis(lo.z, hi.z, P.ra, sd.mn[2], sd.div[2], sd.rlo[t][2], sd.rhi[t][2]);
     }
+}
+
+__device__ __forceinline__ void halo_gather(const Dev &d, Halo &hl, const int (&hid)[HREG],
+                                            const float4 *__restrict__ Vsrc)
+{
+    const int t = threadIdx.x;
 #pragma unroll
     for (int q = 0; q < HREG; ++q) {
         if (hid[q] < 0) break;
@@ -166,19 +197,20 @@ __device__ __forceinline__ void slots_phase_b(const Dev &d, const InstParams &P,
 // ---------------------------------------------------------------------------
 template <int MODE>
 __device__ __forceinline__ void contact_sweep(const Dev &d, const InstParams &P, const SlotData &sd, const Halo &hl,
-                                              int a, int i, float3 x, float3 v, float3 nrm, double3 &cf, double3 &vt)
+                                              int a, int i, float3 x, float3 v, float3 nrm, int ne,
+                                              const int (&first)[4], double3 &cf, double3 &vt)
 {
     const int nb0 = node_bin_axis(x.x, sd.mn[0], sd.div[0]);
     const int nb1 = node_bin_axis(x.y, sd.mn[1], sd.div[1]);
     const int nb2 = node_bin_axis(x.z, sd.mn[2], sd.div[2]);
-    const int ne = d.nent[(size_t)a * SLOTS + i];
     const uint16_t *ep = d.ent + (size_t)a * MAXE * SLOTS + i;
     int cur = -1;
     bool ok = false;
     for (int k0 = 0; k0 < ne; k0 += 4) {
         int hh[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) hh[q] = (k0 + q < ne) ? (int)ep[(k0 + q) * SLOTS] : -1;
+        for (int q = 0; q < 4; ++q)
+            hh[q] = (k0 + q < ne) ? (k0 == 0 ? first[q] : (int)ep[(k0 + q) * SLOTS]) : -1;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int h = hh[q];
@@ -456,16 +488,25 @@ __device__ __noinline__ void cell_volume(const Dev &d, const float4 *xs, float3 
 // INIT = true evaluates the initial forces of src/GPUbounce.cu:978-1004
 // (no velocity update; Fd written to FD).
 // ---------------------------------------------------------------------------
+// The arm forces are consumed before the halo is gathered, so they share
+// the halo's position/velocity storage (its slot array stays separate).
+struct ArmForces {
+    double x[NARM], y[NARM], z[NARM];
+};
+static_assert(sizeof(ArmForces) <= 2 * sizeof(float4) * HMAX, "arm forces overlay the halo positions");
+
 struct S1Smem {
     float4 xs[SLOTS];
     float4 vs[SLOTS];
-    double armx[NARM], army[NARM], armz[NARM];
     SlotData sd;
-    Halo hl;
+    union {
+        Halo hl;
+        ArmForces arm;
+    };
 };
 
 template <bool INIT>
-__global__ void __launch_bounds__(SLOTS) k_s1(Dev d, int par)
+__global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
 {
     extern __shared__ __align__(16) unsigned char s1_raw[];  // sizeof(S1Smem), > 48 KB
     S1Smem &sm = *reinterpret_cast<S1Smem *>(s1_raw);
@@ -483,41 +524,46 @@ __global__ void __launch_bounds__(SLOTS) k_s1(Dev d, int par)
         const int nh = d.halo_n[a];
         float4 x4 = make_float4(0, 0, 0, 0), v4 = make_float4(0, 0, 0, 0);
         if (i < NODES) { x4 = d.X[g]; v4 = d.V[g]; }
+        const int ne = d.nent[g];
+        int first[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) first[q] = d.ent[((size_t)a * MAXE + q) * SLOTS + i];
         sm.xs[i] = x4;
         sm.vs[i] = v4;
         int hid[HREG];
         slots_phase_a(d, a, &d.st[inst], par, sm.sd, sm.hl, nc, nh, hid);
         __syncthreads();
-        slots_phase_b(d, P, par, sm.sd, sm.hl, nc, hid, d.V);
+        slots_boxes(d, P, par, sm.sd, nc);
         const float3 x = f3(x4);
         const float3 v = f3(v4);
         // bond angles: thread = vertex, three angles each
         if (P.angles && i < NODES) {
             float3 pa = sub3(f3(sm.xs[n0]), x), pb = sub3(f3(sm.xs[n1]), x), pc = sub3(f3(sm.xs[n2]), x);
             const double2 *cs0 = d.topo.cs0 + 3 * i;
+            const float4 th = __ldg(&d.topo.th0[i]);
             double3 Fp, Fq;
             int o = i * 6;
             double2 t0 = __ldg(&cs0[0]);
-            angle_pair(pa, pb, t0.x, t0.y, Fp, Fq);
-            sm.armx[o] = Fp.x; sm.army[o] = Fp.y; sm.armz[o] = Fp.z;
-            sm.armx[o + 1] = Fq.x; sm.army[o + 1] = Fq.y; sm.armz[o + 1] = Fq.z;
+            angle_pair(pa, pb, th.x, t0.x, t0.y, Fp, Fq);
+            sm.arm.x[o] = Fp.x; sm.arm.y[o] = Fp.y; sm.arm.z[o] = Fp.z;
+            sm.arm.x[o + 1] = Fq.x; sm.arm.y[o + 1] = Fq.y; sm.arm.z[o + 1] = Fq.z;
             t0 = __ldg(&cs0[1]);
-            angle_pair(pb, pc, t0.x, t0.y, Fp, Fq);
-            sm.armx[o + 2] = Fp.x; sm.army[o + 2] = Fp.y; sm.armz[o + 2] = Fp.z;
-            sm.armx[o + 3] = Fq.x; sm.army[o + 3] = Fq.y; sm.armz[o + 3] = Fq.z;
+            angle_pair(pb, pc, th.y, t0.x, t0.y, Fp, Fq);
+            sm.arm.x[o + 2] = Fp.x; sm.arm.y[o + 2] = Fp.y; sm.arm.z[o + 2] = Fp.z;
+            sm.arm.x[o + 3] = Fq.x; sm.arm.y[o + 3] = Fq.y; sm.arm.z[o + 3] = Fq.z;
             t0 = __ldg(&cs0[2]);
-            angle_pair(pa, pc, t0.x, t0.y, Fp, Fq);
-            sm.armx[o + 4] = Fp.x; sm.army[o + 4] = Fp.y; sm.armz[o + 4] = Fp.z;
-            sm.armx[o + 5] = Fq.x; sm.army[o + 5] = Fq.y; sm.armz[o + 5] = Fq.z;
+            angle_pair(pa, pc, th.z, t0.x, t0.y, Fp, Fq);
+            sm.arm.x[o + 4] = Fp.x; sm.arm.y[o + 4] = Fp.y; sm.arm.z[o + 4] = Fp.z;
+            sm.arm.x[o + 5] = Fq.x; sm.arm.y[o + 5] = Fq.y; sm.arm.z[o + 5] = Fq.z;
         }
         __syncthreads();
+        // The node force is accumulated in FP64: its terms (pressure up to
+        // ~1e3, stiff contact repulsion up to ~1e4) can cancel to a net force
+        // orders of magnitude smaller, and the sum is rounded to float once,
+        // as the reference stores it.
+        double FX = 0.0, FY = 0.0, FZ = 0.0;
         if (i < NODES) {
             if (isnan(x.x) || isnan(x.y) || isnan(x.z)) atomic_or_err(&d.st[inst], CS3D_ERRBIT_NAN);
-            // The node force is accumulated in FP64: its terms (pressure up
-            // to ~1e3, stiff contact repulsion up to ~1e4) can cancel to a
-            // net force orders of magnitude smaller, and the sum is rounded
-            // to float once, as the reference stores it.
-            double FX = 0.0, FY = 0.0, FZ = 0.0;
             // springs, src/propagate.cu:298-314
             const double stiff = d.E[a];
             const float4 r0 = __ldg(&d.topo.r0[i]);
@@ -544,20 +590,25 @@ __global__ void __launch_bounds__(SLOTS) k_s1(Dev d, int par)
                 const int o = i * 6;
 #pragma unroll
                 for (int q = 0; q < 3; ++q) {
-                    ax -= sm.armx[o + 2 * q] + sm.armx[o + 2 * q + 1];
-                    ay -= sm.army[o + 2 * q] + sm.army[o + 2 * q + 1];
-                    az -= sm.armz[o + 2 * q] + sm.armz[o + 2 * q + 1];
+                    ax -= sm.arm.x[o + 2 * q] + sm.arm.x[o + 2 * q + 1];
+                    ay -= sm.arm.y[o + 2 * q] + sm.arm.y[o + 2 * q + 1];
+                    az -= sm.arm.z[o + 2 * q] + sm.arm.z[o + 2 * q + 1];
                 }
                 const uint4 am = __ldg(&d.topo.arm[i]);
                 const unsigned idx[6] = {am.x & 0xffffu, am.x >> 16, am.y & 0xffffu, am.y >> 16, am.z & 0xffffu, am.z >> 16};
 #pragma unroll
-                for (int q = 0; q < 6; ++q) { ax += sm.armx[idx[q]]; ay += sm.army[idx[q]]; az += sm.armz[idx[q]]; }
+                for (int q = 0; q < 6; ++q) { ax += sm.arm.x[idx[q]]; ay += sm.arm.y[idx[q]]; az += sm.arm.z[idx[q]]; }
                 FX += ax; FY += ay; FZ += az;
             }
+        }
+        __syncthreads();  // the arm forces are consumed: gather the halo over them
+        halo_gather(d, sm.hl, hid, d.V);
+        __syncthreads();
+        if (i < NODES) {
             const float3 nrm = node_normal(sm.xs, n0, n1, n2, sgn);
             double3 cf = make_double3(0.0, 0.0, 0.0);
             double3 vt = make_double3(0.0, 0.0, 0.0);
-            contact_sweep<0>(d, P, sm.sd, sm.hl, a, i, x, v, nrm, cf, vt);
+            contact_sweep<0>(d, P, sm.sd, sm.hl, a, i, x, v, nrm, ne, first, cf, vt);
             FX += cf.x; FY += cf.y; FZ += cf.z;
             // rigid box walls, src/propagate.cu:474-510 (float gap tests)
             if (P.rigid) {
@@ -618,7 +669,7 @@ __device__ __forceinline__ void flush_mm(Dev &d, int inst, int pn, const float *
 }
 
 template <bool DIV>
-__global__ void __launch_bounds__(SLOTS) k_s2(Dev d, int par)
+__global__ void __launch_bounds__(SLOTS, 5) k_s2(Dev d, int par)
 {
     __shared__ S2Smem sm;
     const int W = n_work(d);
@@ -639,19 +690,24 @@ __global__ void __launch_bounds__(SLOTS) k_s2(Dev d, int par)
         const int nh = d.halo_n[a];
         float4 x4 = make_float4(0, 0, 0, 0), v4 = make_float4(0, 0, 0, 0);
         if (i < NODES) { x4 = d.X[g]; v4 = d.Vb[g]; }
+        const int ne = d.nent[g];
+        int first[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) first[q] = d.ent[((size_t)a * MAXE + q) * SLOTS + i];
         sm.xs[i] = x4;
         sm.vs[i] = v4;
         int hid[HREG];
         slots_phase_a(d, a, st, par, sm.sd, sm.hl, nc, nh, hid);
         __syncthreads();
-        slots_phase_b(d, P, par, sm.sd, sm.hl, nc, hid, d.Vb);
+        slots_boxes(d, P, par, sm.sd, nc);
+        halo_gather(d, sm.hl, hid, d.Vb);
         __syncthreads();
         const float3 x = f3(x4), v = f3(v4);
         if (i < NODES) {
             const float3 nrm = node_normal(sm.xs, n0, n1, n2, sgn);
             double3 cf = make_double3(0.0, 0.0, 0.0);
             double3 vt = make_double3(0.0, 0.0, 0.0);
-            contact_sweep<1>(d, P, sm.sd, sm.hl, a, i, x, v, nrm, cf, vt);
+            contact_sweep<1>(d, P, sm.sd, sm.hl, a, i, x, v, nrm, ne, first, cf, vt);
             const float3 fd = dis_force(P, sm.vs, n0, n1, n2, v, vt);
             d.FD[g] = make_float4(fd.x, fd.y, fd.z, 0.f);
             d.V[g] = v4;

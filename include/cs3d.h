@@ -51,7 +51,7 @@ extern "C" {
 
 #define CS3D_MAX_CAND      64   /* contact-candidate cells per cell */
 #define CS3D_MAX_ENTRIES   32   /* contact-candidate nodes per node */
-#define CS3D_MAX_HALO     512   /* distinct contact-candidate nodes per cell */
+#define CS3D_MAX_HALO    1024   /* distinct contact-candidate nodes per cell */
 
 /* ---- parameters of the hot path (one simulation instance) ------------- */
 /* Field meaning and units are the reference's inp.json keys.              */
