@@ -79,7 +79,7 @@ EXPORTS = [
     "cs3d_create_ensemble", "cs3d_load_state", "cs3d_set_rng", "cs3d_get_rng", "cs3d_step", "cs3d_get_state",
     "cs3d_get_forces", "cs3d_get_cells", "cs3d_get_grid", "cs3d_set_option", "cs3d_get_pairs",
     "cs3d_get_events", "cs3d_last_error", "cs3d_get_stats", "cs3d_profile_step", "cs3d_last_step_ms",
-    "cs3d_destroy",
+    "cs3d_destroy", "cs3d_forces_static",
 ]
 
 _lib = None
@@ -141,6 +141,7 @@ def lib():
     L.cs3d_profile_step.argtypes = [P, C.c_int, fp, C.c_char_p, C.c_int, C.c_int, ip]
     L.cs3d_last_step_ms.argtypes = [P, fp]
     L.cs3d_destroy.argtypes = [P]
+    L.cs3d_forces_static.argtypes = [C.POINTER(Params), C.POINTER(Topology), C.c_int] + [C.c_void_p] * 14 + [P]
     for name in EXPORTS:
         fn = getattr(L, name)
         if name not in ("cs3d_strerror",):

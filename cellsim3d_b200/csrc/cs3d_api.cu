@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -830,3 +831,260 @@ int cs3d_get_stats(cs3d_ctx *c, long long *stats, int n)
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// cs3d_forces_static: the initial force evaluation on caller-owned device
+// buffers, with every scratch buffer carved out of one file-scope static
+// device array (no allocation anywhere on this path).
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int SCAP = CS3D_STATIC_MAX_CELLS;
+constexpr int SBINS = 8 * SCAP + 65536;  // bin capacity rule of cs3d_create_ensemble
+constexpr int SEVENTS = 16;
+
+struct StaticScratch {
+    InstParams prm;
+    InstState st;
+    float4 X[SCAP * SLOTS], V[SCAP * SLOTS], Vb[SCAP * SLOTS], FC[SCAP * SLOTS], FD[SCAP * SLOTS], Xb[SCAP * SLOTS];
+    float4 CM[SCAP];
+    float press[SCAP], E[SCAP], vol[SCAP], area[SCAP];
+    uint8_t divflag[SCAP];
+    float4 aabb0[2 * SCAP], aabb1[2 * SCAP], aabb_cur[2 * SCAP];
+    int cell_inst[SCAP], work[SCAP], work_n;
+    int cand[SCAP * MAXC], ncand[SCAP];
+    int halo[SCAP * HMAX], halo_n[SCAP];
+    uint8_t halo_slot[SCAP * HMAX];
+    uint16_t ent[SCAP * MAXE * SLOTS];
+    uint8_t nent[SCAP * SLOTS];
+    int bin_count[SBINS + 1], bin_start[SBINS + 1], bin_cells[SCAP], cell_bin[SCAP], cell_rank[SCAP], total_bins;
+    DivEntry divtab[SCAP];
+    int div_total;
+    int4 events[SEVENTS];
+    int n_events;
+    int flags[4];
+    int4 pairs[1];
+    unsigned long long n_pairs;
+    uint32_t nnpack[SLOTS];
+    float4 r0[SLOTS], th0[SLOTS];
+    uint4 arm[SLOTS];
+    uint8_t faces[CS3D_FACES * 7];
+    double2 cs0[3 * SLOTS];
+};
+
+// The scratch of cs3d_forces_static.  In host code this name is only a
+// stand-in for the device object: kernels receive the address resolved with
+// cudaGetSymbolAddress, per device.
+static __device__ __align__(256) unsigned char g_static_scratch[sizeof(StaticScratch)];
+
+struct StaticDevice {
+    bool ready = false;
+    StaticScratch *base = nullptr;
+    int grid_cells = 1, grid_flat = 1;
+};
+
+constexpr int kMaxDevices = 64;
+StaticDevice g_static_dev[kMaxDevices];
+std::mutex g_static_mutex;
+
+// Host copies of the mesh tables (the same tables upload_topology builds).
+struct TopoTables {
+    uint32_t nnp[SLOTS];
+    float4 r0[SLOTS], th[SLOTS];
+    uint4 arm[SLOTS];
+    uint8_t faces[CS3D_FACES * 7];
+    double2 cs0[3 * SLOTS];
+};
+
+int topo_tables(const cs3d_topology *t, TopoTables &o)
+{
+    memset(&o, 0, sizeof o);
+    for (int i = 0; i < 3 * SLOTS; ++i) o.cs0[i] = make_double2(1.0, 0.0);
+    for (int i = 0; i < NODES; ++i) {
+        int a = t->nn[i], b = t->nn[192 + i], cc = t->nn[384 + i];
+        if (a < 0 || a >= NODES || b < 0 || b >= NODES || cc < 0 || cc >= NODES) return CS3D_E_ARG;
+        o.nnp[i] = (uint32_t)a | ((uint32_t)b << 8) | ((uint32_t)cc << 16) | ((uint32_t)(uint8_t)(int8_t)t->sign[i] << 24);
+        o.r0[i] = make_float4(t->r0[i], t->r0[192 + i], t->r0[384 + i], 0.f);
+        o.th[i] = make_float4(t->theta0[3 * i], t->theta0[3 * i + 1], t->theta0[3 * i + 2], 0.f);
+        for (int k = 0; k < 3; ++k) {
+            const double th = (double)t->theta0[3 * i + k];
+            o.cs0[3 * i + k] = make_double2(cos(th), sin(th));
+        }
+    }
+    for (int i = 0; i < NODES; ++i) {
+        unsigned idx[6];
+        for (int q = 0; q < 3; ++q) {
+            int n = t->nn[q * 192 + i];
+            int na = t->nn[n], nb = t->nn[192 + n], nc = t->nn[384 + n];
+            unsigned base = (unsigned)n * 6;
+            if (na == i) { idx[2 * q] = base + 0; idx[2 * q + 1] = base + 4; }
+            else if (nb == i) { idx[2 * q] = base + 1; idx[2 * q + 1] = base + 2; }
+            else if (nc == i) { idx[2 * q] = base + 5; idx[2 * q + 1] = base + 3; }
+            else return CS3D_E_ARG;
+        }
+        o.arm[i] = make_uint4(idx[0] | (idx[1] << 16), idx[2] | (idx[3] << 16), idx[4] | (idx[5] << 16), 0u);
+    }
+    for (int f = 0; f < CS3D_FACES * 7; ++f) {
+        if (t->faces[f] < 0 || t->faces[f] >= NODES) return CS3D_E_ARG;
+        o.faces[f] = (uint8_t)t->faces[f];
+    }
+    return CS3D_OK;
+}
+
+Dev static_dev(StaticScratch *s)
+{
+    Dev d{};
+    d.n_inst = 1;
+    d.cap_total = SCAP;
+    d.single = 1;
+    d.prm = &s->prm;
+    d.st = &s->st;
+    d.topo.nnpack = s->nnpack;
+    d.topo.r0 = s->r0;
+    d.topo.th0 = s->th0;
+    d.topo.arm = s->arm;
+    d.topo.faces = s->faces;
+    d.topo.cs0 = s->cs0;
+    d.X = s->X; d.V = s->V; d.Vb = s->Vb; d.FC = s->FC; d.FD = s->FD; d.Xb = s->Xb;
+    d.CM = s->CM;
+    d.press = s->press; d.E = s->E; d.vol = s->vol; d.area = s->area;
+    d.divflag = s->divflag;
+    d.aabb[0] = s->aabb0; d.aabb[1] = s->aabb1; d.aabb_cur = s->aabb_cur;
+    d.cell_inst = s->cell_inst; d.work = s->work; d.work_n = &s->work_n;
+    d.cand = s->cand; d.ncand = s->ncand;
+    d.halo = s->halo; d.halo_slot = s->halo_slot; d.halo_n = s->halo_n;
+    d.ent = s->ent; d.nent = s->nent;
+    d.bin_count = s->bin_count; d.bin_start = s->bin_start; d.bin_cells = s->bin_cells;
+    d.cell_bin = s->cell_bin; d.cell_rank = s->cell_rank; d.bin_cap = SBINS; d.total_bins = &s->total_bins;
+    d.divtab = s->divtab; d.div_total = &s->div_total;
+    d.events = s->events; d.n_events = &s->n_events; d.ev_cap = SEVENTS;
+    d.flags = s->flags;
+    d.pairs = s->pairs; d.n_pairs = &s->n_pairs; d.pair_cap = 1; d.record_pairs = 0;
+    return d;
+}
+
+// Caller's 192-stride SoA inputs into the scratch (float4), defaults for the
+// per-cell arrays, zero forces.
+__global__ void k_static_load(Dev d, int n, const float *X, const float *Y, const float *Z, const float *VX,
+                              const float *VY, const float *VZ, const float *press, const float *E, float minp,
+                              float stiff1)
+{
+    const int total = n * SLOTS;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+        const bool real = (g % SLOTS) < NODES;
+        d.X[g] = real ? make_float4(X[g], Y[g], Z[g], 0.f) : make_float4(0, 0, 0, 0);
+        d.V[g] = (real && VX) ? make_float4(VX[g], VY[g], VZ[g], 0.f) : make_float4(0, 0, 0, 0);
+        d.FC[g] = make_float4(0, 0, 0, 0);
+        d.FD[g] = make_float4(0, 0, 0, 0);
+        if (g < n) {
+            d.press[g] = press ? press[g] : minp;
+            d.E[g] = E ? E[g] : stiff1;
+            d.cell_inst[g] = 0;
+            d.CM[g] = make_float4(0, 0, 0, 0);
+        }
+    }
+}
+
+__global__ void k_static_store(Dev d, int n, float *FCX, float *FCY, float *FCZ, float *FDX, float *FDY, float *FDZ)
+{
+    const int total = n * SLOTS;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+        const bool real = (g % SLOTS) < NODES;
+        const float4 c = real ? d.FC[g] : make_float4(0, 0, 0, 0);
+        const float4 f = real ? d.FD[g] : make_float4(0, 0, 0, 0);
+        FCX[g] = c.x; FCY[g] = c.y; FCZ[g] = c.z;
+        FDX[g] = f.x; FDY[g] = f.y; FDZ[g] = f.z;
+    }
+}
+
+// Per-device set-up: resolve the static array's device address and set the
+// kernel attributes the init sequence needs.  Runs once per device.
+int static_setup(int dev, StaticDevice **out)
+{
+    if (dev < 0 || dev >= kMaxDevices) return CS3D_E_ARG;
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    StaticDevice &sd = g_static_dev[dev];
+    if (!sd.ready) {
+        void *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+        if (e != cudaSuccess || !ptr) {
+            fprintf(stderr, "cs3d: cudaGetSymbolAddress of the static scratch failed: %s\n", cudaGetErrorString(e));
+            return CS3D_E_CUDA;
+        }
+        sd.base = (StaticScratch *)ptr;
+        CK(cudaFuncSetAttribute(k_s1<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(S1Smem)));
+        int nsm = 148, occ = 1;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_s1<true>, SLOTS, sizeof(S1Smem)));
+        sd.grid_cells = std::max(1, std::min(SCAP, nsm * std::max(occ, 1)));
+        sd.grid_flat = std::max(1, std::min((SCAP * SLOTS + 255) / 256, nsm * 8));
+        sd.ready = true;
+    }
+    *out = &sd;
+    return CS3D_OK;
+}
+
+}  // namespace
+
+extern "C" int cs3d_forces_static(const cs3d_params *params, const cs3d_topology *topo, int n_cells,
+                                  const float *X, const float *Y, const float *Z, const float *VX, const float *VY,
+                                  const float *VZ, const float *pressure, const float *youngs, float *FCX,
+                                  float *FCY, float *FCZ, float *FDX, float *FDY, float *FDZ, void *stream)
+{
+    if (!params || !topo || !X || !Y || !Z || !FCX || !FCY || !FCZ || !FDX || !FDY || !FDZ) return CS3D_E_ARG;
+    if ((VX || VY || VZ) && !(VX && VY && VZ)) return CS3D_E_ARG;
+    if (n_cells < 1 || n_cells > SCAP) {
+        fprintf(stderr, "cs3d_forces_static: %d cells requested, the static scratch holds 1..%d\n", n_cells, SCAP);
+        return CS3D_E_ARG;
+    }
+    if (check_params(*params)) return CS3D_E_CONFIG;
+    TopoTables tt;
+    int rc = topo_tables(topo, tt);
+    if (rc) return rc;
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    StaticDevice *sd = nullptr;
+    if ((rc = static_setup(dev, &sd))) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    StaticScratch *S = sd->base;
+    const Dev d = static_dev(S);
+    // parameters, mesh tables and a cleared instance state
+    const InstParams ip = make_inst(*params, 0, SCAP, 0.1f);
+    InstState st0;
+    memset(&st0, 0, sizeof st0);
+    st0.n = n_cells;
+    CK(cudaMemcpyAsync(&S->prm, &ip, sizeof ip, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(&S->st, &st0, sizeof st0, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(S->nnpack, tt.nnp, sizeof tt.nnp, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(S->r0, tt.r0, sizeof tt.r0, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(S->th0, tt.th, sizeof tt.th, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(S->arm, tt.arm, sizeof tt.arm, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(S->faces, tt.faces, sizeof tt.faces, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(S->cs0, tt.cs0, sizeof tt.cs0, cudaMemcpyHostToDevice, s));
+    // the previous call's neighbour lists, boxes and flags must not leak in
+    CK(cudaMemsetAsync(S->ncand, 0, sizeof S->ncand, s));
+    CK(cudaMemsetAsync(S->halo_n, 0, sizeof S->halo_n, s));
+    CK(cudaMemsetAsync(S->nent, 0, sizeof S->nent, s));
+    CK(cudaMemsetAsync(S->flags, 0, sizeof S->flags, s));
+    CK(cudaMemsetAsync(&S->n_events, 0, sizeof S->n_events, s));
+    k_static_load<<<sd->grid_flat, 256, 0, s>>>(d, n_cells, X, Y, Z, VX, VY, VZ, pressure, youngs, params->min_pressure,
+                                                  params->stiffness1);
+    // the initialisation sequence of run_init on the static buffers
+    k_build_work<<<1, 256, 0, s>>>(d);
+    k_init_begin<<<1, 256, 0, s>>>(d);
+    k_geom<<<sd->grid_cells, SLOTS, 0, s>>>(d, 0);
+    k_nl_boxes<<<sd->grid_cells, SLOTS, 0, s>>>(d);
+    k_nl_grid<<<1, 32, 0, s>>>(d);
+    k_nl_zero<<<sd->grid_flat, 256, 0, s>>>(d);
+    k_nl_count<<<sd->grid_flat, 256, 0, s>>>(d);
+    k_nl_scan<<<1, 1024, 0, s>>>(d);
+    k_nl_fill<<<sd->grid_flat, 256, 0, s>>>(d);
+    k_nl_build<<<sd->grid_cells, SLOTS, 0, s>>>(d);
+    k_s1<true><<<sd->grid_cells, SLOTS, sizeof(S1Smem), s>>>(d, 0);
+    k_static_store<<<sd->grid_flat, 256, 0, s>>>(d, n_cells, FCX, FCY, FCZ, FDX, FDY, FDZ);
+    CK(cudaGetLastError());
+    unsigned err = 0;
+    CK(cudaMemcpyAsync(&err, &S->st.err, sizeof err, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return err ? CS3D_E_DEVICE_FLAGS : CS3D_OK;
+}

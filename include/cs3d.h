@@ -280,6 +280,45 @@ int cs3d_get_stats(cs3d_ctx *ctx, long long *stats, int n);
 int cs3d_profile_step(cs3d_ctx *ctx, int n_steps, float *kernel_ms, char *names, int names_len,
                       int max_kernels, int *n_kernels);
 
+/* ---- force evaluation without allocation ------------------------------ */
+
+/* Largest system cs3d_forces_static accepts. */
+#define CS3D_STATIC_MAX_CELLS 64
+
+/* Forces of one system of n_cells <= CS3D_STATIC_MAX_CELLS cells -- the
+ * force evaluation that cs3d_load_state triggers, with the same kernels and
+ * the same results -- computed without allocating any memory.
+ *
+ * No counterpart in the reference.  It is meant for callers that cannot
+ * allocate GPU memory: code running inside a host that has already
+ * partitioned the device (a memory pool or arena owned by someone else), a
+ * real-time loop that must never call cudaMalloc/cudaFree (they synchronise
+ * the device), or a plugin host that forbids allocation in callbacks.  The
+ * caller passes device pointers to inputs and outputs it owns; everything
+ * else the kernels need (the contact lists, grids and per-cell data) lives
+ * in one file-scope static device array of this library (about 5 MB, held
+ * by every GPU that loads the library until the process exits).
+ *
+ * Inputs (device, 192-stride SoA as cs3d_load_state): X, Y, Z, VX, VY, VZ
+ * (VX/VY/VZ may be NULL: zero velocity), pressure and youngs (device, per
+ * cell; NULL: min_pressure and stiffness1).  Outputs (device, 192-stride):
+ * the conservative and dissipative forces; slots 180..191 are set to zero.
+ * stream may be NULL (legacy default stream).
+ *
+ * The first call on a device resolves the static array's device address
+ * (cudaGetSymbolAddress) and sets kernel attributes; make that first call
+ * before any stream capture.  Every call shares the one static array, so
+ * calls that overlap on the GPU (different streams or host threads) race:
+ * serialise them.  The call waits for its kernels and reads back the error
+ * word before returning.  Returns CS3D_E_ARG for n_cells outside
+ * [1, CS3D_STATIC_MAX_CELLS] or a NULL required pointer. */
+int cs3d_forces_static(const cs3d_params *params, const cs3d_topology *topo, int n_cells,
+                       const float *X, const float *Y, const float *Z,
+                       const float *VX, const float *VY, const float *VZ,
+                       const float *pressure, const float *youngs,
+                       float *FCX, float *FCY, float *FCZ, float *FDX, float *FDY, float *FDZ,
+                       void *stream);
+
 /* Device time of the last cs3d_step call (ms, CUDA events). */
 int cs3d_last_step_ms(cs3d_ctx *ctx, float *ms);
 
