@@ -33,6 +33,8 @@ struct cs3d_ctx {
     float skin = 0.1f;
     int grid_cells = 0;            // blocks of the per-cell kernels
     int grid_flat = 0;             // blocks of the per-thread kernels
+    int grid_nodes = 0;            // blocks of the neighbour-list kernels
+    int grid_tiles = 0;            // blocks of the bucket scan
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     float last_ms = 0.f;
@@ -213,19 +215,35 @@ struct Prof {
     }
 };
 
-int launch_nl_build(cs3d_ctx *c, const Prof &pf = Prof())
+// Neighbour-list build: spatial hash of the nodes (counting sort by
+// bucket), then the per-cell lists.  Every kernel returns at once when no
+// instance rebuilds this step.
+int launch_nl_kernels(const Dev &d, cudaStream_t s, int grid_nodes, int grid_tiles, const Prof &pf = Prof())
 {
-    const Dev &d = c->d;
-    cudaStream_t s = c->stream;
-    k_nl_boxes<<<c->grid_cells, SLOTS, 0, s>>>(d); pf.mark(s, "nl_boxes");
-    k_nl_grid<<<1, 32, 0, s>>>(d); pf.mark(s, "nl_grid");
-    k_nl_zero<<<c->grid_flat, 256, 0, s>>>(d); pf.mark(s, "nl_zero");
-    k_nl_count<<<c->grid_flat, 256, 0, s>>>(d); pf.mark(s, "nl_count");
-    k_nl_scan<<<1, 1024, 0, s>>>(d); pf.mark(s, "nl_scan");
-    k_nl_fill<<<c->grid_flat, 256, 0, s>>>(d); pf.mark(s, "nl_fill");
-    k_nl_build<<<c->grid_cells, SLOTS, 0, s>>>(d); pf.mark(s, "nl_build");
+    k_nh_zero<<<grid_tiles, 256, 0, s>>>(d); pf.mark(s, "nh_zero");
+    k_nh_count<<<grid_nodes, SLOTS, 0, s>>>(d); pf.mark(s, "nh_count");
+    k_nh_scan_tiles<<<grid_tiles, 256, 0, s>>>(d); pf.mark(s, "nh_scan_tiles");
+    k_nh_scan_top<<<1, 1024, 0, s>>>(d); pf.mark(s, "nh_scan_top");
+    k_nh_scan_apply<<<grid_tiles, 256, 0, s>>>(d); pf.mark(s, "nh_scan_apply");
+    k_nh_fill<<<grid_nodes, SLOTS, 0, s>>>(d); pf.mark(s, "nh_fill");
+    k_nl_cell<<<grid_nodes, SLOTS, 0, s>>>(d); pf.mark(s, "nl_cell");
     CK(cudaGetLastError());
     return CS3D_OK;
+}
+constexpr int NL_LAUNCHES = 7;
+
+int launch_nl_build(cs3d_ctx *c, const Prof &pf = Prof())
+{
+    return launch_nl_kernels(c->d, c->stream, c->grid_nodes, c->grid_tiles, pf);
+}
+
+// Buckets of the node hash for a capacity of `cells` cells.
+constexpr int hash_size(long long cells)
+{
+    long long n = std::max<long long>(cells * SLOTS, SCAN_TILE);
+    int h = SCAN_TILE;
+    while (h < n) h <<= 1;
+    return h;
 }
 
 int run_init(cs3d_ctx *c)
@@ -255,7 +273,7 @@ int launch_step(cs3d_ctx *c, int par, bool div, const Prof &pf = Prof())
     k_step_begin<<<1, 256, 0, s>>>(d, par ^ 1); ++n; pf.mark(s, "step_begin");
     int rc = launch_nl_build(c, pf);
     if (rc) return rc;
-    n += 7;
+    n += NL_LAUNCHES;
     k_s1<false><<<c->grid_cells, SLOTS, sizeof(S1Smem), s>>>(d, par); ++n; pf.mark(s, "s1_con_dis");
     if (div) k_s2<true><<<c->grid_cells, SLOTS, 0, s>>>(d, par);
     else k_s2<false><<<c->grid_cells, SLOTS, 0, s>>>(d, par);
@@ -386,7 +404,6 @@ int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topol
     AL(d.press, c->cap_total); AL(d.E, c->cap_total); AL(d.vol, c->cap_total); AL(d.area, c->cap_total);
     AL(d.divflag, c->cap_total);
     AL(d.aabb[0], 2 * (size_t)c->cap_total); AL(d.aabb[1], 2 * (size_t)c->cap_total);
-    AL(d.aabb_cur, 2 * (size_t)c->cap_total);
     AL(d.cell_inst, c->cap_total);
     AL(d.work, c->cap_total); AL(d.work_n, 1);
     AL(d.cand, (size_t)c->cap_total * MAXC); AL(d.ncand, c->cap_total);
@@ -394,10 +411,9 @@ int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topol
     AL(d.halo_slot, (size_t)c->cap_total * HMAX);
     AL(d.Xb, nodes);
     AL(d.ent, (size_t)c->cap_total * MAXE * SLOTS); AL(d.nent, nodes);
-    d.bin_cap = 8 * c->cap_total + 65536;
-    AL(d.bin_count, (size_t)d.bin_cap + 1); AL(d.bin_start, (size_t)d.bin_cap + 1);
-    AL(d.bin_cells, c->cap_total); AL(d.cell_bin, c->cap_total); AL(d.cell_rank, c->cap_total);
-    AL(d.total_bins, 1);
+    d.hsize = hash_size(c->cap_total);
+    AL(d.hcount, (size_t)d.hsize + SCAN_TILE); AL(d.hscan, (size_t)d.hsize / SCAN_TILE + 1);
+    AL(d.hpos, nodes); AL(d.node_rank, nodes);
     AL(d.divtab, c->cap_total); AL(d.div_total, 1);
     d.ev_cap = std::max(1 << 16, 2 * c->cap_total);
     AL(d.events, d.ev_cap); AL(d.n_events, 1);
@@ -434,6 +450,10 @@ int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topol
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_s1<false>, SLOTS, sizeof(S1Smem));
     c->grid_cells = std::max(1, std::min(c->cap_total, c->nsm * std::max(occ, 1)));
     c->grid_flat = std::max(1, std::min((c->cap_total + 255) / 256 + 1, c->nsm * 8));
+    int occ_nl = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_nl, k_nl_cell, SLOTS, 0);
+    c->grid_nodes = std::max(1, std::min(c->cap_total, c->nsm * std::max(occ_nl, 1)));
+    c->grid_tiles = std::max(1, std::min(d.hsize / SCAN_TILE + 1, c->nsm * 8));
     *out = c;
     return CS3D_OK;
 }
@@ -840,7 +860,7 @@ int cs3d_get_stats(cs3d_ctx *c, long long *stats, int n)
 namespace {
 
 constexpr int SCAP = CS3D_STATIC_MAX_CELLS;
-constexpr int SBINS = 8 * SCAP + 65536;  // bin capacity rule of cs3d_create_ensemble
+constexpr int SHASH = hash_size(SCAP);   // bucket rule of cs3d_create_ensemble
 constexpr int SEVENTS = 16;
 
 struct StaticScratch {
@@ -850,14 +870,16 @@ struct StaticScratch {
     float4 CM[SCAP];
     float press[SCAP], E[SCAP], vol[SCAP], area[SCAP];
     uint8_t divflag[SCAP];
-    float4 aabb0[2 * SCAP], aabb1[2 * SCAP], aabb_cur[2 * SCAP];
+    float4 aabb0[2 * SCAP], aabb1[2 * SCAP];
+    float4 hpos[SCAP * SLOTS];
+    alignas(16) int hcount[SHASH + SCAN_TILE];
+    int hscan[SHASH / SCAN_TILE + 1], node_rank[SCAP * SLOTS];
     int cell_inst[SCAP], work[SCAP], work_n;
     int cand[SCAP * MAXC], ncand[SCAP];
     int halo[SCAP * HMAX], halo_n[SCAP];
     uint8_t halo_slot[SCAP * HMAX];
     uint16_t ent[SCAP * MAXE * SLOTS];
     uint8_t nent[SCAP * SLOTS];
-    int bin_count[SBINS + 1], bin_start[SBINS + 1], bin_cells[SCAP], cell_bin[SCAP], cell_rank[SCAP], total_bins;
     DivEntry divtab[SCAP];
     int div_total;
     int4 events[SEVENTS];
@@ -880,7 +902,7 @@ static __device__ __align__(256) unsigned char g_static_scratch[sizeof(StaticScr
 struct StaticDevice {
     bool ready = false;
     StaticScratch *base = nullptr;
-    int grid_cells = 1, grid_flat = 1;
+    int grid_cells = 1, grid_flat = 1, grid_nodes = 1, grid_tiles = 1;
 };
 
 constexpr int kMaxDevices = 64;
@@ -949,13 +971,12 @@ Dev static_dev(StaticScratch *s)
     d.CM = s->CM;
     d.press = s->press; d.E = s->E; d.vol = s->vol; d.area = s->area;
     d.divflag = s->divflag;
-    d.aabb[0] = s->aabb0; d.aabb[1] = s->aabb1; d.aabb_cur = s->aabb_cur;
+    d.aabb[0] = s->aabb0; d.aabb[1] = s->aabb1;
     d.cell_inst = s->cell_inst; d.work = s->work; d.work_n = &s->work_n;
     d.cand = s->cand; d.ncand = s->ncand;
     d.halo = s->halo; d.halo_slot = s->halo_slot; d.halo_n = s->halo_n;
     d.ent = s->ent; d.nent = s->nent;
-    d.bin_count = s->bin_count; d.bin_start = s->bin_start; d.bin_cells = s->bin_cells;
-    d.cell_bin = s->cell_bin; d.cell_rank = s->cell_rank; d.bin_cap = SBINS; d.total_bins = &s->total_bins;
+    d.hsize = SHASH; d.hcount = s->hcount; d.hscan = s->hscan; d.hpos = s->hpos; d.node_rank = s->node_rank;
     d.divtab = s->divtab; d.div_total = &s->div_total;
     d.events = s->events; d.n_events = &s->n_events; d.ev_cap = SEVENTS;
     d.flags = s->flags;
@@ -1018,6 +1039,8 @@ int static_setup(int dev, StaticDevice **out)
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_s1<true>, SLOTS, sizeof(S1Smem)));
         sd.grid_cells = std::max(1, std::min(SCAP, nsm * std::max(occ, 1)));
         sd.grid_flat = std::max(1, std::min((SCAP * SLOTS + 255) / 256, nsm * 8));
+        sd.grid_nodes = std::max(1, std::min(SCAP, nsm * 8));
+        sd.grid_tiles = std::max(1, std::min(SHASH / SCAN_TILE + 1, nsm * 8));
         sd.ready = true;
     }
     *out = &sd;
@@ -1073,13 +1096,7 @@ extern "C" int cs3d_forces_static(const cs3d_params *params, const cs3d_topology
     k_build_work<<<1, 256, 0, s>>>(d);
     k_init_begin<<<1, 256, 0, s>>>(d);
     k_geom<<<sd->grid_cells, SLOTS, 0, s>>>(d, 0);
-    k_nl_boxes<<<sd->grid_cells, SLOTS, 0, s>>>(d);
-    k_nl_grid<<<1, 32, 0, s>>>(d);
-    k_nl_zero<<<sd->grid_flat, 256, 0, s>>>(d);
-    k_nl_count<<<sd->grid_flat, 256, 0, s>>>(d);
-    k_nl_scan<<<1, 1024, 0, s>>>(d);
-    k_nl_fill<<<sd->grid_flat, 256, 0, s>>>(d);
-    k_nl_build<<<sd->grid_cells, SLOTS, 0, s>>>(d);
+    if ((rc = launch_nl_kernels(d, s, sd->grid_nodes, sd->grid_tiles))) return rc;
     k_s1<true><<<sd->grid_cells, SLOTS, sizeof(S1Smem), s>>>(d, 0);
     k_static_store<<<sd->grid_flat, 256, 0, s>>>(d, n_cells, FCX, FCY, FCZ, FDX, FDY, FDZ);
     CK(cudaGetLastError());

@@ -13,6 +13,8 @@ constexpr int NODES = CS3D_NODES;      // real nodes per cell
 constexpr int MAXC = CS3D_MAX_CAND;    // contact-candidate cells per cell
 constexpr int MAXE = CS3D_MAX_ENTRIES; // contact-candidate nodes per node
 constexpr int HMAX = CS3D_MAX_HALO;    // distinct contact-candidate nodes per cell
+constexpr int HPAGE = 1024;            // halo nodes staged in shared memory at a time
+constexpr int SCAN_TILE = 4096;        // elements per block of the bucket scan
 constexpr float DL = 2.9f;             // reference grid spacing, src/GPUbounce.cu:756
 constexpr int NARM = NODES * 3 * 2;    // arm-end forces of the 540 angles
 
@@ -41,12 +43,6 @@ struct InstState {
     unsigned disp_step;    // max node displacement of the current step (float bits)
     int div_count;         // divisions in the current step
     int force_rebuild;
-    int bmm[6];            // build-grid extents (ordered ints)
-    unsigned maxext;       // largest cell extent (float bits)
-    float borg[3];         // build-grid origin
-    float bh;              // build-grid bin size
-    int bdim[3];
-    int boff;              // first bin of this instance in the global bin array
     int max_entries, max_cand, max_halo;
     int rebuilds;
     // RANMAR, src/marsaglia.h:50-52
@@ -85,7 +81,6 @@ struct Dev {
     float *press, *E, *vol, *area;
     uint8_t *divflag;
     float4 *aabb[2];    // [2*cell] lo, hi  (stale boxes by parity)
-    float4 *aabb_cur;   // boxes at neighbour-list build
     int *cell_inst;
     int *work;          // active cells
     int *work_n;
@@ -98,9 +93,13 @@ struct Dev {
     float4 *Xb;         // positions at the last neighbour-list build
     uint16_t *ent;      // [(cell*MAXE + k)*192 + node] halo index
     uint8_t *nent;      // [cell*192 + node]
-    int *bin_count, *bin_start, *bin_cells, *cell_bin, *cell_rank;
-    int bin_cap;
-    int *total_bins;
+    // node-level spatial hash of the neighbour-list build: cubic bins of
+    // edge ~rlist hashed (with the instance) into hsize buckets
+    int hsize;          // buckets (power of two, >= SCAN_TILE)
+    int *hcount;        // [hsize + 1] bucket counts, then exclusive starts
+    int *hscan;         // [hsize / SCAN_TILE + 1] tile sums of the scan
+    float4 *hpos;       // [cap_total*192] positions sorted by bucket, w = node id bits
+    int *node_rank;     // [cap_total*192] position of the node in its bucket
     DivEntry *divtab;
     int *div_total;
     int4 *events;       // (inst, step, parent, daughter)

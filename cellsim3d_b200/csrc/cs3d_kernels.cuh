@@ -112,33 +112,35 @@ __device__ __forceinline__ void angle_pair(float3 P, float3 Q, float th0f, doubl
 }
 
 // Shared per-CTA data of the contact sweep: candidate cells with their stale
-// boxes and stale insertion bin ranges, and the gathered halo.
+// boxes and stale insertion bin ranges.
 struct SlotData {
     int cell[MAXC];
     float4 lo[MAXC], hi[MAXC];
-    int rlo[MAXC][3], rhi[MAXC][3];
+    short rlo[MAXC][3], rhi[MAXC][3];
     float mn[3];
     int div[3];
 };
 
+// One page of the halo: positions, velocities and candidate slots of up to
+// HPAGE halo nodes (halo indices [page*HPAGE, page*HPAGE + HPAGE)).
 struct Halo {
-    float4 x[HMAX];
-    float4 v[HMAX];
-    uint8_t s[HMAX];
+    float4 x[HPAGE];
+    float4 v[HPAGE];
+    uint8_t s[HPAGE];
 };
 
-// Phase A of a cell: candidate cells, stale grid, the halo's node ids (into
-// registers) and slots.  Independent loads only, so they overlap with the
-// caller's own-node loads; the caller then calls __syncthreads().
-constexpr int HREG = (HMAX + SLOTS - 1) / SLOTS;
+constexpr int HREG = (HPAGE + SLOTS - 1) / SLOTS;
 
+// Phase A of a cell: candidate cells, stale grid and the node ids of the
+// first halo page (into registers).  Independent loads only, so they overlap
+// with the caller's own-node loads; the caller then calls __syncthreads().
 __device__ __forceinline__ void slots_phase_a(const Dev &d, int a, const InstState *st, int par, SlotData &sd,
-                                              Halo &hl, int nc, int nh, int (&hid)[HREG])
+                                              int nh, int (&hid)[HREG])
 {
     int t = threadIdx.x;
     // the lists are read in full, whatever their counts, so that no load
     // waits for another (entries past the counts are never used)
-    if (t < MAXC) sd.cell[t] = d.cand[a * MAXC + t];
+    if (t < MAXC) sd.cell[t] = d.cand[(size_t)a * MAXC + t];
     if (t == 0) {
         const int *mm = st->mm[par];
         for (int q = 0; q < 3; ++q) {
@@ -151,20 +153,15 @@ __device__ __forceinline__ void slots_phase_a(const Dev &d, int a, const InstSta
 #pragma unroll
     for (int q = 0; q < HREG; ++q) {
         const int h = t + q * SLOTS;
-        if (h < HMAX) {
+        hid[q] = -1;
+        if (h < HPAGE) {
             const int id = d.halo[(size_t)a * HMAX + h];
-            const uint8_t sl = d.halo_slot[(size_t)a * HMAX + h];
-            hid[q] = h < nh ? id : -1;
-            hl.s[h] = sl;
-        } else {
-            hid[q] = -1;
+            if (h < nh) hid[q] = id;
         }
     }
 }
 
-// Phase B: stale boxes / insertion ranges of the candidates, then the halo
-// gather (positions from X, velocities from Vsrc).  Needs phase A to be
-// visible (__syncthreads() before), and a __syncthreads() after.
+// Stale boxes / insertion ranges of the candidates (phase A visible before).
 __device__ __forceinline__ void slots_boxes(const Dev &d, const InstParams &P, int par, SlotData &sd, int nc)
 {
     int t = threadIdx.x;
@@ -173,86 +170,110 @@ __device__ __forceinline__ void slots_boxes(const Dev &d, const InstParams &P, i
         float4 lo = d.aabb[par][2 * c], hi = d.aabb[par][2 * c + 1];
         sd.lo[t] = lo;
         sd.hi[t] = hi;
-        bin_range_axis(lo.x, hi.x, P.ra, sd.mn[0], sd.div[0], sd.rlo[t][0], sd.rhi[t][0]);
-        bin_range_axis(lo.y, hi.y, P.ra, sd.mn[1], sd.div[1], sd.rlo[t][1], sd.rhi[t][1]);
-        bin_range_axis(lo.z, hi.z, P.ra, sd.mn[2], sd.div[2], sd.rlo[t][2], sd.rhi[t][2]);
+        int st, en;
+        bin_range_axis(lo.x, hi.x, P.ra, sd.mn[0], sd.div[0], st, en); sd.rlo[t][0] = (short)st; sd.rhi[t][0] = (short)en;
+        bin_range_axis(lo.y, hi.y, P.ra, sd.mn[1], sd.div[1], st, en); sd.rlo[t][1] = (short)st; sd.rhi[t][1] = (short)en;
+        bin_range_axis(lo.z, hi.z, P.ra, sd.mn[2], sd.div[2], st, en); sd.rlo[t][2] = (short)st; sd.rhi[t][2] = (short)en;
     }
 }
 
-__device__ __forceinline__ void halo_gather(const Dev &d, Halo &hl, const int (&hid)[HREG],
+// Gather halo page `page` (positions from X, velocities from Vsrc).  Page 0
+// uses the ids prefetched in phase A.  Needs a __syncthreads() after.
+__device__ __forceinline__ void halo_gather(const Dev &d, int a, int page, int nh, Halo &hl, const int (&hid)[HREG],
                                             const float4 *__restrict__ Vsrc)
 {
     const int t = threadIdx.x;
+    const int base = page * HPAGE;
 #pragma unroll
     for (int q = 0; q < HREG; ++q) {
-        if (hid[q] < 0) break;
-        hl.x[t + q * SLOTS] = __ldg(&d.X[hid[q]]);
-        hl.v[t + q * SLOTS] = __ldg(&Vsrc[hid[q]]);
+        const int h = t + q * SLOTS;
+        if (h >= HPAGE) break;
+        if (base + h >= nh) break;
+        const int id = page == 0 ? hid[q] : d.halo[(size_t)a * HMAX + base + h];
+        hl.s[h] = d.halo_slot[(size_t)a * HMAX + base + h];
+        hl.x[h] = __ldg(&d.X[id]);
+        hl.v[h] = __ldg(&Vsrc[id]);
     }
 }
 
 // ---------------------------------------------------------------------------
-// Contact sweep of one node over its neighbour-list entries (halo indices).
-// MODE 0: conservative + dissipative (S1); MODE 1: dissipative only (S2).
+// Contact sweep of one node over its neighbour-list entries (halo indices,
+// ascending) that fall on the staged halo page.  MODE 0: conservative +
+// dissipative (S1); MODE 1: dissipative only (S2).  The cursor k and the
+// per-slot predicate cache carry over from page to page.
 // ---------------------------------------------------------------------------
-template <int MODE>
-__device__ __forceinline__ void contact_sweep(const Dev &d, const InstParams &P, const SlotData &sd, const Halo &hl,
-                                              int a, int i, float3 x, float3 v, float3 nrm, int ne,
-                                              const int (&first)[4], double3 &cf, double3 &vt)
+struct Sweep {
+    int k;          // next entry
+    int cur;        // slot of the cached predicate
+    bool ok;        // cached predicate: stale grid bin and stale box test
+    int nb0, nb1, nb2;
+};
+
+constexpr int EPRE = 8;  // entries prefetched per node
+
+__device__ __forceinline__ void sweep_init(Sweep &sw, const SlotData &sd, float3 x)
 {
-    const int nb0 = node_bin_axis(x.x, sd.mn[0], sd.div[0]);
-    const int nb1 = node_bin_axis(x.y, sd.mn[1], sd.div[1]);
-    const int nb2 = node_bin_axis(x.z, sd.mn[2], sd.div[2]);
+    sw.k = 0;
+    sw.cur = -1;
+    sw.ok = false;
+    sw.nb0 = node_bin_axis(x.x, sd.mn[0], sd.div[0]);
+    sw.nb1 = node_bin_axis(x.y, sd.mn[1], sd.div[1]);
+    sw.nb2 = node_bin_axis(x.z, sd.mn[2], sd.div[2]);
+}
+
+template <int MODE>
+__device__ __forceinline__ void sweep_page(const Dev &d, const InstParams &P, const SlotData &sd, const Halo &hl,
+                                           int a, int i, int page, float3 x, float3 v, float3 nrm, int ne,
+                                           const int (&pre)[EPRE], Sweep &sw, double3 &cf, double3 &vt)
+{
+    const int base = page * HPAGE;
     const uint16_t *ep = d.ent + (size_t)a * MAXE * SLOTS + i;
-    int cur = -1;
-    bool ok = false;
-    for (int k0 = 0; k0 < ne; k0 += 4) {
-        int hh[4];
+    while (sw.k < ne) {
+        int h = 0;
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
-            hh[q] = (k0 + q < ne) ? (k0 == 0 ? first[q] : (int)ep[(k0 + q) * SLOTS]) : -1;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int h = hh[q];
-            if (h < 0) break;
-            const int s = hl.s[h];
-            if (s != cur) {
-                cur = s;
-                ok = nb0 >= sd.rlo[s][0] && nb0 <= sd.rhi[s][0] && nb1 >= sd.rlo[s][1] && nb1 <= sd.rhi[s][1] &&
-                     nb2 >= sd.rlo[s][2] && nb2 <= sd.rhi[s][2] &&
-                     aabb_keep(sd.lo[s], sd.hi[s], x.x, x.y, x.z, P.ra2);
+        for (int q = 0; q < EPRE; ++q)
+            if (sw.k == q) h = pre[q];
+        if (sw.k >= EPRE) h = ep[(size_t)sw.k * SLOTS];
+        const int hp = h - base;
+        if (hp >= HPAGE) break;
+        ++sw.k;
+        const int s = hl.s[hp];
+        if (s != sw.cur) {
+            sw.cur = s;
+            sw.ok = sw.nb0 >= sd.rlo[s][0] && sw.nb0 <= sd.rhi[s][0] && sw.nb1 >= sd.rlo[s][1] &&
+                    sw.nb1 <= sd.rhi[s][1] && sw.nb2 >= sd.rlo[s][2] && sw.nb2 <= sd.rhi[s][2] &&
+                    aabb_keep(sd.lo[s], sd.hi[s], x.x, x.y, x.z, P.ra2);
+        }
+        if (!sw.ok) continue;
+        const float4 xj = hl.x[hp];
+        const float dx = __fsub_rn(x.x, xj.x), dy = __fsub_rn(x.y, xj.y), dz = __fsub_rn(x.z, xj.z);
+        const float r2 = r2_nc(dx, dy, dz);
+        if (r2 > P.ra2) continue;
+        // dissipative pair (non-strict cut-off, src/propagate.cu:641);
+        // velocity differences of floats are exact in FP64
+        const float4 vj = hl.v[hp];
+        const double vx = (double)v.x - vj.x, vy = (double)v.y - vj.y, vz = (double)v.z - vj.z;
+        const double dn = vx * nrm.x + vy * nrm.y + vz * nrm.z;
+        vt.x += vx - dn * nrm.x;
+        vt.y += vy - dn * nrm.y;
+        vt.z += vz - dn * nrm.z;
+        if (MODE == 0) {
+            if (d.record_pairs) {
+                unsigned long long slot = atomicAdd(d.n_pairs, 1ull);
+                const int gj = d.halo[(size_t)a * HMAX + h];
+                if ((long long)slot < d.pair_cap)
+                    d.pairs[slot] = make_int4((a << 8) | i, ((gj / SLOTS) << 8) | (gj % SLOTS), r2 < P.ra2 ? 3 : 2, 0);
             }
-            if (!ok) continue;
-            const float4 xj = hl.x[h];
-            const float dx = __fsub_rn(x.x, xj.x), dy = __fsub_rn(x.y, xj.y), dz = __fsub_rn(x.z, xj.z);
-            const float r2 = r2_nc(dx, dy, dz);
-            if (r2 > P.ra2) continue;
-            // dissipative pair (non-strict cut-off, src/propagate.cu:641);
-            // velocity differences of floats are exact in FP64
-            const float4 vj = hl.v[h];
-            const double vx = (double)v.x - vj.x, vy = (double)v.y - vj.y, vz = (double)v.z - vj.z;
-            const double dn = vx * nrm.x + vy * nrm.y + vz * nrm.z;
-            vt.x += vx - dn * nrm.x;
-            vt.y += vy - dn * nrm.y;
-            vt.z += vz - dn * nrm.z;
-            if (MODE == 0) {
-                if (d.record_pairs) {
-                    unsigned long long slot = atomicAdd(d.n_pairs, 1ull);
-                    const int gj = d.halo[(size_t)a * HMAX + h];
-                    if ((long long)slot < d.pair_cap)
-                        d.pairs[slot] = make_int4((a << 8) | i, ((gj / SLOTS) << 8) | (gj % SLOTS), r2 < P.ra2 ? 3 : 2, 0);
-                }
-                if (r2 < P.ra2) {  // conservative pair (strict cut-off, src/propagate.cu:421)
-                    // distance in FP64: (rr - R) cancels for stiff repulsion
-                    const double R = sqrt_nr((double)dx * dx + (double)dy * dy + (double)dz * dz);
-                    const double iR = rcp_nr(R);
-                    double k = 0.0;
-                    if (R < (double)P.ra) k += -(double)P.asE * ((double)P.ra - R) * iR;
-                    if (R <= (double)P.rr) k += (double)P.rsE * ((double)P.rr - R) * iR;
-                    cf.x += k * dx;
-                    cf.y += k * dy;
-                    cf.z += k * dz;
-                }
+            if (r2 < P.ra2) {  // conservative pair (strict cut-off, src/propagate.cu:421)
+                // distance in FP64: (rr - R) cancels for stiff repulsion
+                const double R = sqrt_nr((double)dx * dx + (double)dy * dy + (double)dz * dz);
+                const double iR = rcp_nr(R);
+                double k = 0.0;
+                if (R < (double)P.ra) k += -(double)P.asE * ((double)P.ra - R) * iR;
+                if (R <= (double)P.rr) k += (double)P.rsE * ((double)P.rr - R) * iR;
+                cf.x += k * dx;
+                cf.y += k * dy;
+                cf.z += k * dz;
             }
         }
     }
@@ -358,10 +379,7 @@ __global__ void k_step_begin(Dev d, int par_next)
         for (int q = 0; q < 3; ++q) {
             st->mm[par_next][2 * q] = f2o(1.0e30f);
             st->mm[par_next][2 * q + 1] = f2o(-1.0e30f);
-            st->bmm[2 * q] = f2o(1.0e30f);
-            st->bmm[2 * q + 1] = f2o(-1.0e30f);
         }
-        st->maxext = 0u;
         if (need) any = 1;
     }
     __syncthreads();
@@ -383,10 +401,7 @@ __global__ void k_init_begin(Dev d)
                 st->mm[p][2 * q + 1] = f2o(-1.0e30f);
             }
         for (int q = 0; q < 3; ++q) {
-            st->bmm[2 * q] = f2o(1.0e30f);
-            st->bmm[2 * q + 1] = f2o(-1.0e30f);
         }
-        st->maxext = 0u;
     }
     if (threadIdx.x == 0) { d.flags[0] = 1; *d.div_total = 0; *d.n_pairs = 0ull; }
 }
@@ -493,7 +508,7 @@ __device__ __noinline__ void cell_volume(const Dev &d, const float4 *xs, float3 
 struct ArmForces {
     double x[NARM], y[NARM], z[NARM];
 };
-static_assert(sizeof(ArmForces) <= 2 * sizeof(float4) * HMAX, "arm forces overlay the halo positions");
+static_assert(sizeof(ArmForces) <= 2 * sizeof(float4) * HPAGE, "arm forces overlay the halo positions");
 
 struct S1Smem {
     float4 xs[SLOTS];
@@ -525,13 +540,13 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
         float4 x4 = make_float4(0, 0, 0, 0), v4 = make_float4(0, 0, 0, 0);
         if (i < NODES) { x4 = d.X[g]; v4 = d.V[g]; }
         const int ne = d.nent[g];
-        int first[4];
+        int pre[EPRE];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) first[q] = d.ent[((size_t)a * MAXE + q) * SLOTS + i];
+        for (int q = 0; q < EPRE; ++q) pre[q] = d.ent[((size_t)a * MAXE + q) * SLOTS + i];
         sm.xs[i] = x4;
         sm.vs[i] = v4;
         int hid[HREG];
-        slots_phase_a(d, a, &d.st[inst], par, sm.sd, sm.hl, nc, nh, hid);
+        slots_phase_a(d, a, &d.st[inst], par, sm.sd, nh, hid);
         __syncthreads();
         slots_boxes(d, P, par, sm.sd, nc);
         const float3 x = f3(x4);
@@ -602,13 +617,21 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
             }
         }
         __syncthreads();  // the arm forces are consumed: gather the halo over them
-        halo_gather(d, sm.hl, hid, d.V);
+        halo_gather(d, a, 0, nh, sm.hl, hid, d.V);
         __syncthreads();
+        const float3 nrm = node_normal(sm.xs, n0, n1, n2, sgn);
+        double3 cf = make_double3(0.0, 0.0, 0.0);
+        double3 vt = make_double3(0.0, 0.0, 0.0);
+        Sweep sw;
+        sweep_init(sw, sm.sd, x);
+        for (int page = 0;; ++page) {
+            if (i < NODES) sweep_page<0>(d, P, sm.sd, sm.hl, a, i, page, x, v, nrm, ne, pre, sw, cf, vt);
+            if ((page + 1) * HPAGE >= nh) break;
+            __syncthreads();
+            halo_gather(d, a, page + 1, nh, sm.hl, hid, d.V);
+            __syncthreads();
+        }
         if (i < NODES) {
-            const float3 nrm = node_normal(sm.xs, n0, n1, n2, sgn);
-            double3 cf = make_double3(0.0, 0.0, 0.0);
-            double3 vt = make_double3(0.0, 0.0, 0.0);
-            contact_sweep<0>(d, P, sm.sd, sm.hl, a, i, x, v, nrm, ne, first, cf, vt);
             FX += cf.x; FY += cf.y; FZ += cf.z;
             // rigid box walls, src/propagate.cu:474-510 (float gap tests)
             if (P.rigid) {
@@ -669,7 +692,7 @@ __device__ __forceinline__ void flush_mm(Dev &d, int inst, int pn, const float *
 }
 
 template <bool DIV>
-__global__ void __launch_bounds__(SLOTS, 5) k_s2(Dev d, int par)
+__global__ void __launch_bounds__(SLOTS, 4) k_s2(Dev d, int par)
 {
     __shared__ S2Smem sm;
     const int W = n_work(d);
@@ -691,23 +714,31 @@ __global__ void __launch_bounds__(SLOTS, 5) k_s2(Dev d, int par)
         float4 x4 = make_float4(0, 0, 0, 0), v4 = make_float4(0, 0, 0, 0);
         if (i < NODES) { x4 = d.X[g]; v4 = d.Vb[g]; }
         const int ne = d.nent[g];
-        int first[4];
+        int pre[EPRE];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) first[q] = d.ent[((size_t)a * MAXE + q) * SLOTS + i];
+        for (int q = 0; q < EPRE; ++q) pre[q] = d.ent[((size_t)a * MAXE + q) * SLOTS + i];
         sm.xs[i] = x4;
         sm.vs[i] = v4;
         int hid[HREG];
-        slots_phase_a(d, a, st, par, sm.sd, sm.hl, nc, nh, hid);
+        slots_phase_a(d, a, st, par, sm.sd, nh, hid);
         __syncthreads();
         slots_boxes(d, P, par, sm.sd, nc);
-        halo_gather(d, sm.hl, hid, d.Vb);
+        halo_gather(d, a, 0, nh, sm.hl, hid, d.Vb);
         __syncthreads();
         const float3 x = f3(x4), v = f3(v4);
+        const float3 nrm = node_normal(sm.xs, n0, n1, n2, sgn);
+        double3 cf = make_double3(0.0, 0.0, 0.0);
+        double3 vt = make_double3(0.0, 0.0, 0.0);
+        Sweep sw;
+        sweep_init(sw, sm.sd, x);
+        for (int page = 0;; ++page) {
+            if (i < NODES) sweep_page<1>(d, P, sm.sd, sm.hl, a, i, page, x, v, nrm, ne, pre, sw, cf, vt);
+            if ((page + 1) * HPAGE >= nh) break;
+            __syncthreads();
+            halo_gather(d, a, page + 1, nh, sm.hl, hid, d.Vb);
+            __syncthreads();
+        }
         if (i < NODES) {
-            const float3 nrm = node_normal(sm.xs, n0, n1, n2, sgn);
-            double3 cf = make_double3(0.0, 0.0, 0.0);
-            double3 vt = make_double3(0.0, 0.0, 0.0);
-            contact_sweep<1>(d, P, sm.sd, sm.hl, a, i, x, v, nrm, ne, first, cf, vt);
             const float3 fd = dis_force(P, sm.vs, n0, n1, n2, v, vt);
             d.FD[g] = make_float4(fd.x, fd.y, fd.z, 0.f);
             d.V[g] = v4;
@@ -980,193 +1011,231 @@ __global__ void k_grid_fix(Dev d, int par)
 }
 
 // ---------------------------------------------------------------------------
-// Neighbour-list build (only for instances whose displacement bound reached
-// the skin, or that divided).  R1: current boxes and build extents.
+// Neighbour-list build (instances whose displacement bound reached the skin,
+// or that divided).  The nodes are binned in cubes of edge hb slightly above
+// the list radius and the bins hashed into hsize buckets; a counting sort
+// puts the positions in bucket order (hpos).  Bucket of bin (ix, iy, iz):
+// the low bits of each coordinate side by side, plus an instance offset, so
+// that the 27 bins around a node fall in 27 distinct buckets and the three
+// bins along x are (unless they wrap) three consecutive buckets.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(SLOTS) k_nl_boxes(Dev d)
+struct BinGeom {
+    float inv;          // 1 / bin edge
+    int bx, by;         // bits of x, y in the bucket number
+    unsigned mask;      // hsize - 1
+    unsigned off;       // instance offset
+};
+
+__device__ __forceinline__ BinGeom bin_geom(const Dev &d, const InstParams &P, int inst)
+{
+    BinGeom b;
+    // bin edge 1% above the list radius: float rounding of x / edge cannot
+    // put two nodes closer than the radius more than one bin apart
+    b.inv = 1.0f / ((P.rlist + 1e-4f) * 1.01f);
+    const int B = 31 - __clz(d.hsize);
+    b.bx = B / 3;
+    b.by = B / 3;
+    b.mask = (unsigned)d.hsize - 1u;
+    b.off = (unsigned)inst * 2654435761u;
+    return b;
+}
+
+__device__ __forceinline__ int bin_coord(float v, float inv)
+{
+    return (int)floorf(fminf(fmaxf(v * inv, -1.0e9f), 1.0e9f));
+}
+
+__device__ __forceinline__ unsigned bucket_of(const BinGeom &b, int ix, int iy, int iz)
+{
+    const unsigned code = ((unsigned)ix & ((1u << b.bx) - 1u)) | (((unsigned)iy & ((1u << b.by) - 1u)) << b.bx) |
+                          ((unsigned)iz << (b.bx + b.by));
+    return (code + b.off) & b.mask;
+}
+
+// Block-wide exclusive scan (NT threads, NT a multiple of 32); wsum[32].
+template <int NT>
+__device__ __forceinline__ int block_excl_scan(int v, int *wsum, int &total)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        int s = lane < NT / 32 ? wsum[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        wsum[lane] = s;
+    }
+    __syncthreads();
+    const int r = (wid > 0 ? wsum[wid - 1] : 0) + x - v;
+    total = wsum[NT / 32 - 1];
+    __syncthreads();
+    return r;
+}
+
+// B1: zero the bucket counts (hsize + SCAN_TILE entries, the tail pads the
+// last scan tile).
+__global__ void k_nh_zero(Dev d)
 {
     if (!d.flags[0]) return;
-    __shared__ float4 xs[SLOTS];
-    __shared__ GeomScratch gs;
+    int4 *p = reinterpret_cast<int4 *>(d.hcount);
+    const int n4 = (d.hsize + SCAN_TILE) / 4;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += gridDim.x * blockDim.x)
+        p[q] = make_int4(0, 0, 0, 0);
+}
+
+// B2: count the nodes of every bucket; each node keeps its rank.
+__global__ void __launch_bounds__(SLOTS) k_nh_count(Dev d)
+{
+    if (!d.flags[0]) return;
     const int W = n_work(d);
     const int i = threadIdx.x;
     for (int w = blockIdx.x; w < W; w += gridDim.x) {
         const int a = cell_of(d, w);
         const int inst = inst_of(d, a);
-        if (!d.st[inst].rebuild) continue;  // uniform across the block
-        xs[i] = (i < NODES) ? d.X[(size_t)a * SLOTS + i] : make_float4(0, 0, 0, 0);
+        if (!d.st[inst].rebuild || i >= NODES) continue;
+        const BinGeom b = bin_geom(d, d.prm[inst], inst);
+        const size_t g = (size_t)a * SLOTS + i;
+        const float4 x = d.X[g];
+        const unsigned k = bucket_of(b, bin_coord(x.x, b.inv), bin_coord(x.y, b.inv), bin_coord(x.z, b.inv));
+        d.node_rank[g] = atomicAdd(&d.hcount[k], 1);
+    }
+}
+
+// B3: sums of the scan tiles.
+__global__ void __launch_bounds__(256) k_nh_scan_tiles(Dev d)
+{
+    if (!d.flags[0]) return;
+    __shared__ int wsum[32];
+    const int ntile = d.hsize / SCAN_TILE + 1;
+    for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
+        const int4 *p = reinterpret_cast<const int4 *>(d.hcount + (size_t)t * SCAN_TILE);
+        int s = 0;
+#pragma unroll
+        for (int q = 0; q < SCAN_TILE / 4 / 256; ++q) {
+            const int4 v = p[threadIdx.x + q * 256];
+            s += v.x + v.y + v.z + v.w;
+        }
+        s = warp_sum(s);
+        if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = s;
         __syncthreads();
-        float3 cm;
-        float4 lo, hi;
-        cell_geom(xs, gs, cm, lo, hi);
-        if (i == 0) {
-            d.aabb_cur[2 * a] = lo;
-            d.aabb_cur[2 * a + 1] = hi;
-            InstState *st = &d.st[inst];
-            atomicMin(&st->bmm[0], f2o(lo.x)); atomicMax(&st->bmm[1], f2o(hi.x));
-            atomicMin(&st->bmm[2], f2o(lo.y)); atomicMax(&st->bmm[3], f2o(hi.y));
-            atomicMin(&st->bmm[4], f2o(lo.z)); atomicMax(&st->bmm[5], f2o(hi.z));
-            float ext = fmaxf(hi.x - lo.x, fmaxf(hi.y - lo.y, hi.z - lo.z));
-            atomicMax(&st->maxext, __float_as_uint(ext));
+        if (threadIdx.x == 0) {
+            int tot = 0;
+            for (int q = 0; q < 8; ++q) tot += wsum[q];
+            d.hscan[t] = tot;
         }
         __syncthreads();
     }
 }
 
-// R2: build-grid geometry per instance and global bin offsets (one thread).
-__global__ void k_nl_grid(Dev d)
-{
-    if (!d.flags[0]) return;
-    if (threadIdx.x != 0) return;
-    int off = 0;
-    for (int k = 0; k < d.n_inst; ++k) {
-        InstState *st = &d.st[k];
-        if (!st->rebuild || st->n == 0) { st->boff = off; st->bdim[0] = st->bdim[1] = st->bdim[2] = 0; continue; }
-        const InstParams &P = d.prm[k];
-        float h = __uint_as_float(st->maxext) + P.rlist + 1e-3f;
-        int nb = 1;
-        for (int q = 0; q < 3; ++q) {
-            float mn = o2f(st->bmm[2 * q]), mx = o2f(st->bmm[2 * q + 1]);
-            float ext = mx - mn;
-            if (ext / h > 1000.0f) h = ext / 1000.0f;
-        }
-        for (int q = 0; q < 3; ++q) {
-            float mn = o2f(st->bmm[2 * q]), mx = o2f(st->bmm[2 * q + 1]);
-            int dim = (int)((mx - mn) / h) + 1;
-            if (dim < 1) dim = 1;
-            st->bdim[q] = dim;
-            st->borg[q] = mn;
-            nb *= dim;
-        }
-        st->bh = h;
-        st->boff = off;
-        off += nb;
-    }
-    if (off > d.bin_cap) {
-        for (int k = 0; k < d.n_inst; ++k)
-            if (d.st[k].rebuild) atomicOr(&d.st[k].err, CS3D_ERRBIT_GRID_OVERFLOW);
-        off = 0;
-        for (int k = 0; k < d.n_inst; ++k) d.st[k].rebuild = 0;
-    }
-    *d.total_bins = off;
-}
-
-__global__ void k_nl_zero(Dev d)
-{
-    if (!d.flags[0]) return;
-    int tb = *d.total_bins;
-    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= tb; b += gridDim.x * blockDim.x) d.bin_count[b] = 0;
-}
-
-__device__ __forceinline__ int build_bin(const InstState *st, float4 lo, float4 hi, int b[3])
-{
-    float c[3] = {0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z)};
-    for (int q = 0; q < 3; ++q) {
-        int v = (int)((c[q] - st->borg[q]) / st->bh);
-        if (v < 0) v = 0;
-        if (v >= st->bdim[q]) v = st->bdim[q] - 1;
-        b[q] = v;
-    }
-    return st->boff + (b[2] * st->bdim[1] + b[1]) * st->bdim[0] + b[0];
-}
-
-__global__ void k_nl_count(Dev d)
-{
-    if (!d.flags[0]) return;
-    const int W = n_work(d);
-    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < W; w += gridDim.x * blockDim.x) {
-        int a = cell_of(d, w);
-        const InstState *st = &d.st[inst_of(d, a)];
-        if (!st->rebuild) continue;
-        int b3[3];
-        int bin = build_bin(st, d.aabb_cur[2 * a], d.aabb_cur[2 * a + 1], b3);
-        d.cell_bin[a] = bin;
-        d.cell_rank[a] = atomicAdd(&d.bin_count[bin], 1);
-    }
-}
-
-// Exclusive scan of bin counts (single block of 1024 threads).
-__global__ void __launch_bounds__(1024) k_nl_scan(Dev d)
+// B4: exclusive scan of the tile sums (one block).
+__global__ void __launch_bounds__(1024) k_nh_scan_top(Dev d)
 {
     if (!d.flags[0]) return;
     __shared__ int wsum[32];
     __shared__ int carry;
-    const int tb = *d.total_bins;
+    const int ntile = d.hsize / SCAN_TILE + 1;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    for (int b0 = 0; b0 < tb; b0 += 1024) {
-        int b = b0 + threadIdx.x;
-        int v = b < tb ? d.bin_count[b] : 0;
-        int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-        int x = v;
-        for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        if (lane == 31) wsum[wid] = x;
+    for (int t0 = 0; t0 < ntile; t0 += 1024) {
+        const int t = t0 + threadIdx.x;
+        const int v = t < ntile ? d.hscan[t] : 0;
+        int tot;
+        const int e = block_excl_scan<1024>(v, wsum, tot);
+        if (t < ntile) d.hscan[t] = carry + e;
         __syncthreads();
-        if (wid == 0) {
-            int s = wsum[lane];
-            for (int o = 1; o < 32; o <<= 1) {
-                int y = __shfl_up_sync(0xffffffffu, s, o);
-                if (lane >= o) s += y;
-            }
-            wsum[lane] = s;
-        }
-        __syncthreads();
-        int excl = carry + (wid > 0 ? wsum[wid - 1] : 0) + x - v;
-        if (b < tb) d.bin_start[b] = excl;
-        __syncthreads();
-        if (threadIdx.x == 0) carry += wsum[31];
+        if (threadIdx.x == 0) carry += tot;
         __syncthreads();
     }
-    if (threadIdx.x == 0) d.bin_start[tb] = carry;
 }
 
-__global__ void k_nl_fill(Dev d)
+// B5: bucket starts (exclusive scan of the counts, in place).
+__global__ void __launch_bounds__(256) k_nh_scan_apply(Dev d)
+{
+    if (!d.flags[0]) return;
+    __shared__ int wsum[32];
+    constexpr int PER = SCAN_TILE / 256;  // 16 consecutive buckets per thread
+    const int ntile = d.hsize / SCAN_TILE + 1;
+    for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
+        int4 *p = reinterpret_cast<int4 *>(d.hcount + (size_t)t * SCAN_TILE + threadIdx.x * PER);
+        int4 v[PER / 4];
+        int s = 0;
+#pragma unroll
+        for (int q = 0; q < PER / 4; ++q) {
+            v[q] = p[q];
+            s += v[q].x + v[q].y + v[q].z + v[q].w;
+        }
+        int tot;
+        int run = d.hscan[t] + block_excl_scan<256>(s, wsum, tot);
+#pragma unroll
+        for (int q = 0; q < PER / 4; ++q) {
+            int4 o;
+            o.x = run; run += v[q].x;
+            o.y = run; run += v[q].y;
+            o.z = run; run += v[q].z;
+            o.w = run; run += v[q].w;
+            p[q] = o;
+        }
+    }
+}
+
+// B6: positions in bucket order.
+__global__ void __launch_bounds__(SLOTS) k_nh_fill(Dev d)
 {
     if (!d.flags[0]) return;
     const int W = n_work(d);
-    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < W; w += gridDim.x * blockDim.x) {
-        int a = cell_of(d, w);
-        if (!d.st[inst_of(d, a)].rebuild) continue;
-        d.bin_cells[d.bin_start[d.cell_bin[a]] + d.cell_rank[a]] = a;
+    const int i = threadIdx.x;
+    for (int w = blockIdx.x; w < W; w += gridDim.x) {
+        const int a = cell_of(d, w);
+        const int inst = inst_of(d, a);
+        if (!d.st[inst].rebuild || i >= NODES) continue;
+        const BinGeom b = bin_geom(d, d.prm[inst], inst);
+        const size_t g = (size_t)a * SLOTS + i;
+        const float4 x = d.X[g];
+        const unsigned k = bucket_of(b, bin_coord(x.x, b.inv), bin_coord(x.y, b.inv), bin_coord(x.z, b.inv));
+        d.hpos[d.hcount[k] + d.node_rank[g]] = make_float4(x.x, x.y, x.z, __int_as_float((int)g));
     }
 }
 
-// Block-wide ordered compaction of flags (192 threads): returns the rank of
-// this thread's element among the set flags and the total.
-__device__ __forceinline__ int block_rank(int flag, int *wcnt, int &total)
-{
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    unsigned b = __ballot_sync(0xffffffffu, flag);
-    if (lane == 0) wcnt[wid] = __popc(b);
-    __syncthreads();
-    int off = 0, tot = 0;
-    for (int q = 0; q < SLOTS / 32; ++q) {
-        if (q < wid) off += wcnt[q];
-        tot += wcnt[q];
-    }
-    total = tot;
-    return off + __popc(b & ((1u << lane) - 1u));
-}
-
-// R7: per cell, the candidate cells (boxes within rlist, ascending id), the
-// halo (nodes of candidate cells within rlist of some node of the cell,
-// ordered by slot then node) and each node's halo indices (ascending).
+// B7: per cell, from the nodes of other cells within the list radius of its
+// nodes: the candidate cells (ascending id), the halo (ordered by candidate
+// slot, then node) and each node's halo indices (ascending).  Candidate
+// cells are first collected in a shared open-addressing set ("temporary
+// slots"), each node's entries kept as (temporary slot, node) and remapped
+// once the slots are sorted.
 struct BuildSmem {
-    float4 xs[SLOTS];
-    float4 cs[SLOTS];
-    int cand[MAXC];
-    float4 clo[MAXC], chi[MAXC];
-    uint8_t near[SLOTS];     // compacted nodes of the candidate near the cell
-    uint8_t mark[SLOTS];
-    uint16_t hmap[SLOTS];
-    int wcnt[SLOTS / 32];
-    int ncand;
+    int tkey[256];           // candidate cell of each temporary slot, -1 if free
+    uint32_t mask[256][6];   // halo nodes of each temporary slot
+    int comp_key[256], comp_t[256];
+    short slot_of_t[256];    // final slot of a temporary slot, -1 if dropped
+    int slot_t[MAXC];        // temporary slot of each final slot
+    int scell[MAXC];         // cell of each final slot
+    int hbase[MAXC];         // first halo index of each final slot
+    int wsum[32];
+    int ncomp;
 };
 
-__global__ void __launch_bounds__(SLOTS) k_nl_build(Dev d)
+__device__ __forceinline__ int halo_index(const BuildSmem &sm, int t, int j)
+{
+    const int s = sm.slot_of_t[t];
+    if (s < 0) return -1;
+    int h = sm.hbase[s];
+    const int wj = j >> 5;
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+        if (k < wj) h += __popc(sm.mask[t][k]);
+    return h + __popc(sm.mask[t][wj] & ((1u << (j & 31)) - 1u));
+}
+
+__global__ void __launch_bounds__(SLOTS) k_nl_cell(Dev d)
 {
     if (!d.flags[0]) return;
     __shared__ BuildSmem sm;
@@ -1178,121 +1247,142 @@ __global__ void __launch_bounds__(SLOTS) k_nl_build(Dev d)
         InstState *st = &d.st[inst];
         if (!st->rebuild) continue;  // uniform across the block
         const InstParams &P = d.prm[inst];
+        const BinGeom b = bin_geom(d, P, inst);
         const float rl = P.rlist + 1e-4f;
         const float rl2 = rl * rl;
-        if (i == 0) sm.ncand = 0;
-        sm.xs[i] = (i < NODES) ? d.X[(size_t)a * SLOTS + i] : make_float4(0, 0, 0, 0);
-        sm.mark[i] = 0;
+        for (int t = i; t < 256; t += SLOTS) sm.tkey[t] = -1;
+        for (int q = i; q < 256 * 6; q += SLOTS) (&sm.mask[0][0])[q] = 0u;
+        if (i == 0) sm.ncomp = 0;
         __syncthreads();
-        const float4 alo = d.aabb_cur[2 * a], ahi = d.aabb_cur[2 * a + 1];
-        if (i < 27) {
-            int b3[3];
-            build_bin(st, alo, ahi, b3);
-            int bx = b3[0] + (i % 3) - 1, by = b3[1] + (i / 3) % 3 - 1, bz = b3[2] + i / 9 - 1;
-            if (bx >= 0 && by >= 0 && bz >= 0 && bx < st->bdim[0] && by < st->bdim[1] && bz < st->bdim[2]) {
-                int bin = st->boff + (bz * st->bdim[1] + by) * st->bdim[0] + bx;
-                for (int q = d.bin_start[bin]; q < d.bin_start[bin + 1]; ++q) {
-                    int c = d.bin_cells[q];
-                    if (c == a) continue;
-                    float4 lo = d.aabb_cur[2 * c], hi = d.aabb_cur[2 * c + 1];
-                    float gx = fmaxf(0.f, fmaxf(lo.x - ahi.x, alo.x - hi.x));
-                    float gy = fmaxf(0.f, fmaxf(lo.y - ahi.y, alo.y - hi.y));
-                    float gz = fmaxf(0.f, fmaxf(lo.z - ahi.z, alo.z - hi.z));
-                    if (gx * gx + gy * gy + gz * gz >= rl2) continue;
-                    int s = atomicAdd(&sm.ncand, 1);
-                    if (s < MAXC) sm.cand[s] = c;
-                }
-            }
-        }
-        __syncthreads();
-        int nc = sm.ncand;
-        if (nc > MAXC) {
-            if (i == 0) atomicOr(&st->err, CS3D_ERRBIT_CAND_OVERFLOW);
-            nc = MAXC;
-        }
-        if (i == 0) {
-            for (int p = 1; p < nc; ++p) {  // ascending cell order, nc <= 32
-                int v = sm.cand[p], q = p - 1;
-                while (q >= 0 && sm.cand[q] > v) { sm.cand[q + 1] = sm.cand[q]; --q; }
-                sm.cand[q + 1] = v;
-            }
-            d.ncand[a] = nc;
-            atomicMax(&st->max_cand, sm.ncand);
-        }
-        __syncthreads();
-        if (i < nc) {
-            d.cand[a * MAXC + i] = sm.cand[i];
-            sm.clo[i] = d.aabb_cur[2 * sm.cand[i]];
-            sm.chi[i] = d.aabb_cur[2 * sm.cand[i] + 1];
-        }
-        __syncthreads();
-        const float3 x = f3(sm.xs[i]);
+        const size_t g = (size_t)a * SLOTS + i;
+        const float4 x = (i < NODES) ? d.X[g] : make_float4(0, 0, 0, 0);
         uint16_t *ep = d.ent + (size_t)a * MAXE * SLOTS + i;
-        int cnt = 0, hbase = 0;
-        bool hover = false;
-        for (int s = 0; s < nc; ++s) {
-            const int c = sm.cand[s];
-            const float4 y4 = (i < NODES) ? d.X[(size_t)c * SLOTS + i] : make_float4(0, 0, 0, 0);
-            sm.cs[i] = y4;
-            // nodes of c within rlist of this cell's box, in ascending order
-            float gx = fmaxf(0.f, fmaxf(alo.x - y4.x, y4.x - ahi.x));
-            float gy = fmaxf(0.f, fmaxf(alo.y - y4.y, y4.y - ahi.y));
-            float gz = fmaxf(0.f, fmaxf(alo.z - y4.z, y4.z - ahi.z));
-            int fl = (i < NODES) && (gx * gx + gy * gy + gz * gz < rl2);
-            int nnear;
-            int r = block_rank(fl, sm.wcnt, nnear);
-            if (fl) sm.near[r] = (uint8_t)i;
-            __syncthreads();
-            const int k_first = cnt;
-            if (i < NODES) {
-                const float4 lo = sm.clo[s], hi = sm.chi[s];
-                float hx = fmaxf(0.f, fmaxf(lo.x - x.x, x.x - hi.x));
-                float hy = fmaxf(0.f, fmaxf(lo.y - x.y, x.y - hi.y));
-                float hz = fmaxf(0.f, fmaxf(lo.z - x.z, x.z - hi.z));
-                if (hx * hx + hy * hy + hz * hz < rl2) {
-                    for (int q = 0; q < nnear; ++q) {
-                        const int j = sm.near[q];
-                        const float4 yj = sm.cs[j];
-                        const float dx = x.x - yj.x, dy = x.y - yj.y, dz = x.z - yj.z;
-                        if (dx * dx + dy * dy + dz * dz < rl2) {
-                            if (cnt < MAXE) ep[(size_t)cnt * SLOTS] = (uint16_t)j;
-                            ++cnt;
-                            sm.mark[j] = 1;
+        int cnt = 0;
+        bool lost = false;
+        if (i < NODES) {
+            const int ix = bin_coord(x.x, b.inv), iy = bin_coord(x.y, b.inv), iz = bin_coord(x.z, b.inv);
+            int last_c = -1, last_t = -1;
+            for (int r = 0; r < 9; ++r) {
+                const int jy = iy + (r % 3) - 1, jz = iz + r / 3 - 1;
+                const unsigned k0 = bucket_of(b, ix - 1, jy, jz);
+                const unsigned k2 = bucket_of(b, ix + 1, jy, jz);
+                // three consecutive buckets unless the x bits or the table wrap
+                const int nrun = (k2 == k0 + 2u) ? 1 : 3;
+                for (int u = 0; u < nrun; ++u) {
+                    unsigned kb, ke;
+                    if (nrun == 1) { kb = k0; ke = k0 + 3u; }
+                    else { kb = bucket_of(b, ix - 1 + u, jy, jz); ke = kb + 1u; }
+                    const int p1 = d.hcount[ke];
+                    for (int p = d.hcount[kb]; p < p1; ++p) {
+                        const float4 y = d.hpos[p];
+                        const int id = __float_as_int(y.w);
+                        const int c = id / SLOTS;
+                        if (c == a) continue;
+                        const float dx = x.x - y.x, dy = x.y - y.y, dz = x.z - y.z;
+                        if (!(dx * dx + dy * dy + dz * dz < rl2)) continue;
+                        if (!d.single && d.cell_inst[c] != inst) continue;
+                        int t = last_t;
+                        if (c != last_c) {
+                            t = -1;
+                            unsigned q = ((unsigned)c * 2654435761u) >> 24;
+                            for (int probe = 0; probe < 256; ++probe, q = (q + 1u) & 255u) {
+                                const int old = atomicCAS(&sm.tkey[q], -1, c);
+                                if (old == -1 || old == c) { t = (int)q; break; }
+                            }
+                            if (t < 0) { lost = true; continue; }
+                            last_c = c;
+                            last_t = t;
                         }
+                        const int j = id - c * SLOTS;
+                        atomicOr(&sm.mask[t][j >> 5], 1u << (j & 31));
+                        if (cnt < MAXE) ep[(size_t)cnt * SLOTS] = (uint16_t)((t << 8) | j);
+                        ++cnt;
                     }
                 }
             }
-            __syncthreads();
-            // halo entries of this slot: marked nodes, ascending
-            const int mk = sm.mark[i];
-            int nmk;
-            const int hr = block_rank(mk, sm.wcnt, nmk);
-            if (mk) {
-                const int h = hbase + hr;
-                sm.hmap[i] = (uint16_t)h;
+        }
+        __syncthreads();
+        for (int t = i; t < 256; t += SLOTS) {
+            const int c = sm.tkey[t];
+            if (c >= 0) {
+                const int q = atomicAdd(&sm.ncomp, 1);
+                sm.comp_key[q] = c;
+                sm.comp_t[q] = t;
+            }
+        }
+        __syncthreads();
+        const int nct = sm.ncomp;
+        for (int q = i; q < nct; q += SLOTS) {
+            const int key = sm.comp_key[q];
+            int r = 0;
+            for (int m = 0; m < nct; ++m) r += sm.comp_key[m] < key;
+            const int t = sm.comp_t[q];
+            sm.slot_of_t[t] = (short)(r < MAXC ? r : -1);
+            if (r < MAXC) {
+                sm.slot_t[r] = t;
+                sm.scell[r] = key;
+                d.cand[(size_t)a * MAXC + r] = key;
+            }
+        }
+        __syncthreads();
+        const int nc = nct < MAXC ? nct : MAXC;
+        int ns = 0;
+        if (i < nc) {
+            const int t = sm.slot_t[i];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) ns += __popc(sm.mask[t][k]);
+        }
+        int nh;
+        const int hb = block_excl_scan<SLOTS>(ns, sm.wsum, nh);
+        if (i < nc) sm.hbase[i] = hb;
+        __syncthreads();
+        // halo: one (slot, 32-node word) per work item
+        for (int e = i; e < nc * 6; e += SLOTS) {
+            const int s = e / 6, k = e - s * 6;
+            const int t = sm.slot_t[s];
+            int h = sm.hbase[s];
+            for (int m = 0; m < k; ++m) h += __popc(sm.mask[t][m]);
+            unsigned bits = sm.mask[t][k];
+            const int c = sm.scell[s];
+            while (bits) {
+                const int j = k * 32 + __ffs(bits) - 1;
+                bits &= bits - 1u;
                 if (h < HMAX) {
-                    d.halo[(size_t)a * HMAX + h] = c * SLOTS + i;
+                    d.halo[(size_t)a * HMAX + h] = c * SLOTS + j;
                     d.halo_slot[(size_t)a * HMAX + h] = (uint8_t)s;
                 }
+                ++h;
             }
-            __syncthreads();
-            for (int k = k_first; k < cnt && k < MAXE; ++k) ep[(size_t)k * SLOTS] = sm.hmap[ep[(size_t)k * SLOTS]];
-            hbase += nmk;
-            if (hbase > HMAX) hover = true;
-            sm.mark[i] = 0;
-            __syncthreads();
         }
+        // entries: temporary (slot, node) -> halo index, ascending
         if (i < NODES) {
+            uint16_t ord[MAXE];
+            int m = 0;
+            const int ne = cnt < MAXE ? cnt : MAXE;
+            for (int k = 0; k < ne; ++k) {
+                const unsigned e = ep[(size_t)k * SLOTS];
+                const int h = halo_index(sm, (int)(e >> 8), (int)(e & 255u));
+                if (h < 0 || h >= HMAX) continue;
+                int pos = m;
+                while (pos > 0 && ord[pos - 1] > h) { ord[pos] = ord[pos - 1]; --pos; }
+                ord[pos] = (uint16_t)h;
+                ++m;
+            }
+            for (int k = 0; k < m; ++k) ep[(size_t)k * SLOTS] = ord[k];
+            d.nent[g] = (uint8_t)m;
+            d.Xb[g] = x;  // reference for the displacement test
             if (cnt > MAXE) atomicOr(&st->err, CS3D_ERRBIT_ENTRY_OVERFLOW);
-            // a halo overflow leaves the cell without contacts (and the error
-            // bit set): its entries would index past the shared halo
-            d.nent[(size_t)a * SLOTS + i] = hover ? (uint8_t)0 : (uint8_t)(cnt < MAXE ? cnt : MAXE);
-            d.Xb[(size_t)a * SLOTS + i] = sm.xs[i];  // reference for the displacement test
+            if (lost) atomicOr(&st->err, CS3D_ERRBIT_CAND_OVERFLOW);
+        } else {
+            d.nent[g] = 0;
         }
         if (i == 0) {
-            if (hover) atomicOr(&st->err, CS3D_ERRBIT_HALO_OVERFLOW);
-            d.halo_n[a] = hbase < HMAX ? hbase : HMAX;
-            atomicMax(&st->max_halo, hbase);
+            if (nct > MAXC) atomicOr(&st->err, CS3D_ERRBIT_CAND_OVERFLOW);
+            if (nh > HMAX) atomicOr(&st->err, CS3D_ERRBIT_HALO_OVERFLOW);
+            d.ncand[a] = nc;
+            d.halo_n[a] = nh < HMAX ? nh : HMAX;
+            atomicMax(&st->max_cand, nct);
+            atomicMax(&st->max_halo, nh);
         }
         int wm = cnt;
         for (int o = 16; o > 0; o >>= 1) wm = max(wm, __shfl_xor_sync(0xffffffffu, wm, o));

@@ -49,9 +49,9 @@ extern "C" {
 #define CS3D_ERRBIT_PAIR_OVERFLOW  0x080u  /* pair-recording buffer full */
 #define CS3D_ERRBIT_HALO_OVERFLOW  0x100u  /* > CS3D_MAX_HALO contact nodes for one cell */
 
-#define CS3D_MAX_CAND      64   /* contact-candidate cells per cell */
-#define CS3D_MAX_ENTRIES   32   /* contact-candidate nodes per node */
-#define CS3D_MAX_HALO    1024   /* distinct contact-candidate nodes per cell */
+#define CS3D_MAX_CAND     128   /* contact-candidate cells per cell */
+#define CS3D_MAX_ENTRIES   64   /* contact-candidate nodes per node */
+#define CS3D_MAX_HALO    4096   /* distinct contact-candidate nodes per cell */
 
 /* ---- parameters of the hot path (one simulation instance) ------------- */
 /* Field meaning and units are the reference's inp.json keys.              */
