@@ -35,6 +35,7 @@ struct cs3d_ctx {
     int grid_flat = 0;             // blocks of the per-thread kernels
     int grid_nodes = 0;            // blocks of the neighbour-list kernels
     int grid_tiles = 0;            // blocks of the bucket scan
+    int grid_s2 = 0;               // blocks of S2 and the integrator
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     float last_ms = 0.f;
@@ -269,14 +270,14 @@ int launch_step(cs3d_ctx *c, int par, bool div, const Prof &pf = Prof())
     const Dev &d = c->d;
     cudaStream_t s = c->stream;
     int n = 0;
-    k_integrate<<<c->grid_cells, SLOTS, 0, s>>>(d); ++n; pf.mark(s, "integrate");
+    k_integrate<<<c->grid_s2, SLOTS, 0, s>>>(d); ++n; pf.mark(s, "integrate");
     k_step_begin<<<1, 256, 0, s>>>(d, par ^ 1); ++n; pf.mark(s, "step_begin");
     int rc = launch_nl_build(c, pf);
     if (rc) return rc;
     n += NL_LAUNCHES;
     k_s1<false><<<c->grid_cells, SLOTS, sizeof(S1Smem), s>>>(d, par); ++n; pf.mark(s, "s1_con_dis");
-    if (div) k_s2<true><<<c->grid_cells, SLOTS, 0, s>>>(d, par);
-    else k_s2<false><<<c->grid_cells, SLOTS, 0, s>>>(d, par);
+    if (div) k_s2<true><<<c->grid_s2, SLOTS, 0, s>>>(d, par);
+    else k_s2<false><<<c->grid_s2, SLOTS, 0, s>>>(d, par);
     ++n; pf.mark(s, "s2_dis_geom");
     if (div) {
         k_div_select<<<c->n_inst, 256, 0, s>>>(d, par); ++n; pf.mark(s, "div_select");
@@ -407,8 +408,7 @@ int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topol
     AL(d.cell_inst, c->cap_total);
     AL(d.work, c->cap_total); AL(d.work_n, 1);
     AL(d.cand, (size_t)c->cap_total * MAXC); AL(d.ncand, c->cap_total);
-    AL(d.halo, (size_t)c->cap_total * HMAX); AL(d.halo_n, c->cap_total);
-    AL(d.halo_slot, (size_t)c->cap_total * HMAX);
+    AL(d.dmask, nodes);
     AL(d.Xb, nodes);
     AL(d.ent, (size_t)c->cap_total * MAXE * SLOTS); AL(d.nent, nodes);
     d.hsize = hash_size(c->cap_total);
@@ -454,6 +454,9 @@ int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topol
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_nl, k_nl_cell, SLOTS, 0);
     c->grid_nodes = std::max(1, std::min(c->cap_total, c->nsm * std::max(occ_nl, 1)));
     c->grid_tiles = std::max(1, std::min(d.hsize / SCAN_TILE + 1, c->nsm * 8));
+    int occ_s2 = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s2, k_s2<true>, SLOTS, 0);
+    c->grid_s2 = std::max(1, std::min(c->cap_total, c->nsm * std::max(occ_s2, 1)));
     *out = c;
     return CS3D_OK;
 }
@@ -876,8 +879,7 @@ struct StaticScratch {
     int hscan[SHASH / SCAN_TILE + 1], node_rank[SCAP * SLOTS];
     int cell_inst[SCAP], work[SCAP], work_n;
     int cand[SCAP * MAXC], ncand[SCAP];
-    int halo[SCAP * HMAX], halo_n[SCAP];
-    uint8_t halo_slot[SCAP * HMAX];
+    unsigned long long dmask[SCAP * SLOTS];
     uint16_t ent[SCAP * MAXE * SLOTS];
     uint8_t nent[SCAP * SLOTS];
     DivEntry divtab[SCAP];
@@ -974,7 +976,7 @@ Dev static_dev(StaticScratch *s)
     d.aabb[0] = s->aabb0; d.aabb[1] = s->aabb1;
     d.cell_inst = s->cell_inst; d.work = s->work; d.work_n = &s->work_n;
     d.cand = s->cand; d.ncand = s->ncand;
-    d.halo = s->halo; d.halo_slot = s->halo_slot; d.halo_n = s->halo_n;
+    d.dmask = s->dmask;
     d.ent = s->ent; d.nent = s->nent;
     d.hsize = SHASH; d.hcount = s->hcount; d.hscan = s->hscan; d.hpos = s->hpos; d.node_rank = s->node_rank;
     d.divtab = s->divtab; d.div_total = &s->div_total;
@@ -1086,7 +1088,6 @@ extern "C" int cs3d_forces_static(const cs3d_params *params, const cs3d_topology
     CK(cudaMemcpyAsync(S->cs0, tt.cs0, sizeof tt.cs0, cudaMemcpyHostToDevice, s));
     // the previous call's neighbour lists, boxes and flags must not leak in
     CK(cudaMemsetAsync(S->ncand, 0, sizeof S->ncand, s));
-    CK(cudaMemsetAsync(S->halo_n, 0, sizeof S->halo_n, s));
     CK(cudaMemsetAsync(S->nent, 0, sizeof S->nent, s));
     CK(cudaMemsetAsync(S->flags, 0, sizeof S->flags, s));
     CK(cudaMemsetAsync(&S->n_events, 0, sizeof S->n_events, s));

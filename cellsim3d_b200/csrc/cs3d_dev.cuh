@@ -12,8 +12,6 @@ constexpr int SLOTS = CS3D_SLOTS;      // node slots per cell (reference padding
 constexpr int NODES = CS3D_NODES;      // real nodes per cell
 constexpr int MAXC = CS3D_MAX_CAND;    // contact-candidate cells per cell
 constexpr int MAXE = CS3D_MAX_ENTRIES; // contact-candidate nodes per node
-constexpr int HMAX = CS3D_MAX_HALO;    // distinct contact-candidate nodes per cell
-constexpr int HPAGE = 1024;            // halo nodes staged in shared memory at a time
 constexpr int SCAN_TILE = 4096;        // elements per block of the bucket scan
 constexpr float DL = 2.9f;             // reference grid spacing, src/GPUbounce.cu:756
 constexpr int NARM = NODES * 3 * 2;    // arm-end forces of the 540 angles
@@ -87,12 +85,13 @@ struct Dev {
     int single;         // one instance with base 0: the work table is the identity
     int *cand;          // [cell*MAXC]
     int *ncand;         // [cell]
-    int *halo;          // [cell*HMAX] global node index (cell*192 + node) of the contact candidates
-    uint8_t *halo_slot; // [cell*HMAX] candidate-cell slot of each halo node
-    int *halo_n;        // [cell]
     float4 *Xb;         // positions at the last neighbour-list build
-    uint16_t *ent;      // [(cell*MAXE + k)*192 + node] halo index
+    // contact candidates of each node: slot << 8 | node, ascending, where
+    // slot indexes the cell's candidate list (cand) and node the node in
+    // that cell
+    uint16_t *ent;      // [(cell*MAXE + k)*192 + node]
     uint8_t *nent;      // [cell*192 + node]
+    unsigned long long *dmask;  // [cell*192 + node] entries that are dissipative pairs this step
     // node-level spatial hash of the neighbour-list build: cubic bins of
     // edge ~rlist hashed (with the instance) into hsize buckets
     int hsize;          // buckets (power of two, >= SCAN_TILE)

@@ -2,20 +2,20 @@
 //
 // One CTA of 192 threads (six warps) owns one cell at a time and walks the
 // active cells grid-stride; thread i owns node i.  The cell's 180 positions
-// and velocities are staged in shared memory together with its "halo": the
-// nodes of neighbouring cells that lie within the neighbour-list radius of
-// any of its nodes, gathered in one round trip per step.  The 540 bond
-// angles are evaluated once each (the reference evaluates every angle twice,
-// from the vertex and from the arm end) and their arm-end forces are
-// gathered from shared memory in the reference's summation order.
+// and velocities are staged in shared memory; the 540 bond angles are
+// evaluated once each (the reference evaluates every angle twice, from the
+// vertex and from the arm end) and their arm-end forces are gathered from
+// shared memory in the reference's summation order.
 //
-// The neighbour list (per cell: candidate cells, halo, per-node halo
-// indices) is rebuilt on the device whenever the accumulated displacement
-// bound reaches the skin, or after a division.  Every step the reference's
-// own contact predicates -- stale grid bin of the node, stale bounding box of
-// the neighbour cell, strict (conservative) and non-strict (dissipative)
+// The neighbour list (per cell: candidate cells; per node: the nodes of
+// candidate cells within the list radius, as slot << 8 | node) is rebuilt
+// on the device whenever the accumulated displacement bound reaches the
+// skin, or after a division.  Every step the reference's own contact
+// predicates -- stale grid bin of the node, stale bounding box of the
+// neighbour cell, strict (conservative) and non-strict (dissipative)
 // cut-offs in float -- are evaluated on every list entry, so the contact
-// pairs are exactly the reference's.
+// pairs are exactly the reference's.  Partner nodes are read straight from
+// global memory: the few hundred partners of a cell stay in L1/L2.
 #pragma once
 #include "cs3d_dev.cuh"
 
@@ -121,25 +121,13 @@ struct SlotData {
     int div[3];
 };
 
-// One page of the halo: positions, velocities and candidate slots of up to
-// HPAGE halo nodes (halo indices [page*HPAGE, page*HPAGE + HPAGE)).
-struct Halo {
-    float4 x[HPAGE];
-    float4 v[HPAGE];
-    uint8_t s[HPAGE];
-};
-
-constexpr int HREG = (HPAGE + SLOTS - 1) / SLOTS;
-
-// Phase A of a cell: candidate cells, stale grid and the node ids of the
-// first halo page (into registers).  Independent loads only, so they overlap
-// with the caller's own-node loads; the caller then calls __syncthreads().
-__device__ __forceinline__ void slots_phase_a(const Dev &d, int a, const InstState *st, int par, SlotData &sd,
-                                              int nh, int (&hid)[HREG])
+// Candidate cells and stale grid of cell a (independent loads only, so they
+// overlap with the caller's own-node loads; a __syncthreads() follows).
+__device__ __forceinline__ void slots_load(const Dev &d, int a, const InstState *st, int par, SlotData &sd)
 {
-    int t = threadIdx.x;
-    // the lists are read in full, whatever their counts, so that no load
-    // waits for another (entries past the counts are never used)
+    const int t = threadIdx.x;
+    // read in full whatever the count, so that no load waits for another
+    // (entries past the count are never used)
     if (t < MAXC) sd.cell[t] = d.cand[(size_t)a * MAXC + t];
     if (t == 0) {
         const int *mm = st->mm[par];
@@ -150,18 +138,9 @@ __device__ __forceinline__ void slots_phase_a(const Dev &d, int a, const InstSta
             sd.div[q] = grid_div(mn, mx);
         }
     }
-#pragma unroll
-    for (int q = 0; q < HREG; ++q) {
-        const int h = t + q * SLOTS;
-        hid[q] = -1;
-        if (h < HPAGE) {
-            const int id = d.halo[(size_t)a * HMAX + h];
-            if (h < nh) hid[q] = id;
-        }
-    }
 }
 
-// Stale boxes / insertion ranges of the candidates (phase A visible before).
+// Stale boxes / insertion ranges of the candidates (slots_load visible).
 __device__ __forceinline__ void slots_boxes(const Dev &d, const InstParams &P, int par, SlotData &sd, int nc)
 {
     int t = threadIdx.x;
@@ -177,108 +156,159 @@ __device__ __forceinline__ void slots_boxes(const Dev &d, const InstParams &P, i
     }
 }
 
-// Gather halo page `page` (positions from X, velocities from Vsrc).  Page 0
-// uses the ids prefetched in phase A.  Needs a __syncthreads() after.
-__device__ __forceinline__ void halo_gather(const Dev &d, int a, int page, int nh, Halo &hl, const int (&hid)[HREG],
-                                            const float4 *__restrict__ Vsrc)
-{
-    const int t = threadIdx.x;
-    const int base = page * HPAGE;
-#pragma unroll
-    for (int q = 0; q < HREG; ++q) {
-        const int h = t + q * SLOTS;
-        if (h >= HPAGE) break;
-        if (base + h >= nh) break;
-        const int id = page == 0 ? hid[q] : d.halo[(size_t)a * HMAX + base + h];
-        hl.s[h] = d.halo_slot[(size_t)a * HMAX + base + h];
-        hl.x[h] = __ldg(&d.X[id]);
-        hl.v[h] = __ldg(&Vsrc[id]);
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Contact sweep of one node over its neighbour-list entries (halo indices,
-// ascending) that fall on the staged halo page.  MODE 0: conservative +
-// dissipative (S1); MODE 1: dissipative only (S2).  The cursor k and the
-// per-slot predicate cache carry over from page to page.
-// ---------------------------------------------------------------------------
-struct Sweep {
-    int k;          // next entry
-    int cur;        // slot of the cached predicate
-    bool ok;        // cached predicate: stale grid bin and stale box test
+// The reference's cell-level contact filter for one node, cached per
+// candidate slot (the entries are sorted by slot): the node's stale grid bin
+// lies in the slot cell's stale insertion range (the cell is in the node's
+// bin list, src/propagatebound.cu:209-256) and the node is within the
+// cut-off of the slot cell's stale box (src/propagate.cu:382-392).
+struct SlotPred {
+    int cur;
+    bool ok;
     int nb0, nb1, nb2;
 };
 
-constexpr int EPRE = 8;  // entries prefetched per node
-
-__device__ __forceinline__ void sweep_init(Sweep &sw, const SlotData &sd, float3 x)
+__device__ __forceinline__ void pred_init(SlotPred &sp, const SlotData &sd, float3 x)
 {
-    sw.k = 0;
-    sw.cur = -1;
-    sw.ok = false;
-    sw.nb0 = node_bin_axis(x.x, sd.mn[0], sd.div[0]);
-    sw.nb1 = node_bin_axis(x.y, sd.mn[1], sd.div[1]);
-    sw.nb2 = node_bin_axis(x.z, sd.mn[2], sd.div[2]);
+    sp.cur = -1;
+    sp.ok = false;
+    sp.nb0 = node_bin_axis(x.x, sd.mn[0], sd.div[0]);
+    sp.nb1 = node_bin_axis(x.y, sd.mn[1], sd.div[1]);
+    sp.nb2 = node_bin_axis(x.z, sd.mn[2], sd.div[2]);
 }
 
-template <int MODE>
-__device__ __forceinline__ void sweep_page(const Dev &d, const InstParams &P, const SlotData &sd, const Halo &hl,
-                                           int a, int i, int page, float3 x, float3 v, float3 nrm, int ne,
-                                           const int (&pre)[EPRE], Sweep &sw, double3 &cf, double3 &vt)
+__device__ __forceinline__ bool pred_ok(SlotPred &sp, const SlotData &sd, const InstParams &P, float3 x, int s)
 {
-    const int base = page * HPAGE;
-    const uint16_t *ep = d.ent + (size_t)a * MAXE * SLOTS + i;
-    while (sw.k < ne) {
-        int h = 0;
+    if (s != sp.cur) {
+        sp.cur = s;
+        sp.ok = sp.nb0 >= sd.rlo[s][0] && sp.nb0 <= sd.rhi[s][0] && sp.nb1 >= sd.rlo[s][1] &&
+                sp.nb1 <= sd.rhi[s][1] && sp.nb2 >= sd.rlo[s][2] && sp.nb2 <= sd.rhi[s][2] &&
+                aabb_keep(sd.lo[s], sd.hi[s], x.x, x.y, x.z, P.ra2);
+    }
+    return sp.ok;
+}
+
+constexpr int EPRE = 8;  // entries prefetched per node at the start of a cell
+constexpr int SB = 4;    // entries whose partner loads are in flight together
+
+// Entry k of a node: from the prefetched words (two entries each) or global.
+__device__ __forceinline__ unsigned entry_at(const uint16_t *ep, const uint32_t (&pre)[EPRE / 2], int k)
+{
+    if (k >= EPRE) return ep[(size_t)k * SLOTS];
+    uint32_t w = 0;
 #pragma unroll
-        for (int q = 0; q < EPRE; ++q)
-            if (sw.k == q) h = pre[q];
-        if (sw.k >= EPRE) h = ep[(size_t)sw.k * SLOTS];
-        const int hp = h - base;
-        if (hp >= HPAGE) break;
-        ++sw.k;
-        const int s = hl.s[hp];
-        if (s != sw.cur) {
-            sw.cur = s;
-            sw.ok = sw.nb0 >= sd.rlo[s][0] && sw.nb0 <= sd.rhi[s][0] && sw.nb1 >= sd.rlo[s][1] &&
-                    sw.nb1 <= sd.rhi[s][1] && sw.nb2 >= sd.rlo[s][2] && sw.nb2 <= sd.rhi[s][2] &&
-                    aabb_keep(sd.lo[s], sd.hi[s], x.x, x.y, x.z, P.ra2);
+    for (int r = 0; r < EPRE / 2; ++r)
+        if ((k >> 1) == r) w = pre[r];
+    return (k & 1) ? (w >> 16) : (w & 0xffffu);
+}
+
+// ---------------------------------------------------------------------------
+// S1 contact sweep of node i over its entries: conservative contact force
+// (strict cut-off, src/propagate.cu:406-442) added to F, tangential
+// velocity sum of the dissipative pairs (non-strict cut-off,
+// src/propagate.cu:600-656) in vt.  Returns the mask of the entries that are
+// dissipative pairs (positions do not change before S2, so S2 reuses it).
+// Partner positions and velocities are read from global memory (L1/L2
+// resident: the partners of a cell are a few hundred nodes).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long sweep_s1(const Dev &d, const InstParams &P, const SlotData &sd, int a,
+                                                       int i, float3 x, float3 v, float3 nrm, int ne,
+                                                       const uint32_t (&pre)[EPRE / 2], double &FX, double &FY,
+                                                       double &FZ, double3 &vt)
+{
+    const uint16_t *ep = d.ent + (size_t)a * MAXE * SLOTS + i;
+    SlotPred sp;
+    pred_init(sp, sd, x);
+    unsigned long long dm = 0ull;
+    for (int k0 = 0; k0 < ne; k0 += SB) {
+        unsigned e[SB];
+#pragma unroll
+        for (int q = 0; q < SB; ++q) e[q] = (k0 + q < ne) ? entry_at(ep, pre, k0 + q) : 0xffffu;
+        int id[SB];
+#pragma unroll
+        for (int q = 0; q < SB; ++q) {
+            id[q] = -1;
+            if (e[q] != 0xffffu && pred_ok(sp, sd, P, x, (int)(e[q] >> 8)))
+                id[q] = sd.cell[e[q] >> 8] * SLOTS + (int)(e[q] & 255u);
         }
-        if (!sw.ok) continue;
-        const float4 xj = hl.x[hp];
-        const float dx = __fsub_rn(x.x, xj.x), dy = __fsub_rn(x.y, xj.y), dz = __fsub_rn(x.z, xj.z);
-        const float r2 = r2_nc(dx, dy, dz);
-        if (r2 > P.ra2) continue;
-        // dissipative pair (non-strict cut-off, src/propagate.cu:641);
-        // velocity differences of floats are exact in FP64
-        const float4 vj = hl.v[hp];
-        const double vx = (double)v.x - vj.x, vy = (double)v.y - vj.y, vz = (double)v.z - vj.z;
-        const double dn = vx * nrm.x + vy * nrm.y + vz * nrm.z;
-        vt.x += vx - dn * nrm.x;
-        vt.y += vy - dn * nrm.y;
-        vt.z += vz - dn * nrm.z;
-        if (MODE == 0) {
+        float4 xj[SB];
+#pragma unroll
+        for (int q = 0; q < SB; ++q) xj[q] = id[q] >= 0 ? __ldg(&d.X[id[q]]) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int q = 0; q < SB; ++q) {
+            if (id[q] < 0) continue;
+            const float dx = __fsub_rn(x.x, xj[q].x), dy = __fsub_rn(x.y, xj[q].y), dz = __fsub_rn(x.z, xj[q].z);
+            const float r2 = r2_nc(dx, dy, dz);
+            if (r2 > P.ra2) { id[q] = -1; continue; }
+            dm |= 1ull << (k0 + q);
             if (d.record_pairs) {
-                unsigned long long slot = atomicAdd(d.n_pairs, 1ull);
-                const int gj = d.halo[(size_t)a * HMAX + h];
+                const unsigned long long slot = atomicAdd(d.n_pairs, 1ull);
                 if ((long long)slot < d.pair_cap)
-                    d.pairs[slot] = make_int4((a << 8) | i, ((gj / SLOTS) << 8) | (gj % SLOTS), r2 < P.ra2 ? 3 : 2, 0);
+                    d.pairs[slot] = make_int4((a << 8) | i, ((id[q] / SLOTS) << 8) | (id[q] % SLOTS),
+                                              r2 < P.ra2 ? 3 : 2, 0);
             }
-            if (r2 < P.ra2) {  // conservative pair (strict cut-off, src/propagate.cu:421)
+            if (r2 < P.ra2) {
                 // distance in FP64: (rr - R) cancels for stiff repulsion
                 const double R = sqrt_nr((double)dx * dx + (double)dy * dy + (double)dz * dz);
                 const double iR = rcp_nr(R);
                 double k = 0.0;
                 if (R < (double)P.ra) k += -(double)P.asE * ((double)P.ra - R) * iR;
                 if (R <= (double)P.rr) k += (double)P.rsE * ((double)P.rr - R) * iR;
-                cf.x += k * dx;
-                cf.y += k * dy;
-                cf.z += k * dz;
+                FX += k * dx;
+                FY += k * dy;
+                FZ += k * dz;
             }
         }
+        float4 vj[SB];
+#pragma unroll
+        for (int q = 0; q < SB; ++q) vj[q] = id[q] >= 0 ? __ldg(&d.V[id[q]]) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int q = 0; q < SB; ++q) {
+            if (id[q] < 0) continue;
+            // velocity differences of floats are exact in FP64
+            const double vx = (double)v.x - vj[q].x, vy = (double)v.y - vj[q].y, vz = (double)v.z - vj[q].z;
+            const double dn = vx * nrm.x + vy * nrm.y + vz * nrm.z;
+            vt.x += vx - dn * nrm.x;
+            vt.y += vy - dn * nrm.y;
+            vt.z += vz - dn * nrm.z;
+        }
     }
+    return dm;
 }
 
+// S2 sweep: tangential velocity sum over the dissipative pairs found by S1,
+// with the velocities after the half kicks.
+__device__ __forceinline__ double3 sweep_s2(const Dev &d, const int *cell, int a, int i, float3 v, float3 nrm,
+                                            unsigned long long dm)
+{
+    const uint16_t *ep = d.ent + (size_t)a * MAXE * SLOTS + i;
+    double3 vt = make_double3(0.0, 0.0, 0.0);
+    while (dm) {
+        int id[SB];
+#pragma unroll
+        for (int q = 0; q < SB; ++q) {
+            id[q] = -1;
+            if (dm) {
+                const int k = __ffsll((long long)dm) - 1;
+                dm &= dm - 1ull;
+                const unsigned e = ep[(size_t)k * SLOTS];
+                id[q] = cell[e >> 8] * SLOTS + (int)(e & 255u);
+            }
+        }
+        float4 vj[SB];
+#pragma unroll
+        for (int q = 0; q < SB; ++q) vj[q] = id[q] >= 0 ? __ldg(&d.Vb[id[q]]) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int q = 0; q < SB; ++q) {
+            if (id[q] < 0) continue;
+            const double vx = (double)v.x - vj[q].x, vy = (double)v.y - vj[q].y, vz = (double)v.z - vj[q].z;
+            const double dn = vx * nrm.x + vy * nrm.y + vz * nrm.z;
+            vt.x += vx - dn * nrm.x;
+            vt.y += vy - dn * nrm.y;
+            vt.z += vz - dn * nrm.z;
+        }
+    }
+    return vt;
+}
 // Unit surface normal of node i for the tangential friction,
 // src/propagate.cu:558-572.
 __device__ __forceinline__ float3 node_normal(const float4 *xs, int n0, int n1, int n2, float sgn)
@@ -503,21 +533,15 @@ __device__ __noinline__ void cell_volume(const Dev &d, const float4 *xs, float3 
 // INIT = true evaluates the initial forces of src/GPUbounce.cu:978-1004
 // (no velocity update; Fd written to FD).
 // ---------------------------------------------------------------------------
-// The arm forces are consumed before the halo is gathered, so they share
-// the halo's position/velocity storage (its slot array stays separate).
 struct ArmForces {
     double x[NARM], y[NARM], z[NARM];
 };
-static_assert(sizeof(ArmForces) <= 2 * sizeof(float4) * HPAGE, "arm forces overlay the halo positions");
 
 struct S1Smem {
     float4 xs[SLOTS];
     float4 vs[SLOTS];
     SlotData sd;
-    union {
-        Halo hl;
-        ArmForces arm;
-    };
+    ArmForces arm;
 };
 
 template <bool INIT>
@@ -536,17 +560,17 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
         const InstParams &P = d.prm[inst];
         const size_t g = (size_t)a * SLOTS + i;
         const int nc = d.ncand[a];
-        const int nh = d.halo_n[a];
         float4 x4 = make_float4(0, 0, 0, 0), v4 = make_float4(0, 0, 0, 0);
         if (i < NODES) { x4 = d.X[g]; v4 = d.V[g]; }
         const int ne = d.nent[g];
-        int pre[EPRE];
+        uint32_t pre[EPRE / 2];
 #pragma unroll
-        for (int q = 0; q < EPRE; ++q) pre[q] = d.ent[((size_t)a * MAXE + q) * SLOTS + i];
+        for (int q = 0; q < EPRE / 2; ++q)
+            pre[q] = (uint32_t)d.ent[((size_t)a * MAXE + 2 * q) * SLOTS + i] |
+                     ((uint32_t)d.ent[((size_t)a * MAXE + 2 * q + 1) * SLOTS + i] << 16);
         sm.xs[i] = x4;
         sm.vs[i] = v4;
-        int hid[HREG];
-        slots_phase_a(d, a, &d.st[inst], par, sm.sd, nh, hid);
+        slots_load(d, a, &d.st[inst], par, sm.sd);
         __syncthreads();
         slots_boxes(d, P, par, sm.sd, nc);
         const float3 x = f3(x4);
@@ -572,12 +596,12 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
             sm.arm.x[o + 5] = Fq.x; sm.arm.y[o + 5] = Fq.y; sm.arm.z[o + 5] = Fq.z;
         }
         __syncthreads();
-        // The node force is accumulated in FP64: its terms (pressure up to
-        // ~1e3, stiff contact repulsion up to ~1e4) can cancel to a net force
-        // orders of magnitude smaller, and the sum is rounded to float once,
-        // as the reference stores it.
-        double FX = 0.0, FY = 0.0, FZ = 0.0;
         if (i < NODES) {
+            // The node force is accumulated in FP64: its terms (pressure up
+            // to ~1e3, stiff contact repulsion up to ~1e4) can cancel to a
+            // net force orders of magnitude smaller, and the sum is rounded to
+            // float once, as the reference stores it.
+            double FX = 0.0, FY = 0.0, FZ = 0.0;
             if (isnan(x.x) || isnan(x.y) || isnan(x.z)) atomic_or_err(&d.st[inst], CS3D_ERRBIT_NAN);
             // springs, src/propagate.cu:298-314
             const double stiff = d.E[a];
@@ -615,24 +639,10 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
                 for (int q = 0; q < 6; ++q) { ax += sm.arm.x[idx[q]]; ay += sm.arm.y[idx[q]]; az += sm.arm.z[idx[q]]; }
                 FX += ax; FY += ay; FZ += az;
             }
-        }
-        __syncthreads();  // the arm forces are consumed: gather the halo over them
-        halo_gather(d, a, 0, nh, sm.hl, hid, d.V);
-        __syncthreads();
-        const float3 nrm = node_normal(sm.xs, n0, n1, n2, sgn);
-        double3 cf = make_double3(0.0, 0.0, 0.0);
-        double3 vt = make_double3(0.0, 0.0, 0.0);
-        Sweep sw;
-        sweep_init(sw, sm.sd, x);
-        for (int page = 0;; ++page) {
-            if (i < NODES) sweep_page<0>(d, P, sm.sd, sm.hl, a, i, page, x, v, nrm, ne, pre, sw, cf, vt);
-            if ((page + 1) * HPAGE >= nh) break;
-            __syncthreads();
-            halo_gather(d, a, page + 1, nh, sm.hl, hid, d.V);
-            __syncthreads();
-        }
-        if (i < NODES) {
-            FX += cf.x; FY += cf.y; FZ += cf.z;
+            // contacts, src/propagate.cu:356-442 and the first dissipative sweep
+            const float3 nrm = node_normal(sm.xs, n0, n1, n2, sgn);
+            double3 vt = make_double3(0.0, 0.0, 0.0);
+            const unsigned long long dm = sweep_s1(d, P, sm.sd, a, i, x, v, nrm, ne, pre, FX, FY, FZ, vt);
             // rigid box walls, src/propagate.cu:474-510 (float gap tests)
             if (P.rigid) {
                 const double wk = P.wallk, th = P.thresh;
@@ -648,6 +658,7 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
             }
             const float3 fd = dis_force(P, sm.vs, n0, n1, n2, v, vt);
             d.FC[g] = make_float4((float)FX, (float)FY, (float)FZ, 0.f);
+            d.dmask[g] = dm;
             if (INIT) {
                 d.FD[g] = make_float4(fd.x, fd.y, fd.z, 0.f);
             } else {
@@ -672,13 +683,12 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
 // S2: second dissipative force with the updated velocities
 // (src/GPUbounce.cu:1151), centre of mass (:1164), volumes and division
 // flags (:1172, DIV only), bounding boxes and grid extents for the next step
-// (:1312-1334).
+// (:1312-1334).  The dissipative pairs are those S1 found (same positions).
 // ---------------------------------------------------------------------------
 struct S2Smem {
     float4 xs[SLOTS];
     float4 vs[SLOTS];
-    SlotData sd;
-    Halo hl;
+    int cell[MAXC];
     GeomScratch gs;
 };
 
@@ -692,7 +702,7 @@ __device__ __forceinline__ void flush_mm(Dev &d, int inst, int pn, const float *
 }
 
 template <bool DIV>
-__global__ void __launch_bounds__(SLOTS, 4) k_s2(Dev d, int par)
+__global__ void __launch_bounds__(SLOTS, 5) k_s2(Dev d, int par)
 {
     __shared__ S2Smem sm;
     const int W = n_work(d);
@@ -709,36 +719,17 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s2(Dev d, int par)
         const InstParams &P = d.prm[inst];
         InstState *st = &d.st[inst];
         const size_t g = (size_t)a * SLOTS + i;
-        const int nc = d.ncand[a];
-        const int nh = d.halo_n[a];
         float4 x4 = make_float4(0, 0, 0, 0), v4 = make_float4(0, 0, 0, 0);
-        if (i < NODES) { x4 = d.X[g]; v4 = d.Vb[g]; }
-        const int ne = d.nent[g];
-        int pre[EPRE];
-#pragma unroll
-        for (int q = 0; q < EPRE; ++q) pre[q] = d.ent[((size_t)a * MAXE + q) * SLOTS + i];
+        unsigned long long dm = 0ull;
+        if (i < NODES) { x4 = d.X[g]; v4 = d.Vb[g]; dm = d.dmask[g]; }
+        if (i < MAXC) sm.cell[i] = d.cand[(size_t)a * MAXC + i];
         sm.xs[i] = x4;
         sm.vs[i] = v4;
-        int hid[HREG];
-        slots_phase_a(d, a, st, par, sm.sd, nh, hid);
         __syncthreads();
-        slots_boxes(d, P, par, sm.sd, nc);
-        halo_gather(d, a, 0, nh, sm.hl, hid, d.Vb);
-        __syncthreads();
-        const float3 x = f3(x4), v = f3(v4);
-        const float3 nrm = node_normal(sm.xs, n0, n1, n2, sgn);
-        double3 cf = make_double3(0.0, 0.0, 0.0);
-        double3 vt = make_double3(0.0, 0.0, 0.0);
-        Sweep sw;
-        sweep_init(sw, sm.sd, x);
-        for (int page = 0;; ++page) {
-            if (i < NODES) sweep_page<1>(d, P, sm.sd, sm.hl, a, i, page, x, v, nrm, ne, pre, sw, cf, vt);
-            if ((page + 1) * HPAGE >= nh) break;
-            __syncthreads();
-            halo_gather(d, a, page + 1, nh, sm.hl, hid, d.Vb);
-            __syncthreads();
-        }
         if (i < NODES) {
+            const float3 v = f3(v4);
+            const float3 nrm = node_normal(sm.xs, n0, n1, n2, sgn);
+            const double3 vt = sweep_s2(d, sm.cell, a, i, v, nrm, dm);
             const float3 fd = dis_force(P, sm.vs, n0, n1, n2, v, vt);
             d.FD[g] = make_float4(fd.x, fd.y, fd.z, 0.f);
             d.V[g] = v4;
@@ -782,7 +773,6 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s2(Dev d, int par)
     }
     if (threadIdx.x == 0 && acc_inst >= 0) flush_mm(d, acc_inst, pn, acc);
 }
-
 // Centre of mass, bounding boxes and grid extents only (initialisation,
 // src/GPUbounce.cu:739-763).
 __global__ void __launch_bounds__(SLOTS) k_geom(Dev d, int par)
@@ -1206,34 +1196,20 @@ __global__ void __launch_bounds__(SLOTS) k_nh_fill(Dev d)
 }
 
 // B7: per cell, from the nodes of other cells within the list radius of its
-// nodes: the candidate cells (ascending id), the halo (ordered by candidate
-// slot, then node) and each node's halo indices (ascending).  Candidate
+// nodes: the candidate cells (ascending id) and each node's entries
+// (slot << 8 | node, ascending: by candidate cell, then node).  Candidate
 // cells are first collected in a shared open-addressing set ("temporary
 // slots"), each node's entries kept as (temporary slot, node) and remapped
 // once the slots are sorted.
 struct BuildSmem {
     int tkey[256];           // candidate cell of each temporary slot, -1 if free
-    uint32_t mask[256][6];   // halo nodes of each temporary slot
+    uint32_t mask[256][6];   // partner nodes of each temporary slot
     int comp_key[256], comp_t[256];
     short slot_of_t[256];    // final slot of a temporary slot, -1 if dropped
     int slot_t[MAXC];        // temporary slot of each final slot
-    int scell[MAXC];         // cell of each final slot
-    int hbase[MAXC];         // first halo index of each final slot
     int wsum[32];
     int ncomp;
 };
-
-__device__ __forceinline__ int halo_index(const BuildSmem &sm, int t, int j)
-{
-    const int s = sm.slot_of_t[t];
-    if (s < 0) return -1;
-    int h = sm.hbase[s];
-    const int wj = j >> 5;
-#pragma unroll
-    for (int k = 0; k < 6; ++k)
-        if (k < wj) h += __popc(sm.mask[t][k]);
-    return h + __popc(sm.mask[t][wj] & ((1u << (j & 31)) - 1u));
-}
 
 __global__ void __launch_bounds__(SLOTS) k_nl_cell(Dev d)
 {
@@ -1320,12 +1296,12 @@ __global__ void __launch_bounds__(SLOTS) k_nl_cell(Dev d)
             sm.slot_of_t[t] = (short)(r < MAXC ? r : -1);
             if (r < MAXC) {
                 sm.slot_t[r] = t;
-                sm.scell[r] = key;
                 d.cand[(size_t)a * MAXC + r] = key;
             }
         }
         __syncthreads();
         const int nc = nct < MAXC ? nct : MAXC;
+        // distinct partner nodes of the cell (statistics only)
         int ns = 0;
         if (i < nc) {
             const int t = sm.slot_t[i];
@@ -1333,36 +1309,17 @@ __global__ void __launch_bounds__(SLOTS) k_nl_cell(Dev d)
             for (int k = 0; k < 6; ++k) ns += __popc(sm.mask[t][k]);
         }
         int nh;
-        const int hb = block_excl_scan<SLOTS>(ns, sm.wsum, nh);
-        if (i < nc) sm.hbase[i] = hb;
-        __syncthreads();
-        // halo: one (slot, 32-node word) per work item
-        for (int e = i; e < nc * 6; e += SLOTS) {
-            const int s = e / 6, k = e - s * 6;
-            const int t = sm.slot_t[s];
-            int h = sm.hbase[s];
-            for (int m = 0; m < k; ++m) h += __popc(sm.mask[t][m]);
-            unsigned bits = sm.mask[t][k];
-            const int c = sm.scell[s];
-            while (bits) {
-                const int j = k * 32 + __ffs(bits) - 1;
-                bits &= bits - 1u;
-                if (h < HMAX) {
-                    d.halo[(size_t)a * HMAX + h] = c * SLOTS + j;
-                    d.halo_slot[(size_t)a * HMAX + h] = (uint8_t)s;
-                }
-                ++h;
-            }
-        }
-        // entries: temporary (slot, node) -> halo index, ascending
+        block_excl_scan<SLOTS>(ns, sm.wsum, nh);
+        // entries: (temporary slot, node) -> (slot, node), ascending
         if (i < NODES) {
             uint16_t ord[MAXE];
             int m = 0;
             const int ne = cnt < MAXE ? cnt : MAXE;
             for (int k = 0; k < ne; ++k) {
                 const unsigned e = ep[(size_t)k * SLOTS];
-                const int h = halo_index(sm, (int)(e >> 8), (int)(e & 255u));
-                if (h < 0 || h >= HMAX) continue;
+                const int s = sm.slot_of_t[e >> 8];
+                if (s < 0) continue;
+                const unsigned h = ((unsigned)s << 8) | (e & 255u);
                 int pos = m;
                 while (pos > 0 && ord[pos - 1] > h) { ord[pos] = ord[pos - 1]; --pos; }
                 ord[pos] = (uint16_t)h;
@@ -1378,9 +1335,7 @@ __global__ void __launch_bounds__(SLOTS) k_nl_cell(Dev d)
         }
         if (i == 0) {
             if (nct > MAXC) atomicOr(&st->err, CS3D_ERRBIT_CAND_OVERFLOW);
-            if (nh > HMAX) atomicOr(&st->err, CS3D_ERRBIT_HALO_OVERFLOW);
             d.ncand[a] = nc;
-            d.halo_n[a] = nh < HMAX ? nh : HMAX;
             atomicMax(&st->max_cand, nct);
             atomicMax(&st->max_halo, nh);
         }

@@ -45,13 +45,12 @@ extern "C" {
 #define CS3D_ERRBIT_ENTRY_OVERFLOW 0x008u  /* > CS3D_MAX_ENTRIES contact nodes for one node */
 #define CS3D_ERRBIT_NONFINITE_VOL  0x010u  /* src/volume.cu:134-139 */
 #define CS3D_ERRBIT_BAD_NORMAL     0x020u  /* |n| != 1, src/postscriptinit.cu:215-219 */
-#define CS3D_ERRBIT_GRID_OVERFLOW  0x040u  /* rebuild grid larger than its buffer */
+#define CS3D_ERRBIT_GRID_OVERFLOW  0x040u  /* reserved, never raised (the node hash cannot overflow) */
 #define CS3D_ERRBIT_PAIR_OVERFLOW  0x080u  /* pair-recording buffer full */
-#define CS3D_ERRBIT_HALO_OVERFLOW  0x100u  /* > CS3D_MAX_HALO contact nodes for one cell */
+#define CS3D_ERRBIT_HALO_OVERFLOW  0x100u  /* reserved, never raised */
 
 #define CS3D_MAX_CAND     128   /* contact-candidate cells per cell */
 #define CS3D_MAX_ENTRIES   64   /* contact-candidate nodes per node */
-#define CS3D_MAX_HALO    4096   /* distinct contact-candidate nodes per cell */
 
 /* ---- parameters of the hot path (one simulation instance) ------------- */
 /* Field meaning and units are the reference's inp.json keys.              */
@@ -270,7 +269,7 @@ int cs3d_last_error(cs3d_ctx *ctx, int inst, uint32_t *bits);
 
 /* Counters: [0] steps, [1] neighbour-list rebuilds, [2] max entries per node
  * seen, [3] max candidate cells per cell seen, [4] kernel launches per step,
- * [5] max halo nodes per cell seen. */
+ * [5] max distinct contact-candidate nodes (of other cells) per cell seen. */
 int cs3d_get_stats(cs3d_ctx *ctx, long long *stats, int n);
 
 /* Profiling pass: n_steps steps launched kernel by kernel (not as a graph)
