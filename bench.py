@@ -13,9 +13,10 @@ One "step" is one full timestep of the reference's loop
 --impl cs3d (default): the CUDA path through libcs3d.so.  Under torchrun
 each rank steps its own replica (the single-system path does not shard;
 ensembles shard by instance), timed with CUDA events, max over ranks.
---impl reference: the reference has no CPU implementation; its FP64 CPU
-restatement (the oracle, OpenMP over cells, all host threads) steps a bounded
-sample of the same workload on rank 0.
+--impl reference: the reference has no CPU implementation of the timestep;
+its own CUDA kernels, compiled unmodified for sm_100a (oracle/ref.mk) and
+driven through its step sequence, step the same workload on rank 0's GPU.
+Without that build the FP64 oracle port steps a bounded sample on the host.
 """
 import argparse
 import json
@@ -270,6 +271,63 @@ def cpu_baseline(args, steps=None, cells=None):
                       % (steps, st["n"], os.cpu_count())}
 
 
+def run_reference(args):
+    """The reference arm.  The reference has no CPU implementation of the
+    timestep: its own CUDA kernels, compiled unmodified for sm_100a from the
+    reference sources (oracle/ref.mk) and driven through the reference's step
+    sequence (oracle/ref_harness.cu), step the same workload on this GPU.
+    Without that build, the FP64 oracle port steps a bounded sample on the
+    host cores instead."""
+    from oracle import ref
+    line = {"impl": "reference", "metric": "node-steps/s (cells x 180 x steps / s)", "unit": "node-steps/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "data": "synthetic (seeded generator, cellsim3d_b200/workloads.py)"}
+    if not ref.available():
+        base = cpu_baseline(args, steps=max(1, min(args.steps, args.cpu_steps)))
+        line.update({"value": base["value"], "dtype": "f64", "config": {"workload": args.workload, "cells": args.cpu_cells},
+                     "cpu_baseline": base,
+                     "e2e": {"value": base["value"], "unit": "node-steps/s", "h2d_bytes_per_step": 0,
+                             "d2h_bytes_per_step": 0}})
+        return line
+    import cellsim3d_b200 as cs
+    insts = build_workload(args.workload, args.cells)
+    topo = make_topology(insts)
+    total_ms, node_steps, cells0 = 0.0, 0.0, 0
+    statuses, max_bin, max_nn, guard = set(), 0, 0, 0.0
+    with ClockSampler(0) as clk:
+        for p, st, cap in insts:
+            r = ref.run(cs.make_params(p), topo, st, cap, args.warmup + args.steps, warmup=args.warmup)
+            timed = r["steps"] - args.warmup
+            if timed <= 0:
+                raise RuntimeError("reference stopped in the warm-up: " + r["status_text"])
+            ms = r["total_ms"] - r["guard_ms"]
+            total_ms += ms
+            node_steps += 0.5 * (st["n"] + r["n"]) * 180 * timed   # cell count grows by division
+            cells0 += st["n"]
+            statuses.add(r["status_text"])
+            max_bin, max_nn = max(max_bin, r["max_bin"]), max(max_nn, r["max_local_nn"])
+            guard += r["guard_ms"]
+    value = node_steps / (total_ms * 1e-3)
+    line.update({
+        "value": value, "ms_per_step": total_ms / args.steps, "dtype": "f32",
+        "config": {"workload": args.workload, "cells": cells0, "instances": len(insts),
+                   "instances_run": "one after another" if len(insts) > 1 else "single system",
+                   "l2": "inputs larger than L2 (no flush)" if cells0 * 192 * 24 > 126e6 else "L2 resident"},
+        "reference_build": {"kernels": "src/propagate.cu, centermass.cu, volume.cu, propagatebound.cu, "
+                                       "PressureKernels.cu, postscriptinit.cu compiled unmodified for sm_100a "
+                                       "(oracle/ref.mk)",
+                            "driver": "oracle/ref_harness.cu: the step sequence of src/GPUbounce.cu:1055-1338",
+                            "status": sorted(statuses), "max_bin_count": max_bin, "max_cells_per_node_filter": max_nn,
+                            "guard_ms_excluded": guard},
+        "cpu_baseline": {"value": value, "unit": "node-steps/s", "cores": 0, "kind": "reference",
+                         "sample": "no CPU implementation exists: the reference's CUDA kernels on this GPU, "
+                                   "%d timed steps after %d warm-up steps" % (args.steps, args.warmup)},
+        "e2e": {"value": value, "unit": "node-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "clocks": clk.summary(),
+    })
+    return line
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -289,15 +347,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        base = cpu_baseline(args, steps=max(1, min(args.steps, args.cpu_steps)))
-        line = {"impl": "reference", "metric": "node-steps/s (cells x 180 x steps / s)", "value": base["value"],
-                "unit": "node-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic", "config": {"workload": args.workload, "cells": args.cpu_cells},
-                "cpu_baseline": base,
-                "e2e": {"value": base["value"], "unit": "node-steps/s", "h2d_bytes_per_step": 0,
-                        "d2h_bytes_per_step": 0}}
-        print(json.dumps(line))
+        print(json.dumps(run_reference(args)))
         return
     res = run_cs3d(args, world, rank, local)
     if rank == 0:

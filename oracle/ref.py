@@ -1,0 +1,110 @@
+"""Runner of oracle/_ref/cs3d_ref: the reference CellSim3D CUDA kernels,
+compiled unmodified from the reference sources by oracle/ref.mk and driven
+through the reference's timestep by oracle/ref_harness.cu.
+
+TEST AND BASELINE INFRASTRUCTURE ONLY: the parity tests use it to pin the
+restatement against the reference's own arithmetic, and the benchmark uses it
+to time the reference on the same GPU.  Nothing in the product imports it.
+
+File formats (little-endian):
+  input   "CS3DREF1", cs3d_params, cs3d_topology (include/cs3d.h),
+          int32 n, capacity, steps, flags (bit 0: dump the initial forces),
+          warmup (steps before the timed region),
+          float32 X, Y, Z, VX, VY, VZ [n*192], pressure [n], youngs [n]
+  output  "CS3DREFO", int32 status, steps_done, n, n_events, max_bin, max_nn,
+          float32 total_ms, guard_ms (timed region), int32 events [n_events*3] (step, parent,
+          daughter), float32 X, Y, Z, VX, VY, VZ, FCX..FCZ, FDX..FDZ [n*192],
+          pressure [n], CM x, y, z [n], int32 n_init, n_first, float32 initial
+          FCX..FCZ, FDX..FDZ [n_init*192] when requested.
+"""
+import os
+import struct
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BIN = os.path.join(HERE, "_ref", "cs3d_ref")
+
+STATUS = {0: "ok", 1: "a grid bin held more than 32 cells (clamped)",
+          2: "more than 10 cells passed the box filter for a node (bin cut)",
+          3: "NaN position", 4: "division past capacity", 5: "grid larger than the reference's buffers"}
+
+
+def available():
+    return os.path.exists(BIN)
+
+
+def build(ref_root="/root/reference"):
+    """Compile oracle/_ref/cs3d_ref with oracle/ref.mk (needs the reference sources)."""
+    subprocess.run(["make", "-s", "-f", os.path.join(HERE, "ref.mk"), "REF=" + ref_root, "-j8"], check=True)
+
+
+def _f32(a, n):
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float32).ravel()[:n])
+    if a.size != n:
+        raise ValueError("array of %d values, %d needed" % (a.size, n))
+    return a
+
+
+def run(params, topo, state, capacity, steps, dump_init=False, warmup=0, timeout=3600, workdir=None):
+    """Run the reference for `steps` steps from `state`.
+
+    params, topo: ctypes structures with the layout of cs3d_params and
+    cs3d_topology; state: dict with X, Y, Z (and optionally VX, VY, VZ,
+    pressure, youngs) and n.  Returns a dict of the output file."""
+    if not available():
+        raise FileNotFoundError(BIN + " not built (make -f oracle/ref.mk)")
+    n = int(state["n"])
+    k = n * 192
+    zeros = np.zeros(k, np.float32)
+    press = state.get("pressure")
+    if press is None:
+        press = np.full(n, params.min_pressure, np.float32)
+    youngs = state.get("youngs")
+    if youngs is None:
+        youngs = np.full(n, params.stiffness1, np.float32)
+    with tempfile.TemporaryDirectory(dir=workdir) as tmp:
+        fin, fout = os.path.join(tmp, "in.bin"), os.path.join(tmp, "out.bin")
+        with open(fin, "wb") as f:
+            f.write(b"CS3DREF1")
+            f.write(bytes(params))
+            f.write(bytes(topo))
+            f.write(struct.pack("<5i", n, int(capacity), int(steps), 1 if dump_init else 0, int(warmup)))
+            for key in ("X", "Y", "Z", "VX", "VY", "VZ"):
+                a = state.get(key)
+                f.write((_f32(a, k) if a is not None else zeros).tobytes())
+            f.write(_f32(press, n).tobytes())
+            f.write(_f32(youngs, n).tobytes())
+        p = subprocess.run([BIN, fin, fout], capture_output=True, text=True, timeout=timeout)
+        if p.returncode != 0:
+            raise RuntimeError("cs3d_ref failed (%d): %s" % (p.returncode, p.stderr[-2000:]))
+        with open(fout, "rb") as f:
+            buf = f.read()
+    if buf[:8] != b"CS3DREFO":
+        raise RuntimeError("cs3d_ref: bad output")
+    off = 8
+    status, done, nf, nev, max_bin, max_nn = struct.unpack_from("<6i", buf, off)
+    off += 24
+    total_ms, guard_ms = struct.unpack_from("<2f", buf, off)
+    off += 8
+    ev = np.frombuffer(buf, np.int32, 3 * nev, off).reshape(nev, 3).copy()
+    off += 12 * nev
+    out = {"status": status, "status_text": STATUS.get(status, "?"), "steps": done, "n": nf,
+           "max_bin": max_bin, "max_local_nn": max_nn, "total_ms": total_ms, "guard_ms": guard_ms,
+           "events": ev}
+    kf = nf * 192
+    for key in ("X", "Y", "Z", "VX", "VY", "VZ", "FCX", "FCY", "FCZ", "FDX", "FDY", "FDZ"):
+        out[key] = np.frombuffer(buf, np.float32, kf, off).copy()
+        off += 4 * kf
+    out["pressure"] = np.frombuffer(buf, np.float32, nf, off).copy()
+    off += 4 * nf
+    out["cm"] = np.frombuffer(buf, np.float32, 3 * nf, off).reshape(3, nf).T.copy()
+    off += 12 * nf
+    n_init, n_first = struct.unpack_from("<2i", buf, off)
+    off += 8
+    if n_first:
+        first = np.frombuffer(buf, np.float32, n_first, off).reshape(6, n_init * 192)
+        out["init"] = {key: first[q].copy() for q, key in enumerate(("FCX", "FCY", "FCZ", "FDX", "FDY", "FDZ"))}
+    return out
