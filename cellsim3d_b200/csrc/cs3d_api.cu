@@ -412,7 +412,7 @@ int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topol
     AL(d.Xb, nodes);
     AL(d.ent, (size_t)c->cap_total * MAXE * SLOTS); AL(d.nent, nodes);
     d.hsize = hash_size(c->cap_total);
-    AL(d.hcount, (size_t)d.hsize + SCAN_TILE); AL(d.hscan, (size_t)d.hsize / SCAN_TILE + 1);
+    AL(d.hcount, (size_t)d.hsize + SCAN_TILE); AL(d.hscan, (size_t)d.hsize / SCAN_TILE + 1); AL(d.hsz, 1);
     AL(d.hpos, nodes); AL(d.node_rank, nodes);
     AL(d.divtab, c->cap_total); AL(d.div_total, 1);
     d.ev_cap = std::max(1 << 16, 2 * c->cap_total);
@@ -876,7 +876,7 @@ struct StaticScratch {
     float4 aabb0[2 * SCAP], aabb1[2 * SCAP];
     float4 hpos[SCAP * SLOTS];
     alignas(16) int hcount[SHASH + SCAN_TILE];
-    int hscan[SHASH / SCAN_TILE + 1], node_rank[SCAP * SLOTS];
+    int hscan[SHASH / SCAN_TILE + 1], node_rank[SCAP * SLOTS], hsz;
     int cell_inst[SCAP], work[SCAP], work_n;
     int cand[SCAP * MAXC], ncand[SCAP];
     unsigned long long dmask[SCAP * SLOTS];
@@ -978,7 +978,7 @@ Dev static_dev(StaticScratch *s)
     d.cand = s->cand; d.ncand = s->ncand;
     d.dmask = s->dmask;
     d.ent = s->ent; d.nent = s->nent;
-    d.hsize = SHASH; d.hcount = s->hcount; d.hscan = s->hscan; d.hpos = s->hpos; d.node_rank = s->node_rank;
+    d.hsize = SHASH; d.hsz = &s->hsz; d.hcount = s->hcount; d.hscan = s->hscan; d.hpos = s->hpos; d.node_rank = s->node_rank;
     d.divtab = s->divtab; d.div_total = &s->div_total;
     d.events = s->events; d.n_events = &s->n_events; d.ev_cap = SEVENTS;
     d.flags = s->flags;

@@ -94,8 +94,9 @@ struct Dev {
     unsigned long long *dmask;  // [cell*192 + node] entries that are dissipative pairs this step
     // node-level spatial hash of the neighbour-list build: cubic bins of
     // edge ~rlist hashed (with the instance) into hsize buckets
-    int hsize;          // buckets (power of two, >= SCAN_TILE)
-    int *hcount;        // [hsize + 1] bucket counts, then exclusive starts
+    int hsize;          // bucket capacity (power of two, >= SCAN_TILE)
+    int *hsz;           // buckets in use this build (power of two, SCAN_TILE..hsize)
+    int *hcount;        // [hsize + SCAN_TILE] bucket counts, then exclusive starts
     int *hscan;         // [hsize / SCAN_TILE + 1] tile sums of the scan
     float4 *hpos;       // [cap_total*192] positions sorted by bucket, w = node id bits
     int *node_rank;     // [cap_total*192] position of the node in its bucket

@@ -385,10 +385,20 @@ __global__ void __launch_bounds__(SLOTS) k_integrate(Dev d)
 // Per-step bookkeeping (one block): step counter, rebuild decision, reset of
 // the accumulators that this step fills.
 // ---------------------------------------------------------------------------
+// Buckets of the node hash for `nodes` nodes: the next power of two, within
+// [SCAN_TILE, hsize].
+__device__ __forceinline__ int hash_buckets(const Dev &d, long long nodes)
+{
+    int h = SCAN_TILE;
+    while (h < nodes && h < d.hsize) h <<= 1;
+    return h;
+}
+
 __global__ void k_step_begin(Dev d, int par_next)
 {
     __shared__ int any;
-    if (threadIdx.x == 0) { any = 0; *d.div_total = 0; }
+    __shared__ unsigned long long nodes;
+    if (threadIdx.x == 0) { any = 0; nodes = 0ull; *d.div_total = 0; }
     __syncthreads();
     for (int k = threadIdx.x; k < d.n_inst; k += blockDim.x) {
         InstState *st = &d.st[k];
@@ -405,7 +415,10 @@ __global__ void k_step_begin(Dev d, int par_next)
         st->force_rebuild = 0;
         st->disp_acc = ds;
         st->div_count = 0;
-        if (need) st->rebuilds += 1;
+        if (need) {
+            st->rebuilds += 1;
+            atomicAdd(&nodes, (unsigned long long)st->n * NODES);
+        }
         for (int q = 0; q < 3; ++q) {
             st->mm[par_next][2 * q] = f2o(1.0e30f);
             st->mm[par_next][2 * q + 1] = f2o(-1.0e30f);
@@ -413,12 +426,19 @@ __global__ void k_step_begin(Dev d, int par_next)
         if (need) any = 1;
     }
     __syncthreads();
-    if (threadIdx.x == 0) { d.flags[0] = any; *d.n_pairs = 0ull; }
+    if (threadIdx.x == 0) {
+        d.flags[0] = any;
+        *d.n_pairs = 0ull;
+        *d.hsz = hash_buckets(d, (long long)nodes);
+    }
 }
 
 // Init variant: rebuild everything, reset the grid accumulators.
 __global__ void k_init_begin(Dev d)
 {
+    __shared__ unsigned long long nodes;
+    if (threadIdx.x == 0) nodes = 0ull;
+    __syncthreads();
     for (int k = threadIdx.x; k < d.n_inst; k += blockDim.x) {
         InstState *st = &d.st[k];
         st->rebuild = 1;
@@ -430,10 +450,15 @@ __global__ void k_init_begin(Dev d)
                 st->mm[p][2 * q] = f2o(1.0e30f);
                 st->mm[p][2 * q + 1] = f2o(-1.0e30f);
             }
-        for (int q = 0; q < 3; ++q) {
-        }
+        atomicAdd(&nodes, (unsigned long long)st->n * NODES);
     }
-    if (threadIdx.x == 0) { d.flags[0] = 1; *d.div_total = 0; *d.n_pairs = 0ull; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        d.flags[0] = 1;
+        *d.div_total = 0;
+        *d.n_pairs = 0ull;
+        *d.hsz = hash_buckets(d, (long long)nodes);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1022,10 +1047,11 @@ __device__ __forceinline__ BinGeom bin_geom(const Dev &d, const InstParams &P, i
     // bin edge 1% above the list radius: float rounding of x / edge cannot
     // put two nodes closer than the radius more than one bin apart
     b.inv = 1.0f / ((P.rlist + 1e-4f) * 1.01f);
-    const int B = 31 - __clz(d.hsize);
+    const int hs = *d.hsz;
+    const int B = 31 - __clz(hs);
     b.bx = B / 3;
     b.by = B / 3;
-    b.mask = (unsigned)d.hsize - 1u;
+    b.mask = (unsigned)hs - 1u;
     b.off = (unsigned)inst * 2654435761u;
     return b;
 }
@@ -1077,7 +1103,7 @@ __global__ void k_nh_zero(Dev d)
 {
     if (!d.flags[0]) return;
     int4 *p = reinterpret_cast<int4 *>(d.hcount);
-    const int n4 = (d.hsize + SCAN_TILE) / 4;
+    const int n4 = (*d.hsz + SCAN_TILE) / 4;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += gridDim.x * blockDim.x)
         p[q] = make_int4(0, 0, 0, 0);
 }
@@ -1105,7 +1131,7 @@ __global__ void __launch_bounds__(256) k_nh_scan_tiles(Dev d)
 {
     if (!d.flags[0]) return;
     __shared__ int wsum[32];
-    const int ntile = d.hsize / SCAN_TILE + 1;
+    const int ntile = *d.hsz / SCAN_TILE + 1;
     for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
         const int4 *p = reinterpret_cast<const int4 *>(d.hcount + (size_t)t * SCAN_TILE);
         int s = 0;
@@ -1132,7 +1158,7 @@ __global__ void __launch_bounds__(1024) k_nh_scan_top(Dev d)
     if (!d.flags[0]) return;
     __shared__ int wsum[32];
     __shared__ int carry;
-    const int ntile = d.hsize / SCAN_TILE + 1;
+    const int ntile = *d.hsz / SCAN_TILE + 1;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
     for (int t0 = 0; t0 < ntile; t0 += 1024) {
@@ -1153,7 +1179,7 @@ __global__ void __launch_bounds__(256) k_nh_scan_apply(Dev d)
     if (!d.flags[0]) return;
     __shared__ int wsum[32];
     constexpr int PER = SCAN_TILE / 256;  // 16 consecutive buckets per thread
-    const int ntile = d.hsize / SCAN_TILE + 1;
+    const int ntile = *d.hsz / SCAN_TILE + 1;
     for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
         int4 *p = reinterpret_cast<int4 *>(d.hcount + (size_t)t * SCAN_TILE + threadIdx.x * PER);
         int4 v[PER / 4];
