@@ -227,11 +227,12 @@ int launch_nl_kernels(const Dev &d, cudaStream_t s, int grid_nodes, int grid_til
     k_nh_scan_top<<<1, 1024, 0, s>>>(d); pf.mark(s, "nh_scan_top");
     k_nh_scan_apply<<<grid_tiles, 256, 0, s>>>(d); pf.mark(s, "nh_scan_apply");
     k_nh_fill<<<grid_nodes, SLOTS, 0, s>>>(d); pf.mark(s, "nh_fill");
-    k_nl_cell<<<grid_nodes, SLOTS, 0, s>>>(d); pf.mark(s, "nl_cell");
+    k_nl_cell<<<grid_nodes, SLOTS, 0, s>>>(d, 0); pf.mark(s, "nl_cell");
+    k_nl_cell<<<grid_nodes, SLOTS, 0, s>>>(d, 1); pf.mark(s, "nl_cell_nbr");
     CK(cudaGetLastError());
     return CS3D_OK;
 }
-constexpr int NL_LAUNCHES = 7;
+constexpr int NL_LAUNCHES = 8;
 
 int launch_nl_build(cs3d_ctx *c, const Prof &pf = Prof())
 {
@@ -408,7 +409,7 @@ int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topol
     AL(d.cell_inst, c->cap_total);
     AL(d.work, c->cap_total); AL(d.work_n, 1);
     AL(d.cand, (size_t)c->cap_total * MAXC); AL(d.ncand, c->cap_total);
-    AL(d.dmask, nodes);
+    AL(d.dmask, nodes); AL(d.dirty, c->cap_total);
     AL(d.Xb, nodes);
     AL(d.ent, (size_t)c->cap_total * MAXE * SLOTS); AL(d.nent, nodes);
     d.hsize = hash_size(c->cap_total);
@@ -880,6 +881,7 @@ struct StaticScratch {
     int cell_inst[SCAP], work[SCAP], work_n;
     int cand[SCAP * MAXC], ncand[SCAP];
     unsigned long long dmask[SCAP * SLOTS];
+    int dirty[SCAP];
     uint16_t ent[SCAP * MAXE * SLOTS];
     uint8_t nent[SCAP * SLOTS];
     DivEntry divtab[SCAP];
@@ -976,7 +978,7 @@ Dev static_dev(StaticScratch *s)
     d.aabb[0] = s->aabb0; d.aabb[1] = s->aabb1;
     d.cell_inst = s->cell_inst; d.work = s->work; d.work_n = &s->work_n;
     d.cand = s->cand; d.ncand = s->ncand;
-    d.dmask = s->dmask;
+    d.dmask = s->dmask; d.dirty = s->dirty;
     d.ent = s->ent; d.nent = s->nent;
     d.hsize = SHASH; d.hsz = &s->hsz; d.hcount = s->hcount; d.hscan = s->hscan; d.hpos = s->hpos; d.node_rank = s->node_rank;
     d.divtab = s->divtab; d.div_total = &s->div_total;
@@ -1089,6 +1091,7 @@ extern "C" int cs3d_forces_static(const cs3d_params *params, const cs3d_topology
     // the previous call's neighbour lists, boxes and flags must not leak in
     CK(cudaMemsetAsync(S->ncand, 0, sizeof S->ncand, s));
     CK(cudaMemsetAsync(S->nent, 0, sizeof S->nent, s));
+    CK(cudaMemsetAsync(S->dirty, 0, sizeof S->dirty, s));
     CK(cudaMemsetAsync(S->flags, 0, sizeof S->flags, s));
     CK(cudaMemsetAsync(&S->n_events, 0, sizeof S->n_events, s));
     k_static_load<<<sd->grid_flat, 256, 0, s>>>(d, n_cells, X, Y, Z, VX, VY, VZ, pressure, youngs, params->min_pressure,

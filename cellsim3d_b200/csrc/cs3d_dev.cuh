@@ -35,7 +35,8 @@ struct InstState {
     int n;                 // current cell count
     int step;              // number of the step in progress / last finished
     unsigned err;          // CS3D_ERRBIT_*
-    int rebuild;           // neighbour list must be rebuilt before the next sweep
+    int rebuild;           // list rebuild this step: 0 none, 1 around divisions, 2 whole instance
+    float rcur;            // list radius of this step's build
     int mm[2][6];          // grid extents (ordered-int min/max) by step parity
     float disp_acc;        // displacement bound accumulated since the last rebuild
     unsigned disp_step;    // max node displacement of the current step (float bits)
@@ -85,7 +86,8 @@ struct Dev {
     int single;         // one instance with base 0: the work table is the identity
     int *cand;          // [cell*MAXC]
     int *ncand;         // [cell]
-    float4 *Xb;         // positions at the last neighbour-list build
+    float4 *Xb;         // anchors of the displacement test (positions at a build)
+    int *dirty;         // [cell] 1: divided last step, 2: within the list radius of such a cell
     // contact candidates of each node: slot << 8 | node, ascending, where
     // slot indexes the cell's candidate list (cand) and node the node in
     // that cell

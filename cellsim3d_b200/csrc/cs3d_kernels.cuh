@@ -404,26 +404,34 @@ __global__ void k_step_begin(Dev d, int par_next)
         InstState *st = &d.st[k];
         const InstParams &P = d.prm[k];
         st->step += 1;
-        // ds: the largest distance of any node from its position at the
-        // last build.  While 2*ds stays below the skin, every pair within
-        // the contact cut-off now was within the list radius then; the
-        // 1e-3 slack covers float rounding of the distances.
-        float ds = __uint_as_float(st->disp_step);
+        // ds: the largest distance of any node from its anchor (Xb, its
+        // position at a build).  Every list built at time tb with radius
+        // ra + skin + 2*ds(tb) stays complete while all nodes stay within
+        // skin/2 of their anchors: a pair within ra now was within
+        // ra + 2*(skin/2 + ds(tb)) at tb.  Whole-instance builds (ds reset
+        // to 0) use ra + skin; the 1e-3 slack covers float rounding.
+        // After divisions, only the divided cells (anchors reset) and the
+        // cells within the list radius of them are rebuilt, unless ds is
+        // already large.
+        const float ds = __uint_as_float(st->disp_step);
         st->disp_step = 0u;
-        bool need = st->force_rebuild || !(2.0f * ds + 1e-3f < P.skin);
-        st->rebuild = need ? 1 : 0;
+        const bool full = st->force_rebuild || !(2.0f * ds + 1e-3f < P.skin) ||
+                          (st->div_count > 0 && ds > 0.25f * P.skin);
+        const bool part = !full && st->div_count > 0;
+        st->rebuild = full ? 2 : part ? 1 : 0;
+        st->rcur = full ? P.rlist : P.rlist + 2.0f * ds + 1e-3f;
         st->force_rebuild = 0;
         st->disp_acc = ds;
         st->div_count = 0;
-        if (need) {
-            st->rebuilds += 1;
+        if (full || part) {
+            if (full) st->rebuilds += 1;
             atomicAdd(&nodes, (unsigned long long)st->n * NODES);
+            any = 1;
         }
         for (int q = 0; q < 3; ++q) {
             st->mm[par_next][2 * q] = f2o(1.0e30f);
             st->mm[par_next][2 * q + 1] = f2o(-1.0e30f);
         }
-        if (need) any = 1;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -441,7 +449,8 @@ __global__ void k_init_begin(Dev d)
     __syncthreads();
     for (int k = threadIdx.x; k < d.n_inst; k += blockDim.x) {
         InstState *st = &d.st[k];
-        st->rebuild = 1;
+        st->rebuild = 2;
+        st->rcur = d.prm[k].rlist;
         st->force_rebuild = 0;
         st->disp_acc = 0.0f;
         st->disp_step = 0u;
@@ -890,7 +899,6 @@ __global__ void __launch_bounds__(256) k_div_select(Dev d, int par)
         if (total > room) atomicOr(&st->err, CS3D_ERRBIT_CAPACITY);
         base_slot = atomicAdd(d.div_total, ndiv);
         st->div_count = ndiv;
-        st->force_rebuild = 1;
         atomicOr(&d.flags[1], 1);
     }
     __syncthreads();
@@ -995,11 +1003,15 @@ __global__ void __launch_bounds__(SLOTS) k_div_apply(Dev d, int par)
             d.press[b] = P.minp;
             d.E[b] = P.daught_same ? d.E[a] : P.stiff1;
             d.cell_inst[b] = e.inst;
+            d.dirty[a] = 1;  // lists rebuilt around the two cells next step
+            d.dirty[b] = 1;
         }
         if (i < NODES) {
             size_t ga = (size_t)a * SLOTS + i, gb = (size_t)b * SLOTS + i;
             d.X[ga] = xa;
             d.X[gb] = xb;
+            d.Xb[ga] = xa;   // new anchors of the displacement test
+            d.Xb[gb] = xb;
             d.V[gb] = d.V[ga];
             d.FC[gb] = make_float4(0, 0, 0, 0);
             d.FD[gb] = make_float4(0, 0, 0, 0);
@@ -1046,7 +1058,7 @@ __device__ __forceinline__ BinGeom bin_geom(const Dev &d, const InstParams &P, i
     BinGeom b;
     // bin edge 1% above the list radius: float rounding of x / edge cannot
     // put two nodes closer than the radius more than one bin apart
-    b.inv = 1.0f / ((P.rlist + 1e-4f) * 1.01f);
+    b.inv = 1.0f / ((d.st[inst].rcur + 1e-4f) * 1.01f);
     const int hs = *d.hsz;
     const int B = 31 - __clz(hs);
     b.bx = B / 3;
@@ -1235,9 +1247,13 @@ struct BuildSmem {
     int slot_t[MAXC];        // temporary slot of each final slot
     int wsum[32];
     int ncomp;
+    int flag;
 };
 
-__global__ void __launch_bounds__(SLOTS) k_nl_cell(Dev d)
+// Phase 0 builds the cells of whole-instance rebuilds and the divided cells
+// (dirty 1) of partial ones, and marks the candidates of the divided cells
+// (dirty 2); phase 1 builds the marked cells and clears all marks.
+__global__ void __launch_bounds__(SLOTS) k_nl_cell(Dev d, int phase)
 {
     if (!d.flags[0]) return;
     __shared__ BuildSmem sm;
@@ -1247,10 +1263,17 @@ __global__ void __launch_bounds__(SLOTS) k_nl_cell(Dev d)
         const int a = cell_of(d, w);
         const int inst = inst_of(d, a);
         InstState *st = &d.st[inst];
-        if (!st->rebuild) continue;  // uniform across the block
-        const InstParams &P = d.prm[inst];
-        const BinGeom b = bin_geom(d, P, inst);
-        const float rl = P.rlist + 1e-4f;
+        const int rb = st->rebuild;
+        if (!rb) continue;  // uniform across the block
+        __syncthreads();
+        if (i == 0) sm.flag = d.dirty[a];
+        __syncthreads();
+        const int mark = sm.flag;
+        if (phase == 1 && mark && i == 0) d.dirty[a] = 0;
+        const bool build = phase == 0 ? (rb == 2 || mark == 1) : (rb == 1 && mark == 2);
+        if (!build) continue;
+        const BinGeom b = bin_geom(d, d.prm[inst], inst);
+        const float rl = st->rcur + 1e-4f;
         const float rl2 = rl * rl;
         for (int t = i; t < 256; t += SLOTS) sm.tkey[t] = -1;
         for (int q = i; q < 256 * 6; q += SLOTS) (&sm.mask[0][0])[q] = 0u;
@@ -1353,12 +1376,15 @@ __global__ void __launch_bounds__(SLOTS) k_nl_cell(Dev d)
             }
             for (int k = 0; k < m; ++k) ep[(size_t)k * SLOTS] = ord[k];
             d.nent[g] = (uint8_t)m;
-            d.Xb[g] = x;  // reference for the displacement test
+            // new anchors, except for the neighbours of divided cells: other
+            // cells' lists rely on their old anchors
+            if (phase == 0) d.Xb[g] = x;
             if (cnt > MAXE) atomicOr(&st->err, CS3D_ERRBIT_ENTRY_OVERFLOW);
             if (lost) atomicOr(&st->err, CS3D_ERRBIT_CAND_OVERFLOW);
         } else {
             d.nent[g] = 0;
         }
+        if (phase == 0 && rb == 1 && i < nc) atomicCAS(&d.dirty[d.cand[(size_t)a * MAXC + i]], 0, 2);
         if (i == 0) {
             if (nct > MAXC) atomicOr(&st->err, CS3D_ERRBIT_CAND_OVERFLOW);
             d.ncand[a] = nc;
