@@ -79,64 +79,80 @@ void free_all(cs3d_ctx *c)
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
 }
 
-// Host-side mesh tables: packed neighbours, R0, theta0 and the arm-end
-// index table that maps node i's six second-neighbour angle terms (the
-// NeighNeighs cases of src/propagate.cu:63-78, theta1 then theta2 per
-// neighbour) onto the arm-force array [(vertex*3 + pair)*2 + end].
-int upload_topology(cs3d_ctx *c, const cs3d_topology *t)
+// Host copies of the mesh tables: packed neighbours, R0 and 1/R0, theta0
+// with its FP64 cosine and sine, and the arm table: for node i and each of
+// its neighbours n, the index n*3 + k of the arm force that the angles at
+// vertex n send to i (k = the slot of i in n's neighbour list; the two
+// angles at n that have i as an arm end, the NeighNeighs cases of
+// src/propagate.cu:63-78).
+struct TopoTables {
+    uint32_t nnp[SLOTS];
+    float4 r0[SLOTS], th[SLOTS];
+    uint4 arm[SLOTS];
+    uint8_t faces[CS3D_FACES * 7];
+    double2 cs0[3 * SLOTS];
+    double r0i[3 * SLOTS];
+};
+
+int topo_tables(const cs3d_topology *t, TopoTables &o)
 {
-    std::vector<uint32_t> nnp(SLOTS, 0);
-    std::vector<float4> r0(SLOTS), th(SLOTS);
-    std::vector<uint4> arm(SLOTS);
-    std::vector<uint8_t> faces(CS3D_FACES * 7);
-    for (int i = 0; i < SLOTS; ++i) {
-        r0[i] = make_float4(0, 0, 0, 0);
-        th[i] = make_float4(0, 0, 0, 0);
-        arm[i] = make_uint4(0, 0, 0, 0);
-    }
+    memset(&o, 0, sizeof o);
+    for (int i = 0; i < 3 * SLOTS; ++i) o.cs0[i] = make_double2(1.0, 0.0);
     for (int i = 0; i < NODES; ++i) {
         int a = t->nn[i], b = t->nn[192 + i], cc = t->nn[384 + i];
         if (a < 0 || a >= NODES || b < 0 || b >= NODES || cc < 0 || cc >= NODES) return CS3D_E_ARG;
-        nnp[i] = (uint32_t)a | ((uint32_t)b << 8) | ((uint32_t)cc << 16) | ((uint32_t)(uint8_t)(int8_t)t->sign[i] << 24);
-        r0[i] = make_float4(t->r0[i], t->r0[192 + i], t->r0[384 + i], 0.f);
-        th[i] = make_float4(t->theta0[3 * i], t->theta0[3 * i + 1], t->theta0[3 * i + 2], 0.f);
+        o.nnp[i] = (uint32_t)a | ((uint32_t)b << 8) | ((uint32_t)cc << 16) | ((uint32_t)(uint8_t)(int8_t)t->sign[i] << 24);
+        o.r0[i] = make_float4(t->r0[i], t->r0[192 + i], t->r0[384 + i], 0.f);
+        o.th[i] = make_float4(t->theta0[3 * i], t->theta0[3 * i + 1], t->theta0[3 * i + 2], 0.f);
+        for (int k = 0; k < 3; ++k) {
+            const double th = (double)t->theta0[3 * i + k];
+            o.cs0[3 * i + k] = make_double2(cos(th), sin(th));
+            const float r0 = t->r0[k * 192 + i];
+            if (!(r0 > 0.0f)) return CS3D_E_ARG;
+            o.r0i[3 * i + k] = 1.0 / (double)r0;
+        }
     }
     for (int i = 0; i < NODES; ++i) {
-        unsigned idx[6];
+        unsigned idx[3];
         for (int q = 0; q < 3; ++q) {
-            int n = t->nn[q * 192 + i];
-            int na = t->nn[n], nb = t->nn[192 + n], nc = t->nn[384 + n];
-            unsigned base = (unsigned)n * 6;
-            if (na == i) { idx[2 * q] = base + 0 * 2 + 0; idx[2 * q + 1] = base + 2 * 2 + 0; }
-            else if (nb == i) { idx[2 * q] = base + 0 * 2 + 1; idx[2 * q + 1] = base + 1 * 2 + 0; }
-            else if (nc == i) { idx[2 * q] = base + 2 * 2 + 1; idx[2 * q + 1] = base + 1 * 2 + 1; }
-            else return CS3D_E_ARG;  // neighbour table not symmetric
+            const int n = t->nn[q * 192 + i];
+            int k = -1;
+            for (int m = 0; m < 3; ++m)
+                if (t->nn[m * 192 + n] == i) k = m;
+            if (k < 0) return CS3D_E_ARG;  // neighbour table not symmetric
+            idx[q] = (unsigned)(n * 3 + k);
         }
-        arm[i] = make_uint4(idx[0] | (idx[1] << 16), idx[2] | (idx[3] << 16), idx[4] | (idx[5] << 16), 0u);
+        o.arm[i] = make_uint4(idx[0], idx[1], idx[2], 0u);
     }
     for (int f = 0; f < CS3D_FACES * 7; ++f) {
         if (t->faces[f] < 0 || t->faces[f] >= NODES) return CS3D_E_ARG;
-        faces[f] = (uint8_t)t->faces[f];
+        o.faces[f] = (uint8_t)t->faces[f];
     }
-    std::vector<double2> cs0(3 * SLOTS, make_double2(1.0, 0.0));
-    for (int i = 0; i < NODES; ++i)
-        for (int k = 0; k < 3; ++k) {
-            const double th = (double)t->theta0[3 * i + k];
-            cs0[3 * i + k] = make_double2(cos(th), sin(th));
-        }
-    int rc;
-    if ((rc = dalloc(c, &c->d.topo.cs0, 3 * SLOTS))) return rc;
-    CK(cudaMemcpyAsync(c->d.topo.cs0, cs0.data(), sizeof(double2) * 3 * SLOTS, cudaMemcpyHostToDevice, c->stream));
-    if ((rc = dalloc(c, &c->d.topo.nnpack, SLOTS))) return rc;
-    if ((rc = dalloc(c, &c->d.topo.r0, SLOTS))) return rc;
-    if ((rc = dalloc(c, &c->d.topo.th0, SLOTS))) return rc;
-    if ((rc = dalloc(c, &c->d.topo.arm, SLOTS))) return rc;
-    if ((rc = dalloc(c, &c->d.topo.faces, CS3D_FACES * 7))) return rc;
-    CK(cudaMemcpyAsync(c->d.topo.nnpack, nnp.data(), SLOTS * 4, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(c->d.topo.r0, r0.data(), SLOTS * 16, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(c->d.topo.th0, th.data(), SLOTS * 16, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(c->d.topo.arm, arm.data(), SLOTS * 16, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(c->d.topo.faces, faces.data(), CS3D_FACES * 7, cudaMemcpyHostToDevice, c->stream));
+    return CS3D_OK;
+}
+
+int upload_topology(cs3d_ctx *c, const cs3d_topology *t)
+{
+    TopoTables tt;
+    int rc = topo_tables(t, tt);
+    if (rc) return rc;
+    Topo &T = c->d.topo;
+    if ((rc = dalloc(c, &T.cs0, 3 * SLOTS))) return rc;
+    if ((rc = dalloc(c, &T.r0i, 3 * SLOTS))) return rc;
+    if ((rc = dalloc(c, &T.nnpack, SLOTS))) return rc;
+    if ((rc = dalloc(c, &T.r0, SLOTS))) return rc;
+    if ((rc = dalloc(c, &T.th0, SLOTS))) return rc;
+    if ((rc = dalloc(c, &T.arm, SLOTS))) return rc;
+    if ((rc = dalloc(c, &T.faces, CS3D_FACES * 7))) return rc;
+    CK(cudaMemcpyAsync(T.cs0, tt.cs0, sizeof tt.cs0, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(T.r0i, tt.r0i, sizeof tt.r0i, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(T.nnpack, tt.nnp, sizeof tt.nnp, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(T.r0, tt.r0, sizeof tt.r0, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(T.th0, tt.th, sizeof tt.th, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(T.arm, tt.arm, sizeof tt.arm, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(T.faces, tt.faces, sizeof tt.faces, cudaMemcpyHostToDevice, c->stream));
+    // the host tables go out of scope: the copies must have completed
+    CK(cudaStreamSynchronize(c->stream));
     return CS3D_OK;
 }
 
@@ -896,6 +912,7 @@ struct StaticScratch {
     uint4 arm[SLOTS];
     uint8_t faces[CS3D_FACES * 7];
     double2 cs0[3 * SLOTS];
+    double r0i[3 * SLOTS];
 };
 
 // The scratch of cs3d_forces_static.  In host code this name is only a
@@ -913,50 +930,6 @@ constexpr int kMaxDevices = 64;
 StaticDevice g_static_dev[kMaxDevices];
 std::mutex g_static_mutex;
 
-// Host copies of the mesh tables (the same tables upload_topology builds).
-struct TopoTables {
-    uint32_t nnp[SLOTS];
-    float4 r0[SLOTS], th[SLOTS];
-    uint4 arm[SLOTS];
-    uint8_t faces[CS3D_FACES * 7];
-    double2 cs0[3 * SLOTS];
-};
-
-int topo_tables(const cs3d_topology *t, TopoTables &o)
-{
-    memset(&o, 0, sizeof o);
-    for (int i = 0; i < 3 * SLOTS; ++i) o.cs0[i] = make_double2(1.0, 0.0);
-    for (int i = 0; i < NODES; ++i) {
-        int a = t->nn[i], b = t->nn[192 + i], cc = t->nn[384 + i];
-        if (a < 0 || a >= NODES || b < 0 || b >= NODES || cc < 0 || cc >= NODES) return CS3D_E_ARG;
-        o.nnp[i] = (uint32_t)a | ((uint32_t)b << 8) | ((uint32_t)cc << 16) | ((uint32_t)(uint8_t)(int8_t)t->sign[i] << 24);
-        o.r0[i] = make_float4(t->r0[i], t->r0[192 + i], t->r0[384 + i], 0.f);
-        o.th[i] = make_float4(t->theta0[3 * i], t->theta0[3 * i + 1], t->theta0[3 * i + 2], 0.f);
-        for (int k = 0; k < 3; ++k) {
-            const double th = (double)t->theta0[3 * i + k];
-            o.cs0[3 * i + k] = make_double2(cos(th), sin(th));
-        }
-    }
-    for (int i = 0; i < NODES; ++i) {
-        unsigned idx[6];
-        for (int q = 0; q < 3; ++q) {
-            int n = t->nn[q * 192 + i];
-            int na = t->nn[n], nb = t->nn[192 + n], nc = t->nn[384 + n];
-            unsigned base = (unsigned)n * 6;
-            if (na == i) { idx[2 * q] = base + 0; idx[2 * q + 1] = base + 4; }
-            else if (nb == i) { idx[2 * q] = base + 1; idx[2 * q + 1] = base + 2; }
-            else if (nc == i) { idx[2 * q] = base + 5; idx[2 * q + 1] = base + 3; }
-            else return CS3D_E_ARG;
-        }
-        o.arm[i] = make_uint4(idx[0] | (idx[1] << 16), idx[2] | (idx[3] << 16), idx[4] | (idx[5] << 16), 0u);
-    }
-    for (int f = 0; f < CS3D_FACES * 7; ++f) {
-        if (t->faces[f] < 0 || t->faces[f] >= NODES) return CS3D_E_ARG;
-        o.faces[f] = (uint8_t)t->faces[f];
-    }
-    return CS3D_OK;
-}
-
 Dev static_dev(StaticScratch *s)
 {
     Dev d{};
@@ -971,6 +944,7 @@ Dev static_dev(StaticScratch *s)
     d.topo.arm = s->arm;
     d.topo.faces = s->faces;
     d.topo.cs0 = s->cs0;
+    d.topo.r0i = s->r0i;
     d.X = s->X; d.V = s->V; d.Vb = s->Vb; d.FC = s->FC; d.FD = s->FD; d.Xb = s->Xb;
     d.CM = s->CM;
     d.press = s->press; d.E = s->E; d.vol = s->vol; d.area = s->area;
@@ -1088,6 +1062,7 @@ extern "C" int cs3d_forces_static(const cs3d_params *params, const cs3d_topology
     CK(cudaMemcpyAsync(S->arm, tt.arm, sizeof tt.arm, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(S->faces, tt.faces, sizeof tt.faces, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(S->cs0, tt.cs0, sizeof tt.cs0, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(S->r0i, tt.r0i, sizeof tt.r0i, cudaMemcpyHostToDevice, s));
     // the previous call's neighbour lists, boxes and flags must not leak in
     CK(cudaMemsetAsync(S->ncand, 0, sizeof S->ncand, s));
     CK(cudaMemsetAsync(S->nent, 0, sizeof S->nent, s));

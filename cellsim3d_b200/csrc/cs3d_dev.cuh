@@ -14,7 +14,6 @@ constexpr int MAXC = CS3D_MAX_CAND;    // contact-candidate cells per cell
 constexpr int MAXE = CS3D_MAX_ENTRIES; // contact-candidate nodes per node
 constexpr int SCAN_TILE = 4096;        // elements per block of the bucket scan
 constexpr float DL = 2.9f;             // reference grid spacing, src/GPUbounce.cu:756
-constexpr int NARM = NODES * 3 * 2;    // arm-end forces of the 540 angles
 
 // Per-instance constants (uploaded once).
 struct InstParams {
@@ -61,7 +60,8 @@ struct Topo {
     float4 *r0;         // [192] equilibrium lengths to nn0..2
     float4 *th0;        // [192] aij, ajk, aik
     double2 *cs0;       // [192*3] (cos, sin) of aij, ajk, aik in FP64
-    uint4 *arm;         // [192] six uint16 indices into the arm-force array
+    double *r0i;        // [192*3] 1/R0 in FP64
+    uint4 *arm;         // [192] x, y, z: arm-force index n*3 + k for the three neighbours n
     uint8_t *faces;     // [92*7]
 };
 

@@ -64,6 +64,11 @@ __device__ __forceinline__ double rcp_nr(double x)
     double r = (double)__frcp_rn((float)x);
     return r * (2.0 - x * r);
 }
+__device__ __forceinline__ double rsqrt_nr(double x)
+{
+    const double y = (double)rsqrtf((float)x);
+    return y * (1.5 - 0.5 * x * y * y);
+}
 
 // Bond-angle term for one angle at a vertex with arms P (to the p-end node)
 // and Q (to the q-end node); Fp/Fq are GetAngleForce(P, Q) and
@@ -104,7 +109,7 @@ __device__ __forceinline__ void angle_pair(float3 P, float3 Q, float th0f, doubl
     const double dg = ch * s1 + sh * c1t;                            // d/dh of sin(h) sin(theta0 + h)
     h -= g * rcp_nr(dg);
     const double dth = 2.0 * h;
-    const double c1 = -rcp_nr(sqrt_nr(w2 - idk * idk + 1e-3));
+    const double c1 = -rsqrt_nr(w2 - idk * idk + 1e-3);
     const double f = -1000.0 * c1 * dth;
     const double cp = idk * rcp_nr(rp2), cq = idk * rcp_nr(rq2);
     Fp = make_double3(f * (qx - cp * px), f * (qy - cp * py), f * (qz - cp * pz));
@@ -248,8 +253,9 @@ __device__ __forceinline__ unsigned long long sweep_s1(const Dev &d, const InstP
             }
             if (r2 < P.ra2) {
                 // distance in FP64: (rr - R) cancels for stiff repulsion
-                const double R = sqrt_nr((double)dx * dx + (double)dy * dy + (double)dz * dz);
-                const double iR = rcp_nr(R);
+                const double R2 = (double)dx * dx + (double)dy * dy + (double)dz * dz;
+                const double iR = rsqrt_nr(R2);
+                const double R = R2 * iR;
                 double k = 0.0;
                 if (R < (double)P.ra) k += -(double)P.asE * ((double)P.ra - R) * iR;
                 if (R <= (double)P.rr) k += (double)P.rsE * ((double)P.rr - R) * iR;
@@ -567,8 +573,10 @@ __device__ __noinline__ void cell_volume(const Dev &d, const float4 *xs, float3 
 // INIT = true evaluates the initial forces of src/GPUbounce.cu:978-1004
 // (no velocity update; Fd written to FD).
 // ---------------------------------------------------------------------------
+// Arm forces of the angles at each vertex, summed by destination: entry
+// vertex*3 + k goes to the vertex's k-th neighbour.
 struct ArmForces {
-    double x[NARM], y[NARM], z[NARM];
+    double x[SLOTS * 3], y[SLOTS * 3], z[SLOTS * 3];
 };
 
 struct S1Smem {
@@ -614,20 +622,18 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
             float3 pa = sub3(f3(sm.xs[n0]), x), pb = sub3(f3(sm.xs[n1]), x), pc = sub3(f3(sm.xs[n2]), x);
             const double2 *cs0 = d.topo.cs0 + 3 * i;
             const float4 th = __ldg(&d.topo.th0[i]);
-            double3 Fp, Fq;
-            int o = i * 6;
+            // angles (n0, n1), (n1, n2), (n0, n2); arm ends summed by destination
+            double3 F01p, F01q, F12p, F12q, F02p, F02q;
             double2 t0 = __ldg(&cs0[0]);
-            angle_pair(pa, pb, th.x, t0.x, t0.y, Fp, Fq);
-            sm.arm.x[o] = Fp.x; sm.arm.y[o] = Fp.y; sm.arm.z[o] = Fp.z;
-            sm.arm.x[o + 1] = Fq.x; sm.arm.y[o + 1] = Fq.y; sm.arm.z[o + 1] = Fq.z;
+            angle_pair(pa, pb, th.x, t0.x, t0.y, F01p, F01q);
             t0 = __ldg(&cs0[1]);
-            angle_pair(pb, pc, th.y, t0.x, t0.y, Fp, Fq);
-            sm.arm.x[o + 2] = Fp.x; sm.arm.y[o + 2] = Fp.y; sm.arm.z[o + 2] = Fp.z;
-            sm.arm.x[o + 3] = Fq.x; sm.arm.y[o + 3] = Fq.y; sm.arm.z[o + 3] = Fq.z;
+            angle_pair(pb, pc, th.y, t0.x, t0.y, F12p, F12q);
             t0 = __ldg(&cs0[2]);
-            angle_pair(pa, pc, th.z, t0.x, t0.y, Fp, Fq);
-            sm.arm.x[o + 4] = Fp.x; sm.arm.y[o + 4] = Fp.y; sm.arm.z[o + 4] = Fp.z;
-            sm.arm.x[o + 5] = Fq.x; sm.arm.y[o + 5] = Fq.y; sm.arm.z[o + 5] = Fq.z;
+            angle_pair(pa, pc, th.z, t0.x, t0.y, F02p, F02q);
+            const int o = i * 3;
+            sm.arm.x[o] = F01p.x + F02p.x; sm.arm.y[o] = F01p.y + F02p.y; sm.arm.z[o] = F01p.z + F02p.z;
+            sm.arm.x[o + 1] = F01q.x + F12p.x; sm.arm.y[o + 1] = F01q.y + F12p.y; sm.arm.z[o + 1] = F01q.z + F12p.z;
+            sm.arm.x[o + 2] = F12q.x + F02q.x; sm.arm.y[o + 2] = F12q.y + F02q.y; sm.arm.z[o + 2] = F12q.z + F02q.z;
         }
         __syncthreads();
         if (i < NODES) {
@@ -637,16 +643,15 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
             // float once, as the reference stores it.
             double FX = 0.0, FY = 0.0, FZ = 0.0;
             if (isnan(x.x) || isnan(x.y) || isnan(x.z)) atomic_or_err(&d.st[inst], CS3D_ERRBIT_NAN);
-            // springs, src/propagate.cu:298-314
+            // springs, src/propagate.cu:298-314:
+            // k (R - R0) / R0 * d / R = k (1/R0 - 1/R) d
             const double stiff = d.E[a];
-            const float4 r0 = __ldg(&d.topo.r0[i]);
             const int nbr[3] = {n0, n1, n2};
-            const float r0v[3] = {r0.x, r0.y, r0.z};
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 const float3 dd = sub3(f3(sm.xs[nbr[k]]), x);
-                const double R = sqrt_nr((double)dd.x * dd.x + (double)dd.y * dd.y + (double)dd.z * dd.z);
-                const double c = stiff * (R - (double)r0v[k]) * rcp_nr((double)r0v[k] * R);
+                const double iR = rsqrt_nr((double)dd.x * dd.x + (double)dd.y * dd.y + (double)dd.z * dd.z);
+                const double c = stiff * (__ldg(&d.topo.r0i[3 * i + k]) - iR);
                 FX += c * dd.x; FY += c * dd.y; FZ += c * dd.z;
             }
             // internal pressure, src/propagate.cu:318-330 (CM of the previous step)
@@ -654,24 +659,18 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
                 const float4 cm = d.CM[a];
                 const float3 r = make_float3(x.x - cm.x, x.y - cm.y, x.z - cm.z);
                 const double c = 3.0 * (double)d.press[a] *
-                                 rcp_nr(sqrt_nr((double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z));
+                                 rsqrt_nr((double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z);
                 FX += c * r.x; FY += c * r.y; FZ += c * r.z;
             }
-            // bond angles, src/propagate.cu:81-181 (vertex terms then arm terms)
+            // bond angles, src/propagate.cu:81-181: the vertex terms (minus
+            // the arm forces of the angles at i) and the arm terms (the arm
+            // forces that the angles at the three neighbours send to i)
             if (P.angles) {
-                double ax = 0.0, ay = 0.0, az = 0.0;
-                const int o = i * 6;
-#pragma unroll
-                for (int q = 0; q < 3; ++q) {
-                    ax -= sm.arm.x[o + 2 * q] + sm.arm.x[o + 2 * q + 1];
-                    ay -= sm.arm.y[o + 2 * q] + sm.arm.y[o + 2 * q + 1];
-                    az -= sm.arm.z[o + 2 * q] + sm.arm.z[o + 2 * q + 1];
-                }
+                const int o = i * 3;
                 const uint4 am = __ldg(&d.topo.arm[i]);
-                const unsigned idx[6] = {am.x & 0xffffu, am.x >> 16, am.y & 0xffffu, am.y >> 16, am.z & 0xffffu, am.z >> 16};
-#pragma unroll
-                for (int q = 0; q < 6; ++q) { ax += sm.arm.x[idx[q]]; ay += sm.arm.y[idx[q]]; az += sm.arm.z[idx[q]]; }
-                FX += ax; FY += ay; FZ += az;
+                FX += sm.arm.x[am.x] + sm.arm.x[am.y] + sm.arm.x[am.z] - (sm.arm.x[o] + sm.arm.x[o + 1] + sm.arm.x[o + 2]);
+                FY += sm.arm.y[am.x] + sm.arm.y[am.y] + sm.arm.y[am.z] - (sm.arm.y[o] + sm.arm.y[o + 1] + sm.arm.y[o + 2]);
+                FZ += sm.arm.z[am.x] + sm.arm.z[am.y] + sm.arm.z[am.z] - (sm.arm.z[o] + sm.arm.z[o + 1] + sm.arm.z[o + 2]);
             }
             // contacts, src/propagate.cu:356-442 and the first dissipative sweep
             const float3 nrm = node_normal(sm.xs, n0, n1, n2, sgn);
