@@ -33,6 +33,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 NODE_BYTES = 48  # algorithmic bytes per node-step: float32 x and v, read and written once
+# DRAM bytes (read + write) per node of one k_s1 launch, from the ncu capture of
+# profiles/k_s1_packed30k.md (30k cells, 5.4M nodes: 334.8 MB + 194.0 MB), scaled
+# by the nodes of the launch
+S1_TRAFFIC_PER_NODE = 97.9
 
 
 def _peaks():
@@ -138,16 +142,10 @@ def run_cs3d(args, world, rank, local):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
     insts = build_workload(args.workload, args.cells)
     if args.workload == "ensemble256" and world > 1:
-        # shard instances across ranks by predicted cost (cells), greedy
-        order = sorted(range(len(insts)), key=lambda k: -insts[k][1]["n"])
-        load = [0] * world
-        mine = []
-        for k in order:
-            r = min(range(world), key=lambda q: load[q])
-            load[r] += insts[k][1]["n"]
-            if r == rank:
-                mine.append(k)
-        insts = [insts[k] for k in sorted(mine)]
+        # instances shard across ranks by predicted cost, no data-path collective
+        from cellsim3d_b200 import shard
+        mine = shard.partition([shard.predicted_cost(st) for _, st, _ in insts], world)[rank]
+        insts = [insts[k] for k in mine]
     topo = make_topology(insts)
     ens = cs.Ensemble([p for p, _, _ in insts], topo, [cap for _, _, cap in insts], device=local)
     for k, (p, st, cap) in enumerate(insts):
@@ -218,8 +216,12 @@ def run_cs3d(args, world, rank, local):
                        "l2": "inputs larger than L2 (no flush)" if n_nodes * 32 > 126e6 else "L2 resident",
                        "precision": "FP32 forces/integration, FP64 CoM/volume/division"},
             "roofline": {"bound": "hbm", "kernel": "s1_con_dis", "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "traffic": None,
-                         "peak_source": peak_kind,
+                         "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": S1_TRAFFIC_PER_NODE * n_nodes if args.workload == "packed100k" else None,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_s1 launch "
+                                           "on 30k cells, scaled by nodes (profiles/k_s1_packed30k.md)",
+                         "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                         else peak_kind,
                          "algorithmic_bytes_per_node": NODE_BYTES},
             "step_roofline": {"achieved": NODE_BYTES * value / 1e9 / world, "frac": NODE_BYTES * value / 1e9 / world / peak},
             "kernels_ms": {k: round(v, 4) for k, v in prof},
