@@ -388,6 +388,7 @@ int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topol
         total += capacity[k];
     }
     if (total > (1 << 23)) return CS3D_E_ARG;  // cell ids are packed in 24 bits for pair records
+    if (total * SLOTS * 2 > (1ll << 31) - SCAN_TILE) return CS3D_E_ARG;  // int bucket offsets of the node hash
     cs3d_ctx *c = new (std::nothrow) cs3d_ctx();
     if (!c) return CS3D_E_NOMEM;
     c->device = device;
@@ -428,7 +429,7 @@ int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topol
     AL(d.dmask, nodes); AL(d.dirty, c->cap_total);
     AL(d.Xb, nodes);
     AL(d.ent, (size_t)c->cap_total * MAXE * SLOTS); AL(d.nent, nodes);
-    d.hsize = hash_size(c->cap_total);
+    d.hsize = hash_size(2ll * c->cap_total);  // slices: a power of two >= nodes per instance
     AL(d.hcount, (size_t)d.hsize + SCAN_TILE); AL(d.hscan, (size_t)d.hsize / SCAN_TILE + 1); AL(d.hsz, 1);
     AL(d.hpos, nodes); AL(d.node_rank, nodes);
     AL(d.divtab, c->cap_total); AL(d.div_total, 1);
@@ -865,6 +866,7 @@ int cs3d_get_stats(cs3d_ctx *c, long long *stats, int n)
         v[1] += q.rebuilds;
         v[2] = std::max<long long>(v[2], q.max_entries);
         v[3] = std::max<long long>(v[3], q.max_cand);
+        v[6] += q.built;
     }
     for (int k = 0; k < n && k < 8; ++k) stats[k] = v[k];
     return CS3D_OK;
@@ -880,7 +882,7 @@ int cs3d_get_stats(cs3d_ctx *c, long long *stats, int n)
 namespace {
 
 constexpr int SCAP = CS3D_STATIC_MAX_CELLS;
-constexpr int SHASH = hash_size(SCAP);   // bucket rule of cs3d_create_ensemble
+constexpr int SHASH = hash_size(2 * SCAP);   // bucket rule of cs3d_create_ensemble
 constexpr int SEVENTS = 16;
 
 struct StaticScratch {

@@ -42,6 +42,9 @@ struct InstState {
     int div_count;         // divisions in the current step
     int force_rebuild;
     int max_entries, max_cand, max_halo;
+    unsigned hbase;        // first bucket of this instance's slice of the node hash
+    int hbits;             // log2 of the slice size (0: not rebuilding)
+    int built;             // cells whose lists were built (cumulative)
     int rebuilds;
     // RANMAR, src/marsaglia.h:50-52
     float u[98];
@@ -96,8 +99,8 @@ struct Dev {
     unsigned long long *dmask;  // [cell*192 + node] entries that are dissipative pairs this step
     // node-level spatial hash of the neighbour-list build: cubic bins of
     // edge ~rlist hashed (with the instance) into hsize buckets
-    int hsize;          // bucket capacity (power of two, >= SCAN_TILE)
-    int *hsz;           // buckets in use this build (power of two, SCAN_TILE..hsize)
+    int hsize;          // bucket capacity (>= twice the nodes of the capacity)
+    int *hsz;           // buckets in use this build (whole scan tiles, <= hsize)
     int *hcount;        // [hsize + SCAN_TILE] bucket counts, then exclusive starts
     int *hscan;         // [hsize / SCAN_TILE + 1] tile sums of the scan
     float4 *hpos;       // [cap_total*192] positions sorted by bucket, w = node id bits

@@ -37,6 +37,36 @@ __device__ __forceinline__ T warp_sum(T v)
 
 __device__ __forceinline__ void atomic_or_err(InstState *st, unsigned bits) { atomicOr(&st->err, bits); }
 
+// Block-wide exclusive scan (NT threads, NT a multiple of 32); wsum[32].
+template <int NT>
+__device__ __forceinline__ int block_excl_scan(int v, int *wsum, int &total)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        int s = lane < NT / 32 ? wsum[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        wsum[lane] = s;
+    }
+    __syncthreads();
+    const int r = (wid > 0 ? wsum[wid - 1] : 0) + x - v;
+    total = wsum[NT / 32 - 1];
+    __syncthreads();
+    return r;
+}
+
+
 // Active cells: the identity for a single instance, else the work table.
 __device__ __forceinline__ int n_work(const Dev &d) { return d.single ? d.st[0].n : *d.work_n; }
 __device__ __forceinline__ int cell_of(const Dev &d, int w) { return d.single ? w : d.work[w]; }
@@ -391,20 +421,45 @@ __global__ void __launch_bounds__(SLOTS) k_integrate(Dev d)
 // Per-step bookkeeping (one block): step counter, rebuild decision, reset of
 // the accumulators that this step fills.
 // ---------------------------------------------------------------------------
-// Buckets of the node hash for `nodes` nodes: the next power of two, within
-// [SCAN_TILE, hsize].
-__device__ __forceinline__ int hash_buckets(const Dev &d, long long nodes)
+// Hash slices of the list build: every rebuilding instance gets its own
+// power-of-two range of buckets (at least its node count), laid out back to
+// back; *d.hsz = their total rounded up to whole scan tiles.  Whole block
+// (256 threads), after the rebuild decisions.
+__device__ void assign_hash_slices(const Dev &d)
 {
-    int h = SCAN_TILE;
-    while (h < nodes && h < d.hsize) h <<= 1;
-    return h;
+    __shared__ int wsum[32];
+    __shared__ unsigned carry;
+    if (threadIdx.x == 0) carry = 0u;
+    __syncthreads();
+    for (int k0 = 0; k0 < d.n_inst; k0 += 256) {
+        const int k = k0 + threadIdx.x;
+        int size = 0;
+        if (k < d.n_inst) {
+            InstState *st = &d.st[k];
+            int bits = 0;
+            if (st->rebuild) {
+                bits = 6;
+                while ((1ll << bits) < (long long)st->n * NODES) ++bits;
+                size = 1 << bits;
+            }
+            st->hbits = bits;
+        }
+        int tot;
+        const int off = block_excl_scan<256>(size, wsum, tot);
+        if (k < d.n_inst) d.st[k].hbase = carry + (unsigned)off;
+        if (threadIdx.x == 0) carry += (unsigned)tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        unsigned h = (carry + SCAN_TILE - 1) / SCAN_TILE * SCAN_TILE;
+        *d.hsz = (int)(h < (unsigned)SCAN_TILE ? (unsigned)SCAN_TILE : h);
+    }
 }
 
-__global__ void k_step_begin(Dev d, int par_next)
+__global__ void __launch_bounds__(256) k_step_begin(Dev d, int par_next)
 {
     __shared__ int any;
-    __shared__ unsigned long long nodes;
-    if (threadIdx.x == 0) { any = 0; nodes = 0ull; *d.div_total = 0; }
+    if (threadIdx.x == 0) { any = 0; *d.div_total = 0; }
     __syncthreads();
     for (int k = threadIdx.x; k < d.n_inst; k += blockDim.x) {
         InstState *st = &d.st[k];
@@ -431,7 +486,6 @@ __global__ void k_step_begin(Dev d, int par_next)
         st->div_count = 0;
         if (full || part) {
             if (full) st->rebuilds += 1;
-            atomicAdd(&nodes, (unsigned long long)st->n * NODES);
             any = 1;
         }
         for (int q = 0; q < 3; ++q) {
@@ -440,19 +494,16 @@ __global__ void k_step_begin(Dev d, int par_next)
         }
     }
     __syncthreads();
+    assign_hash_slices(d);
     if (threadIdx.x == 0) {
         d.flags[0] = any;
         *d.n_pairs = 0ull;
-        *d.hsz = hash_buckets(d, (long long)nodes);
     }
 }
 
 // Init variant: rebuild everything, reset the grid accumulators.
-__global__ void k_init_begin(Dev d)
+__global__ void __launch_bounds__(256) k_init_begin(Dev d)
 {
-    __shared__ unsigned long long nodes;
-    if (threadIdx.x == 0) nodes = 0ull;
-    __syncthreads();
     for (int k = threadIdx.x; k < d.n_inst; k += blockDim.x) {
         InstState *st = &d.st[k];
         st->rebuild = 2;
@@ -465,14 +516,13 @@ __global__ void k_init_begin(Dev d)
                 st->mm[p][2 * q] = f2o(1.0e30f);
                 st->mm[p][2 * q + 1] = f2o(-1.0e30f);
             }
-        atomicAdd(&nodes, (unsigned long long)st->n * NODES);
     }
     __syncthreads();
+    assign_hash_slices(d);
     if (threadIdx.x == 0) {
         d.flags[0] = 1;
         *d.div_total = 0;
         *d.n_pairs = 0ull;
-        *d.hsz = hash_buckets(d, (long long)nodes);
     }
 }
 
@@ -1039,31 +1089,31 @@ __global__ void k_grid_fix(Dev d, int par)
 // ---------------------------------------------------------------------------
 // Neighbour-list build (instances whose displacement bound reached the skin,
 // or that divided).  The nodes are binned in cubes of edge hb slightly above
-// the list radius and the bins hashed into hsize buckets; a counting sort
-// puts the positions in bucket order (hpos).  Bucket of bin (ix, iy, iz):
-// the low bits of each coordinate side by side, plus an instance offset, so
-// that the 27 bins around a node fall in 27 distinct buckets and the three
+// the list radius and the bins hashed into the instance's slice of the
+// buckets; a counting sort puts the positions in bucket order (hpos).
+// Bucket of bin (ix, iy, iz): the low bits of each coordinate side by side,
+// so that the 27 bins around a node fall in 27 distinct buckets and the three
 // bins along x are (unless they wrap) three consecutive buckets.
 // ---------------------------------------------------------------------------
 struct BinGeom {
     float inv;          // 1 / bin edge
     int bx, by;         // bits of x, y in the bucket number
-    unsigned mask;      // hsize - 1
-    unsigned off;       // instance offset
+    unsigned mask;      // slice size - 1
+    unsigned base;      // first bucket of the instance's slice
 };
 
-__device__ __forceinline__ BinGeom bin_geom(const Dev &d, const InstParams &P, int inst)
+__device__ __forceinline__ BinGeom bin_geom(const Dev &d, int inst)
 {
+    const InstState &st = d.st[inst];
     BinGeom b;
     // bin edge 1% above the list radius: float rounding of x / edge cannot
     // put two nodes closer than the radius more than one bin apart
-    b.inv = 1.0f / ((d.st[inst].rcur + 1e-4f) * 1.01f);
-    const int hs = *d.hsz;
-    const int B = 31 - __clz(hs);
+    b.inv = 1.0f / ((st.rcur + 1e-4f) * 1.01f);
+    const int B = st.hbits;
     b.bx = B / 3;
     b.by = B / 3;
-    b.mask = (unsigned)hs - 1u;
-    b.off = (unsigned)inst * 2654435761u;
+    b.mask = (1u << B) - 1u;
+    b.base = st.hbase;
     return b;
 }
 
@@ -1076,36 +1126,7 @@ __device__ __forceinline__ unsigned bucket_of(const BinGeom &b, int ix, int iy, 
 {
     const unsigned code = ((unsigned)ix & ((1u << b.bx) - 1u)) | (((unsigned)iy & ((1u << b.by) - 1u)) << b.bx) |
                           ((unsigned)iz << (b.bx + b.by));
-    return (code + b.off) & b.mask;
-}
-
-// Block-wide exclusive scan (NT threads, NT a multiple of 32); wsum[32].
-template <int NT>
-__device__ __forceinline__ int block_excl_scan(int v, int *wsum, int &total)
-{
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    int x = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) wsum[wid] = x;
-    __syncthreads();
-    if (wid == 0) {
-        int s = lane < NT / 32 ? wsum[lane] : 0;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, s, o);
-            if (lane >= o) s += y;
-        }
-        wsum[lane] = s;
-    }
-    __syncthreads();
-    const int r = (wid > 0 ? wsum[wid - 1] : 0) + x - v;
-    total = wsum[NT / 32 - 1];
-    __syncthreads();
-    return r;
+    return b.base + (code & b.mask);
 }
 
 // B1: zero the bucket counts (hsize + SCAN_TILE entries, the tail pads the
@@ -1129,7 +1150,7 @@ __global__ void __launch_bounds__(SLOTS) k_nh_count(Dev d)
         const int a = cell_of(d, w);
         const int inst = inst_of(d, a);
         if (!d.st[inst].rebuild || i >= NODES) continue;
-        const BinGeom b = bin_geom(d, d.prm[inst], inst);
+        const BinGeom b = bin_geom(d, inst);
         const size_t g = (size_t)a * SLOTS + i;
         const float4 x = d.X[g];
         const unsigned k = bucket_of(b, bin_coord(x.x, b.inv), bin_coord(x.y, b.inv), bin_coord(x.z, b.inv));
@@ -1224,7 +1245,7 @@ __global__ void __launch_bounds__(SLOTS) k_nh_fill(Dev d)
         const int a = cell_of(d, w);
         const int inst = inst_of(d, a);
         if (!d.st[inst].rebuild || i >= NODES) continue;
-        const BinGeom b = bin_geom(d, d.prm[inst], inst);
+        const BinGeom b = bin_geom(d, inst);
         const size_t g = (size_t)a * SLOTS + i;
         const float4 x = d.X[g];
         const unsigned k = bucket_of(b, bin_coord(x.x, b.inv), bin_coord(x.y, b.inv), bin_coord(x.z, b.inv));
@@ -1271,7 +1292,7 @@ __global__ void __launch_bounds__(SLOTS) k_nl_cell(Dev d, int phase)
         if (phase == 1 && mark && i == 0) d.dirty[a] = 0;
         const bool build = phase == 0 ? (rb == 2 || mark == 1) : (rb == 1 && mark == 2);
         if (!build) continue;
-        const BinGeom b = bin_geom(d, d.prm[inst], inst);
+        const BinGeom b = bin_geom(d, inst);
         const float rl = st->rcur + 1e-4f;
         const float rl2 = rl * rl;
         for (int t = i; t < 256; t += SLOTS) sm.tkey[t] = -1;
@@ -1386,6 +1407,7 @@ __global__ void __launch_bounds__(SLOTS) k_nl_cell(Dev d, int phase)
         if (phase == 0 && rb == 1 && i < nc) atomicCAS(&d.dirty[d.cand[(size_t)a * MAXC + i]], 0, 2);
         if (i == 0) {
             if (nct > MAXC) atomicOr(&st->err, CS3D_ERRBIT_CAND_OVERFLOW);
+            atomicAdd(&st->built, 1);
             d.ncand[a] = nc;
             atomicMax(&st->max_cand, nct);
             atomicMax(&st->max_halo, nh);

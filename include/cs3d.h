@@ -269,7 +269,8 @@ int cs3d_last_error(cs3d_ctx *ctx, int inst, uint32_t *bits);
 
 /* Counters: [0] steps, [1] neighbour-list rebuilds, [2] max entries per node
  * seen, [3] max candidate cells per cell seen, [4] kernel launches per step,
- * [5] max distinct contact-candidate nodes (of other cells) per cell seen. */
+ * [5] max distinct contact-candidate nodes (of other cells) per cell seen,
+ * [6] cell neighbour lists built (cumulative). */
 int cs3d_get_stats(cs3d_ctx *ctx, long long *stats, int n);
 
 /* Profiling pass: n_steps steps launched kernel by kernel (not as a graph)
