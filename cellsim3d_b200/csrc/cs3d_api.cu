@@ -36,7 +36,7 @@ struct cs3d_ctx {
     int grid_nodes = 0;            // blocks of the neighbour-list kernels
     int grid_tiles = 0;            // blocks of the bucket scan
     int grid_s2 = 0;               // blocks of S2 and the integrator
-    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    cudaGraphExec_t graph[2][2][2][2] = {};  // [parity][division][integrate first][fused S2]
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     float last_ms = 0.f;
     long long launches_per_step = 0;
@@ -69,9 +69,11 @@ int dalloc(cs3d_ctx *c, T **p, size_t count)
 
 void free_all(cs3d_ctx *c)
 {
-    for (int p = 0; p < 2; ++p)
-        for (int q = 0; q < 2; ++q)
-            if (c->graph[p][q]) cudaGraphExecDestroy(c->graph[p][q]);
+    for (auto &a : c->graph)
+        for (auto &b : a)
+            for (auto &e : b)
+                for (cudaGraphExec_t g : e)
+                    if (g) cudaGraphExecDestroy(g);
     for (void *q : c->allocs) cudaFree(q);
     c->allocs.clear();
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -282,20 +284,24 @@ int run_init(cs3d_ctx *c)
 }
 
 // One timestep, src/GPUbounce.cu:1055-1338, as a fixed launch sequence.
-int launch_step(cs3d_ctx *c, int par, bool div, const Prof &pf = Prof())
+// k1: the step starts with k_integrate (else the previous step's fused S2
+// did it); fuse: S2 also integrates the next step (no division this step,
+// and the next step follows in the same call).
+int launch_step(cs3d_ctx *c, int par, bool div, bool k1 = true, bool fuse = false, const Prof &pf = Prof())
 {
     const Dev &d = c->d;
     cudaStream_t s = c->stream;
     int n = 0;
-    k_integrate<<<c->grid_s2, SLOTS, 0, s>>>(d); ++n; pf.mark(s, "integrate");
+    if (k1) { k_integrate<<<c->grid_s2, SLOTS, 0, s>>>(d); ++n; pf.mark(s, "integrate"); }
     k_step_begin<<<1, 256, 0, s>>>(d, par ^ 1); ++n; pf.mark(s, "step_begin");
     int rc = launch_nl_build(c, pf);
     if (rc) return rc;
     n += NL_LAUNCHES;
     k_s1<false><<<c->grid_cells, SLOTS, sizeof(S1Smem), s>>>(d, par); ++n; pf.mark(s, "s1_con_dis");
-    if (div) k_s2<true><<<c->grid_s2, SLOTS, 0, s>>>(d, par);
-    else k_s2<false><<<c->grid_s2, SLOTS, 0, s>>>(d, par);
-    ++n; pf.mark(s, "s2_dis_geom");
+    if (div) k_s2<true, false><<<c->grid_s2, SLOTS, 0, s>>>(d, par);
+    else if (fuse) k_s2<false, true><<<c->grid_s2, SLOTS, 0, s>>>(d, par);
+    else k_s2<false, false><<<c->grid_s2, SLOTS, 0, s>>>(d, par);
+    ++n; pf.mark(s, fuse ? "s2_dis_geom_integrate" : "s2_dis_geom");
     if (div) {
         k_div_select<<<c->n_inst, 256, 0, s>>>(d, par); ++n; pf.mark(s, "div_select");
         k_div_apply<<<c->grid_cells, SLOTS, 0, s>>>(d, par); ++n; pf.mark(s, "div_apply");
@@ -306,13 +312,13 @@ int launch_step(cs3d_ctx *c, int par, bool div, const Prof &pf = Prof())
     return CS3D_OK;
 }
 
-int get_graph(cs3d_ctx *c, int par, bool div, cudaGraphExec_t *out)
+int get_graph(cs3d_ctx *c, int par, bool div, bool k1, bool fuse, cudaGraphExec_t *out)
 {
-    cudaGraphExec_t &g = c->graph[par][div ? 1 : 0];
+    cudaGraphExec_t &g = c->graph[par][div ? 1 : 0][k1 ? 1 : 0][fuse ? 1 : 0];
     if (!g) {
         cudaGraph_t graph;
         CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-        int rc = launch_step(c, par, div);
+        int rc = launch_step(c, par, div, k1, fuse);
         cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
         if (rc) { if (e == cudaSuccess) cudaGraphDestroy(graph); return rc; }
         CK(e);
@@ -473,7 +479,7 @@ int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topol
     c->grid_nodes = std::max(1, std::min(c->cap_total, c->nsm * std::max(occ_nl, 1)));
     c->grid_tiles = std::max(1, std::min(d.hsize / SCAN_TILE + 1, c->nsm * 8));
     int occ_s2 = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s2, k_s2<true>, SLOTS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s2, k_s2<true, false>, SLOTS, 0);
     c->grid_s2 = std::max(1, std::min(c->cap_total, c->nsm * std::max(occ_s2, 1)));
     *out = c;
     return CS3D_OK;
@@ -525,9 +531,11 @@ int cs3d_set_option(cs3d_ctx *c, int option, long long value)
         return CS3D_E_ARG;
     }
     // launch parameters are baked into captured graphs: drop them
-    for (int p = 0; p < 2; ++p)
-        for (int q = 0; q < 2; ++q)
-            if (c->graph[p][q]) { cudaGraphExecDestroy(c->graph[p][q]); c->graph[p][q] = nullptr; }
+    for (auto &a : c->graph)
+        for (auto &b : a)
+            for (auto &e : b)
+                for (cudaGraphExec_t &g : e)
+                    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     return CS3D_OK;
 }
 
@@ -610,14 +618,17 @@ int cs3d_step(cs3d_ctx *c, int n_steps)
     int rc = ensure_init(c);
     if (rc) return rc;
     CK(cudaEventRecord(c->ev0, c->stream));
+    bool k1 = true;
     for (int k = 0; k < n_steps; ++k) {
         long long s = c->host_step + 1;
         int par = (int)((s - 1) & 1);
         bool div = c->any_growth && s <= c->max_div_steps;
+        bool fuse = !div && k + 1 < n_steps;
         cudaGraphExec_t g;
-        if ((rc = get_graph(c, par, div, &g))) return rc;
+        if ((rc = get_graph(c, par, div, k1, fuse, &g))) return rc;
         CK(cudaGraphLaunch(g, c->stream));
         c->host_step = s;
+        k1 = !fuse;
     }
     CK(cudaEventRecord(c->ev1, c->stream));
     CK(cudaEventSynchronize(c->ev1));
@@ -650,7 +661,7 @@ int cs3d_profile_step(cs3d_ctx *c, int n_steps, float *kernel_ms, char *names, i
         cudaEvent_t e0;
         CK(cudaEventCreate(&e0));
         CK(cudaEventRecord(e0, c->stream));
-        if ((rc = launch_step(c, par, div, pf))) return rc;
+        if ((rc = launch_step(c, par, div, true, false, pf))) return rc;
         c->host_step = st;
         CK(cudaEventSynchronize(ev.empty() ? e0 : ev.back()));
         if (acc.size() < ev.size()) { acc.resize(ev.size(), 0.0); first_names = nm; }

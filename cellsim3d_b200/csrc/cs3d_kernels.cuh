@@ -784,10 +784,14 @@ __device__ __forceinline__ void flush_mm(Dev &d, int inst, int pn, const float *
     }
 }
 
-template <bool DIV>
+// FUSE (steps without division that are followed by another step of the
+// same launch sequence): the first half kick and drift of the next step
+// (k_integrate) are done here, on the force and velocity in registers.
+template <bool DIV, bool FUSE>
 __global__ void __launch_bounds__(SLOTS, 5) k_s2(Dev d, int par)
 {
     __shared__ S2Smem sm;
+    __shared__ float smax[SLOTS / 32];
     const int W = n_work(d);
     const int i = threadIdx.x;
     const int pn = par ^ 1;
@@ -809,13 +813,36 @@ __global__ void __launch_bounds__(SLOTS, 5) k_s2(Dev d, int par)
         sm.xs[i] = x4;
         sm.vs[i] = v4;
         __syncthreads();
+        float disp = 0.0f;
         if (i < NODES) {
             const float3 v = f3(v4);
             const float3 nrm = node_normal(sm.xs, n0, n1, n2, sgn);
             const double3 vt = sweep_s2(d, sm.cell, a, i, v, nrm, dm);
             const float3 fd = dis_force(P, sm.vs, n0, n1, n2, v, vt);
             d.FD[g] = make_float4(fd.x, fd.y, fd.z, 0.f);
-            d.V[g] = v4;
+            if (FUSE) {
+                // Integrate + ForwardTime of the next step, src/propagate.cu:681-763
+                const float4 fc = d.FC[g];
+                const float dt = P.dt;
+                const double m = P.mass;
+                float4 vn = v4;
+                vn.x = kick(v4.x, __fadd_rn(__fmul_rn(dt, fc.x), __fmul_rn(dt, fd.x)), m);
+                vn.y = kick(v4.y, __fadd_rn(__fmul_rn(dt, fc.y), __fmul_rn(dt, fd.y)), m);
+                vn.z = kick(v4.z, __fadd_rn(__fmul_rn(dt, fc.z), __fmul_rn(dt, fd.z)), m);
+                const float4 xn = make_float4(__fmaf_rn(vn.x, dt, x4.x), __fmaf_rn(vn.y, dt, x4.y),
+                                              __fmaf_rn(vn.z, dt, x4.z), 0.0f);
+                const float4 xb = d.Xb[g];
+                const float ddx = xn.x - xb.x, ddy = xn.y - xb.y, ddz = xn.z - xb.z;
+                disp = sqrtf(ddx * ddx + ddy * ddy + ddz * ddz);
+                d.X[g] = xn;
+                d.V[g] = vn;
+            } else {
+                d.V[g] = v4;
+            }
+        }
+        if (FUSE) {
+            for (int o = 16; o > 0; o >>= 1) disp = fmaxf(disp, __shfl_xor_sync(0xffffffffu, disp, o));
+            if ((i & 31) == 0) smax[i >> 5] = disp;
         }
         float3 cm;
         float4 lo, hi;
@@ -839,6 +866,12 @@ __global__ void __launch_bounds__(SLOTS, 5) k_s2(Dev d, int par)
             }
         }
         if (i == 0) {
+            if (FUSE) {
+                float mx = smax[0];  // visible: cell_geom synchronises the block
+                for (int q = 1; q < SLOTS / 32; ++q) mx = fmaxf(mx, smax[q]);
+                atomicMax(&st->disp_step, __float_as_uint(mx));
+                if (d.press[a] < P.maxp) d.press[a] = d.press[a] + P.growth;  // PressureUpdate
+            }
             d.CM[a] = make_float4(cm.x, cm.y, cm.z, 0.f);
             d.aabb[pn][2 * a] = lo;
             d.aabb[pn][2 * a + 1] = hi;

@@ -166,3 +166,33 @@ def test_capacity_overflow_reports(mesh):
     rc = sim.step(1, raise_on_error=False)
     assert rc == -69
     assert sim.n_cells() == 12
+
+
+def test_multi_step_launch_equals_single_steps(mesh):
+    """cs3d_step(n) fuses the first half kick and drift of each step into the
+    previous step's last kernel; n single-step calls do not.  The two must
+    give bit-identical states (same float operations)."""
+    c, vel, L = W.packed_fcc(64, phi=0.5, seed=5)
+    p = W.base_params(box_len=(L, L, L), growth_rate=0.0, min_pressure=200.0, max_pressure=200.0,
+                      div_time_steps=5000)
+    st = W.state(c, velocities=vel)
+    topo, _ = topo_for(st, mesh)
+    sims = []
+    for mode in ("fused", "single"):
+        sim = cs.Simulation(p, topo, 64)
+        sim.load_state(st["X"], st["Y"], st["Z"], st["VX"], st["VY"], st["VZ"], n_cells=st["n"])
+        if mode == "fused":
+            sim.step(25)
+        else:
+            for _ in range(25):
+                sim.step(1)
+        sims.append(sim)
+    a, b = sims[0].state(), sims[1].state()
+    for k in ("X", "Y", "Z", "VX", "VY", "VZ", "pressure"):
+        assert np.array_equal(a[k].view(np.uint32), b[k].view(np.uint32)), k
+    fa, fb = sims[0].forces(), sims[1].forces()
+    for k in fa:
+        assert np.array_equal(fa[k].view(np.uint32), fb[k].view(np.uint32)), k
+    assert sims[0].stats()["rebuilds"] == sims[1].stats()["rebuilds"]
+    for sim in sims:
+        sim.close()
