@@ -109,7 +109,7 @@ def dist_env():
     return world, rank, local
 
 
-def build_workload(name, cells, seed=123):
+def build_workload(name, cells, seed=123, steps=0):
     from cellsim3d_b200 import workloads as W
     if name == "packed100k":
         c, vel, L = W.packed_fcc(cells, phi=0.5, seed=seed)
@@ -120,7 +120,9 @@ def build_workload(name, cells, seed=123):
         p, st, cap = W.config2()
         return [(p, st, cap)]
     if name == "ensemble256":
-        return [(p, st, 1024) for p, st in W.config4()]
+        # capacity per instance: 10k steps grow the largest instance to ~4500 cells
+        cap = 1024 if steps <= 500 else 6000
+        return [(p, st, cap) for p, st in W.config4()]
     raise ValueError(name)
 
 
@@ -140,7 +142,8 @@ def run_cs3d(args, world, rank, local):
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
-    insts = build_workload(args.workload, args.cells)
+    insts = build_workload(args.workload, args.cells, steps=args.warmup + args.steps)
+    n_total = len(insts)
     if args.workload == "ensemble256" and world > 1:
         # instances shard across ranks by predicted cost, no data-path collective
         from cellsim3d_b200 import shard
@@ -233,6 +236,13 @@ def run_cs3d(args, world, rank, local):
             "max_halo": stats["max_halo"],
             "clocks": clk.summary(),
         }
+        if args.workload == "ensemble256":
+            # whole simulations per hour: the timed steps stand for the run of
+            # warmup + steps steps of every instance
+            secs = ms_max * 1e-3 * (args.warmup + args.steps) / args.steps
+            result["ensemble"] = {"instances": n_total, "steps_per_sim": args.warmup + args.steps,
+                                  "cells_start": cells_before, "cells_end": cells_after,
+                                  "sims_per_hour": n_total * 3600.0 / secs}
         if e2e:
             result["e2e"] = {"value": e2e["node_steps"] * world / e2e["seconds"] if world == 1 else
                              e2e["node_steps"] / e2e["seconds"] * world,
@@ -292,29 +302,58 @@ def run_reference(args):
                              "d2h_bytes_per_step": 0}})
         return line
     import cellsim3d_b200 as cs
-    insts = build_workload(args.workload, args.cells)
+    from concurrent.futures import ThreadPoolExecutor
+    insts = build_workload(args.workload, args.cells, steps=args.warmup + args.steps)
     topo = make_topology(insts)
+    n_all = len(insts)
+    if args.ref_sample and args.ref_sample < n_all:
+        # stratified by initial cell count: every (n_all / k)-th instance in size order
+        order = sorted(range(n_all), key=lambda k: (insts[k][1]["n"], k))
+        pick = sorted({order[int(round(q * (n_all - 1) / (args.ref_sample - 1)))] for q in range(args.ref_sample)})
+        insts = [insts[k] for k in pick]
     total_ms, node_steps, cells0 = 0.0, 0.0, 0
     statuses, max_bin, max_nn, guard = set(), 0, 0, 0.0
+
+    def one(inst):
+        p, st, cap = inst
+        return st, ref.run(cs.make_params(p), topo, st, cap, args.warmup + args.steps, warmup=args.warmup)
+
     with ClockSampler(0) as clk:
-        for p, st, cap in insts:
-            r = ref.run(cs.make_params(p), topo, st, cap, args.warmup + args.steps, warmup=args.warmup)
+        # one simulation after another (device time of each timed region)
+        for st, r in map(one, insts):
             timed = r["steps"] - args.warmup
             if timed <= 0:
                 raise RuntimeError("reference stopped in the warm-up: " + r["status_text"])
-            ms = r["total_ms"] - r["guard_ms"]
-            total_ms += ms
+            total_ms += r["total_ms"] - r["guard_ms"]
             node_steps += 0.5 * (st["n"] + r["n"]) * 180 * timed   # cell count grows by division
             cells0 += st["n"]
             statuses.add(r["status_text"])
             max_bin, max_nn = max(max_bin, r["max_bin"]), max(max_nn, r["max_local_nn"])
             guard += r["guard_ms"]
+        conc = None
+        if len(insts) > 1 and args.ref_concurrency > 1:
+            # the same simulations as concurrent processes sharing the GPU
+            # (wall time of the whole batch, process start-up included)
+            t0 = time.perf_counter()
+            with ThreadPoolExecutor(args.ref_concurrency) as ex:
+                list(ex.map(one, insts))
+            conc = time.perf_counter() - t0
     value = node_steps / (total_ms * 1e-3)
+    extra = {}
+    if conc is not None:
+        extra = {"sequential_node_steps_per_s": value, "concurrent_node_steps_per_s": node_steps / conc,
+                 "concurrent_processes": args.ref_concurrency,
+                 "sims_per_hour_sequential": len(insts) * 3600.0 / (total_ms * 1e-3),
+                 "sims_per_hour_concurrent": len(insts) * 3600.0 / conc}
+        value = max(value, node_steps / conc)
     line.update({
         "value": value, "ms_per_step": total_ms / args.steps, "dtype": "f32",
-        "config": {"workload": args.workload, "cells": cells0, "instances": len(insts),
-                   "instances_run": "one after another" if len(insts) > 1 else "single system",
+        "config": {"workload": args.workload, "cells": cells0, "instances": len(insts), "instances_total": n_all,
+                   "instances_run": ("a stratified sample, " if len(insts) < n_all else "") +
+                                    ("one after another and %d at a time (best kept)" % args.ref_concurrency
+                                     if conc is not None else "single system"),
                    "l2": "inputs larger than L2 (no flush)" if cells0 * 192 * 24 > 126e6 else "L2 resident"},
+        "ensemble": extra,
         "reference_build": {"kernels": "src/propagate.cu, centermass.cu, volume.cu, propagatebound.cu, "
                                        "PressureKernels.cu, postscriptinit.cu compiled unmodified for sm_100a "
                                        "(oracle/ref.mk)",
@@ -342,6 +381,10 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ref-sample", type=int, default=0,
+                    help="reference arm, ensembles: run a stratified sample of this many instances (0: all)")
+    ap.add_argument("--ref-concurrency", type=int, default=8,
+                    help="reference arm, ensembles: also run the simulations this many at a time")
     args = ap.parse_args()
     world, rank, local = dist_env()
     if args.warmup < 3:

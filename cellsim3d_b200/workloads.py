@@ -226,3 +226,60 @@ def config5(n_inst=64, master_seed=2025):
                         div_time_steps=10 ** 9, rng_ij=ij, rng_kl=kl)
         inst.append((p, state(c)))
     return inst
+
+
+def inp_json(p, max_cells, steps, traj_write_int, traj_file="traj.bin", seed=42, binary=True):
+    """The reference's inp.json (src/GPUbounce.cu:1938-2096 keys) for the
+    hot-path parameters `p` (base_params layout); features off the path are
+    switched off.  youngs_mod is the contact modulus, stiffness1 the bond
+    stiffness (stiffFactor1 = stiffness1 / youngs_mod)."""
+    return {
+        "core": {"MaxNoofC180s": int(max_cells), "particle_mass": p["particle_mass"],
+                 "repulsion_range": p["repulsion_range"], "attraction_range": p["attraction_range"],
+                 "repulsion_strength": p["repulsion_strength"], "attraction_strength": p["attraction_strength"],
+                 "Youngs_mod": p["youngs_mod"], "stiffFactor1": p["stiffness1"] / p["youngs_mod"],
+                 "viscotic_damping": p["viscotic_damping"], "internal_damping": p["internal_damping"],
+                 "gamma_visc": p["gamma_visc"], "division_Vol": p["division_vol"], "random_z_offset?": 0,
+                 "z_offset": 0.0, "div_time_steps": int(steps), "time_interval": p["time_interval"],
+                 "Restart": 0, "trajWriteInt": int(traj_write_int), "non_div_time_steps": 0,
+                 "trajFileName": traj_file, "binaryOutput": 1 if binary else 0,
+                 "maxPressure": p["max_pressure"], "minPressure": p["min_pressure"],
+                 "growth_rate": p["growth_rate"], "checkSphericity": bool(p["check_sphericity"]),
+                 "constrainAngles": bool(p["constrain_angles"]), "doAdaptive_dt": False, "dt_max": 1e-4,
+                 "dt_tol": 1e-8, "phase_count": 2000000000, "write_cont_force": False,
+                 "forces_file": "forces.csv", "correct_com": False},
+        "counting": {"mit-index_file_name": "mit-index.dat", "count_only_internal_cells?": False,
+                     "radius_cutoff": 0.6, "overwrite_mit_ind_file?": True,
+                     "cell_count_int": max(1, min(1000, int(steps)))},
+        "population": {"doPopModel": 0, "totalFood": 5000.0, "regular_consumption": 2.0,
+                       "division_consumption": 10.0, "death_release_food": 10.0, "cellLifeTime": 20000,
+                       "max_pop": 1024},
+        "walls": {"useWalls": 0, "perpAxis": "Z", "dAxis": 1.0, "wallLen": 10.0, "wallWidth": 10.0,
+                  "threshDist": p["thresh_dist"]},
+        "divParams": {"useDivPlaneBasis": 0, "divPlaneBasisX": 0.0, "divPlaneBasisY": 1.0, "divPlaneBasisZ": 0.0},
+        "stiffnessParams": {"useDifferentStiffnesses": False, "softStiffFactor": 1.0, "numberOfSofterCells": 0,
+                            "duringGrowth": False, "closenessToCenter": 0.0, "startAtPop": 0,
+                            "fractionOfSofterCells": 0.0, "chooseRandomCellIndices": False,
+                            "daughtSameStiffness": bool(p["daught_same_stiffness"]), "recalc_r0": False},
+        "boxParams": {"useRigidSimulationBox": bool(p["use_rigid_box"]), "usePBCs": False,
+                      "boxLength": float(p["box_len"][0]), "box_len_x": float(p["box_len"][0]),
+                      "box_len_y": float(p["box_len"][1]), "box_len_z": float(p["box_len"][2]),
+                      "flatbox": False, "rand_pos": False},
+        "rand_params": {"add_rands": False, "rand_seed": int(seed), "rand_dist": 0, "rand_scale_factor": 0.1},
+    }
+
+
+def write_init_file(path, st):
+    """The CS3D_INIT_FILE format of the cs3d driver: "CS3DINIT", int32 n,
+    float32 X, Y, Z, VX, VY, VZ [n*192], pressure [n], youngs [n]."""
+    n = int(st["n"])
+    k = n * 192
+    zeros = np.zeros(k, np.float32)
+    with open(path, "wb") as f:
+        f.write(b"CS3DINIT")
+        f.write(np.int32(n).tobytes())
+        for key in ("X", "Y", "Z", "VX", "VY", "VZ"):
+            a = st.get(key)
+            f.write((np.asarray(a, np.float32)[:k] if a is not None else zeros).tobytes())
+        f.write(np.asarray(st.get("pressure", np.full(n, 0.0)), np.float32)[:n].tobytes())
+        f.write(np.asarray(st.get("youngs", np.full(n, 0.0)), np.float32)[:n].tobytes())

@@ -161,3 +161,23 @@ def single_step_check(sim, tag="", tol=TOL, check_pairs=True):
     O.close()
     O2.close()
     return res
+
+
+def write_mesh_files(d, mesh):
+    """The reference's mesh files (C180, C180NN, C180C, C180_pentahexa) from
+    the fixture, in the reference's text formats."""
+    import os
+    with open(os.path.join(d, "C180"), "w") as f:
+        for p in mesh["xyz"]:
+            f.write("%.9g  %.9g  %.9g\n" % tuple(float(v) for v in p))
+    with open(os.path.join(d, "C180NN"), "w") as f:
+        for i in range(180):
+            f.write(" %d,  %d,  %d,  %d\n" % (mesh["nn"][0, i] + 1, mesh["nn"][1, i] + 1, mesh["nn"][2, i] + 1,
+                                            mesh["sign"][i]))
+    with open(os.path.join(d, "C180C"), "w") as f:
+        for a, b in mesh["bonds"]:
+            f.write(" %d,  %d\n" % (a + 1, b + 1))
+    with open(os.path.join(d, "C180_pentahexa"), "w") as f:
+        for k in range(92):
+            m = 5 if k < 12 else 6
+            f.write("  ".join(str(v) for v in mesh["faces"][k, :m]) + "\n")
