@@ -109,7 +109,7 @@ def dist_env():
     return world, rank, local
 
 
-def build_workload(name, cells, seed=123, steps=0):
+def build_workload(name, cells, seed=123, steps=0, instances=0):
     from cellsim3d_b200 import workloads as W
     if name == "packed100k":
         c, vel, L = W.packed_fcc(cells, phi=0.5, seed=seed)
@@ -122,7 +122,13 @@ def build_workload(name, cells, seed=123, steps=0):
     if name == "ensemble256":
         # capacity per instance: 10k steps grow the largest instance to ~4500 cells
         cap = 1024 if steps <= 500 else 6000
-        return [(p, st, cap) for p, st in W.config4()]
+        insts = [(p, st, cap) for p, st in W.config4()]
+        if instances and instances < len(insts):
+            # a stratified subset (by initial cell count) for small profiling runs
+            order = sorted(range(len(insts)), key=lambda k: (insts[k][1]["n"], k))
+            pick = sorted({order[int(round(q * (len(insts) - 1) / max(instances - 1, 1)))] for q in range(instances)})
+            insts = [insts[k] for k in pick]
+        return insts
     raise ValueError(name)
 
 
@@ -142,7 +148,7 @@ def run_cs3d(args, world, rank, local):
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
-    insts = build_workload(args.workload, args.cells, steps=args.warmup + args.steps)
+    insts = build_workload(args.workload, args.cells, steps=args.warmup + args.steps, instances=args.instances)
     n_total = len(insts)
     if args.workload == "ensemble256" and world > 1:
         # instances shard across ranks by predicted cost, no data-path collective
@@ -381,6 +387,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--instances", type=int, default=0,
+                    help="ensemble256: a stratified subset of this many instances (0: all 256)")
     ap.add_argument("--ref-sample", type=int, default=0,
                     help="reference arm, ensembles: run a stratified sample of this many instances (0: all)")
     ap.add_argument("--ref-concurrency", type=int, default=8,

@@ -432,7 +432,7 @@ int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topol
     AL(d.cell_inst, c->cap_total);
     AL(d.work, c->cap_total); AL(d.work_n, 1);
     AL(d.cand, (size_t)c->cap_total * MAXC); AL(d.ncand, c->cap_total);
-    AL(d.dmask, nodes); AL(d.dirty, c->cap_total);
+    AL(d.dlist, (size_t)c->cap_total * MAXD * SLOTS); AL(d.ndis, nodes); AL(d.dirty, c->cap_total);
     AL(d.Xb, nodes);
     AL(d.ent, (size_t)c->cap_total * MAXE * SLOTS); AL(d.nent, nodes);
     d.hsize = hash_size(2ll * c->cap_total);  // slices: a power of two >= nodes per instance
@@ -909,7 +909,8 @@ struct StaticScratch {
     int hscan[SHASH / SCAN_TILE + 1], node_rank[SCAP * SLOTS], hsz;
     int cell_inst[SCAP], work[SCAP], work_n;
     int cand[SCAP * MAXC], ncand[SCAP];
-    unsigned long long dmask[SCAP * SLOTS];
+    uint16_t dlist[SCAP * MAXD * SLOTS];
+    uint8_t ndis[SCAP * SLOTS];
     int dirty[SCAP];
     uint16_t ent[SCAP * MAXE * SLOTS];
     uint8_t nent[SCAP * SLOTS];
@@ -965,7 +966,7 @@ Dev static_dev(StaticScratch *s)
     d.aabb[0] = s->aabb0; d.aabb[1] = s->aabb1;
     d.cell_inst = s->cell_inst; d.work = s->work; d.work_n = &s->work_n;
     d.cand = s->cand; d.ncand = s->ncand;
-    d.dmask = s->dmask; d.dirty = s->dirty;
+    d.dlist = s->dlist; d.ndis = s->ndis; d.dirty = s->dirty;
     d.ent = s->ent; d.nent = s->nent;
     d.hsize = SHASH; d.hsz = &s->hsz; d.hcount = s->hcount; d.hscan = s->hscan; d.hpos = s->hpos; d.node_rank = s->node_rank;
     d.divtab = s->divtab; d.div_total = &s->div_total;

@@ -12,6 +12,7 @@ constexpr int SLOTS = CS3D_SLOTS;      // node slots per cell (reference padding
 constexpr int NODES = CS3D_NODES;      // real nodes per cell
 constexpr int MAXC = CS3D_MAX_CAND;    // contact-candidate cells per cell
 constexpr int MAXE = CS3D_MAX_ENTRIES; // contact-candidate nodes per node
+constexpr int MAXD = CS3D_MAX_DIS;     // dissipative pairs per node
 constexpr int SCAN_TILE = 4096;        // elements per block of the bucket scan
 constexpr float DL = 2.9f;             // reference grid spacing, src/GPUbounce.cu:756
 
@@ -96,7 +97,10 @@ struct Dev {
     // that cell
     uint16_t *ent;      // [(cell*MAXE + k)*192 + node]
     uint8_t *nent;      // [cell*192 + node]
-    unsigned long long *dmask;  // [cell*192 + node] entries that are dissipative pairs this step
+    // the dissipative pairs S1 found this step (slot << 8 | node, in entry
+    // order), read by S2: positions do not change in between
+    uint16_t *dlist;    // [(cell*MAXD + k)*192 + node]
+    uint8_t *ndis;      // [cell*192 + node]
     // node-level spatial hash of the neighbour-list build: cubic bins of
     // edge ~rlist hashed (with the instance) into hsize buckets
     int hsize;          // bucket capacity (>= twice the nodes of the capacity)

@@ -245,15 +245,15 @@ __device__ __forceinline__ unsigned entry_at(const uint16_t *ep, const uint32_t 
 // Partner positions and velocities are read from global memory (L1/L2
 // resident: the partners of a cell are a few hundred nodes).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ unsigned long long sweep_s1(const Dev &d, const InstParams &P, const SlotData &sd, int a,
-                                                       int i, float3 x, float3 v, float3 nrm, int ne,
-                                                       const uint32_t (&pre)[EPRE / 2], double &FX, double &FY,
-                                                       double &FZ, double3 &vt)
+__device__ __forceinline__ int sweep_s1(const Dev &d, const InstParams &P, const SlotData &sd, int a, int i, float3 x,
+                                        float3 v, float3 nrm, int ne, const uint32_t (&pre)[EPRE / 2], double &FX,
+                                        double &FY, double &FZ, double3 &vt)
 {
     const uint16_t *ep = d.ent + (size_t)a * MAXE * SLOTS + i;
+    uint16_t *dl = d.dlist + (size_t)a * MAXD * SLOTS + i;
     SlotPred sp;
     pred_init(sp, sd, x);
-    unsigned long long dm = 0ull;
+    int nd = 0;
     for (int k0 = 0; k0 < ne; k0 += SB) {
         unsigned e[SB];
 #pragma unroll
@@ -274,7 +274,8 @@ __device__ __forceinline__ unsigned long long sweep_s1(const Dev &d, const InstP
             const float dx = __fsub_rn(x.x, xj[q].x), dy = __fsub_rn(x.y, xj[q].y), dz = __fsub_rn(x.z, xj[q].z);
             const float r2 = r2_nc(dx, dy, dz);
             if (r2 > P.ra2) { id[q] = -1; continue; }
-            dm |= 1ull << (k0 + q);
+            if (nd < MAXD) dl[(size_t)nd * SLOTS] = (uint16_t)e[q];
+            ++nd;
             if (d.record_pairs) {
                 const unsigned long long slot = atomicAdd(d.n_pairs, 1ull);
                 if ((long long)slot < d.pair_cap)
@@ -308,34 +309,27 @@ __device__ __forceinline__ unsigned long long sweep_s1(const Dev &d, const InstP
             vt.z += vz - dn * nrm.z;
         }
     }
-    return dm;
+    return nd;
 }
 
-// S2 sweep: tangential velocity sum over the dissipative pairs found by S1,
-// with the velocities after the half kicks.
-__device__ __forceinline__ double3 sweep_s2(const Dev &d, const int *cell, int a, int i, float3 v, float3 nrm,
-                                            unsigned long long dm)
+// S2 sweep: tangential velocity sum over the dissipative pairs found by S1
+// (their list, in column layout), with the velocities after the half kicks.
+__device__ __forceinline__ double3 sweep_s2(const Dev &d, const int *cell, int a, int i, float3 v, float3 nrm, int nd)
 {
-    const uint16_t *ep = d.ent + (size_t)a * MAXE * SLOTS + i;
+    const uint16_t *dl = d.dlist + (size_t)a * MAXD * SLOTS + i;
     double3 vt = make_double3(0.0, 0.0, 0.0);
-    while (dm) {
-        int id[SB];
+    for (int k0 = 0; k0 < nd; k0 += SB) {
+        unsigned e[SB];
 #pragma unroll
-        for (int q = 0; q < SB; ++q) {
-            id[q] = -1;
-            if (dm) {
-                const int k = __ffsll((long long)dm) - 1;
-                dm &= dm - 1ull;
-                const unsigned e = ep[(size_t)k * SLOTS];
-                id[q] = cell[e >> 8] * SLOTS + (int)(e & 255u);
-            }
-        }
+        for (int q = 0; q < SB; ++q) e[q] = k0 + q < nd ? dl[(size_t)(k0 + q) * SLOTS] : 0xffffu;
         float4 vj[SB];
 #pragma unroll
-        for (int q = 0; q < SB; ++q) vj[q] = id[q] >= 0 ? __ldg(&d.Vb[id[q]]) : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int q = 0; q < SB; ++q)
+            vj[q] = e[q] != 0xffffu ? __ldg(&d.Vb[cell[e[q] >> 8] * SLOTS + (int)(e[q] & 255u)])
+                                    : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
         for (int q = 0; q < SB; ++q) {
-            if (id[q] < 0) continue;
+            if (e[q] == 0xffffu) continue;
             const double vx = (double)v.x - vj[q].x, vy = (double)v.y - vj[q].y, vz = (double)v.z - vj[q].z;
             const double dn = vx * nrm.x + vy * nrm.y + vz * nrm.z;
             vt.x += vx - dn * nrm.x;
@@ -345,6 +339,7 @@ __device__ __forceinline__ double3 sweep_s2(const Dev &d, const int *cell, int a
     }
     return vt;
 }
+
 // Unit surface normal of node i for the tangential friction,
 // src/propagate.cu:558-572.
 __device__ __forceinline__ float3 node_normal(const float4 *xs, int n0, int n1, int n2, float sgn)
@@ -725,7 +720,8 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
             // contacts, src/propagate.cu:356-442 and the first dissipative sweep
             const float3 nrm = node_normal(sm.xs, n0, n1, n2, sgn);
             double3 vt = make_double3(0.0, 0.0, 0.0);
-            const unsigned long long dm = sweep_s1(d, P, sm.sd, a, i, x, v, nrm, ne, pre, FX, FY, FZ, vt);
+            const int nd = sweep_s1(d, P, sm.sd, a, i, x, v, nrm, ne, pre, FX, FY, FZ, vt);
+            if (nd > MAXD) atomic_or_err(&d.st[inst], CS3D_ERRBIT_ENTRY_OVERFLOW);
             // rigid box walls, src/propagate.cu:474-510 (float gap tests)
             if (P.rigid) {
                 const double wk = P.wallk, th = P.thresh;
@@ -741,7 +737,7 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
             }
             const float3 fd = dis_force(P, sm.vs, n0, n1, n2, v, vt);
             d.FC[g] = make_float4((float)FX, (float)FY, (float)FZ, 0.f);
-            d.dmask[g] = dm;
+            d.ndis[g] = (uint8_t)(nd < MAXD ? nd : MAXD);
             if (INIT) {
                 d.FD[g] = make_float4(fd.x, fd.y, fd.z, 0.f);
             } else {
@@ -766,7 +762,7 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
 // S2: second dissipative force with the updated velocities
 // (src/GPUbounce.cu:1151), centre of mass (:1164), volumes and division
 // flags (:1172, DIV only), bounding boxes and grid extents for the next step
-// (:1312-1334).  The dissipative pairs are those S1 found (same positions).
+// (:1312-1334).  The dissipative pairs are those S1 listed (same positions).
 // ---------------------------------------------------------------------------
 struct S2Smem {
     float4 xs[SLOTS];
@@ -807,8 +803,8 @@ __global__ void __launch_bounds__(SLOTS, 5) k_s2(Dev d, int par)
         InstState *st = &d.st[inst];
         const size_t g = (size_t)a * SLOTS + i;
         float4 x4 = make_float4(0, 0, 0, 0), v4 = make_float4(0, 0, 0, 0);
-        unsigned long long dm = 0ull;
-        if (i < NODES) { x4 = d.X[g]; v4 = d.Vb[g]; dm = d.dmask[g]; }
+        int nd = 0;
+        if (i < NODES) { x4 = d.X[g]; v4 = d.Vb[g]; nd = d.ndis[g]; }
         if (i < MAXC) sm.cell[i] = d.cand[(size_t)a * MAXC + i];
         sm.xs[i] = x4;
         sm.vs[i] = v4;
@@ -817,7 +813,7 @@ __global__ void __launch_bounds__(SLOTS, 5) k_s2(Dev d, int par)
         if (i < NODES) {
             const float3 v = f3(v4);
             const float3 nrm = node_normal(sm.xs, n0, n1, n2, sgn);
-            const double3 vt = sweep_s2(d, sm.cell, a, i, v, nrm, dm);
+            const double3 vt = sweep_s2(d, sm.cell, a, i, v, nrm, nd);
             const float3 fd = dis_force(P, sm.vs, n0, n1, n2, v, vt);
             d.FD[g] = make_float4(fd.x, fd.y, fd.z, 0.f);
             if (FUSE) {

@@ -42,7 +42,7 @@ extern "C" {
 #define CS3D_ERRBIT_NAN            0x001u  /* NaN position, src/propagate.cu:241-248 */
 #define CS3D_ERRBIT_CAPACITY       0x002u  /* division past capacity */
 #define CS3D_ERRBIT_CAND_OVERFLOW  0x004u  /* > CS3D_MAX_CAND contact cells for one cell */
-#define CS3D_ERRBIT_ENTRY_OVERFLOW 0x008u  /* > CS3D_MAX_ENTRIES contact nodes for one node */
+#define CS3D_ERRBIT_ENTRY_OVERFLOW 0x008u  /* > CS3D_MAX_ENTRIES contact nodes or > CS3D_MAX_DIS pairs for one node */
 #define CS3D_ERRBIT_NONFINITE_VOL  0x010u  /* src/volume.cu:134-139 */
 #define CS3D_ERRBIT_BAD_NORMAL     0x020u  /* |n| != 1, src/postscriptinit.cu:215-219 */
 #define CS3D_ERRBIT_GRID_OVERFLOW  0x040u  /* reserved, never raised (the node hash cannot overflow) */
@@ -51,6 +51,7 @@ extern "C" {
 
 #define CS3D_MAX_CAND     128   /* contact-candidate cells per cell */
 #define CS3D_MAX_ENTRIES   64   /* contact-candidate nodes per node */
+#define CS3D_MAX_DIS       32   /* dissipative contact pairs per node and step */
 
 /* ---- parameters of the hot path (one simulation instance) ------------- */
 /* Field meaning and units are the reference's inp.json keys.              */

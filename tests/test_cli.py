@@ -45,8 +45,9 @@ def test_cli_trajectory_matches_library(tmp_path, mesh):
                        timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     hdr, frames = traj.read_traj(str(tmp_path / "traj.bin"))
-    assert hdr["max_cells"] == 256
     assert [f["step"] for f in frames] == [0, 100, 200, 300]
+    # the first header word ends as the final cell count, src/GPUbounce.cu:1508-1511
+    assert hdr["max_cells"] == frames[-1]["X"].shape[0]
 
     prm = cs.config_to_params(cs.read_json_params(str(tmp_path / "inp.json")))
     topo = cs.build_topology(cs.read_fullerene_nn(str(tmp_path)), st["X"][:192], st["Y"][:192], st["Z"][:192])
