@@ -527,6 +527,12 @@ int cs3d_set_option(cs3d_ctx *c, int option, long long value)
         c->need_init = true;
         break;
     }
+    case CS3D_OPT_REBUILD: {
+        if (int rc = ensure_init(c)) return rc;
+        k_force_rebuild<<<1, 256, 0, c->stream>>>(c->d);
+        CK(cudaGetLastError());
+        return CS3D_OK;  // no launch parameter changed: the graphs stay valid
+    }
     default:
         return CS3D_E_ARG;
     }

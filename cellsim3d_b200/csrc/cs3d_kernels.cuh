@@ -496,6 +496,12 @@ __global__ void __launch_bounds__(256) k_step_begin(Dev d, int par_next)
     }
 }
 
+// Whole-instance list rebuild of every instance at the next step.
+__global__ void k_force_rebuild(Dev d)
+{
+    for (int k = threadIdx.x; k < d.n_inst; k += blockDim.x) d.st[k].force_rebuild = 1;
+}
+
 // Init variant: rebuild everything, reset the grid accumulators.
 __global__ void __launch_bounds__(256) k_init_begin(Dev d)
 {
@@ -1151,6 +1157,8 @@ __device__ __forceinline__ int bin_coord(float v, float inv)
     return (int)floorf(fminf(fmaxf(v * inv, -1.0e9f), 1.0e9f));
 }
 
+constexpr int CB = 4;  // hash candidates loaded together in the list build
+
 __device__ __forceinline__ unsigned bucket_of(const BinGeom &b, int ix, int iy, int iz)
 {
     const unsigned code = ((unsigned)ix & ((1u << b.bx) - 1u)) | (((unsigned)iy & ((1u << b.by) - 1u)) << b.bx) |
@@ -1346,15 +1354,23 @@ __global__ void __launch_bounds__(SLOTS) k_nl_cell(Dev d, int phase)
                     unsigned kb, ke;
                     if (nrun == 1) { kb = k0; ke = k0 + 3u; }
                     else { kb = bucket_of(b, ix - 1 + u, jy, jz); ke = kb + 1u; }
-                    const int p1 = d.hcount[ke];
-                    for (int p = d.hcount[kb]; p < p1; ++p) {
-                        const float4 y = d.hpos[p];
+                    const int p0 = d.hcount[kb], p1 = d.hcount[ke];
+                    // candidates in batches: the loads of a batch are in flight together
+                    for (int p = p0; p < p1; p += CB) {
+                      float4 yb[CB];
+#pragma unroll
+                      for (int q = 0; q < CB; ++q)
+                          yb[q] = p + q < p1 ? d.hpos[p + q] : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+#pragma unroll
+                      for (int q = 0; q < CB; ++q) {
+                        const float4 y = yb[q];
                         const int id = __float_as_int(y.w);
+                        if (id < 0) continue;
+                        // the instance's own hash slice holds only its own nodes
                         const int c = id / SLOTS;
                         if (c == a) continue;
                         const float dx = x.x - y.x, dy = x.y - y.y, dz = x.z - y.z;
                         if (!(dx * dx + dy * dy + dz * dz < rl2)) continue;
-                        if (!d.single && d.cell_inst[c] != inst) continue;
                         int t = last_t;
                         if (c != last_c) {
                             t = -1;
@@ -1371,6 +1387,7 @@ __global__ void __launch_bounds__(SLOTS) k_nl_cell(Dev d, int phase)
                         atomicOr(&sm.mask[t][j >> 5], 1u << (j & 31));
                         if (cnt < MAXE) ep[(size_t)cnt * SLOTS] = (uint16_t)((t << 8) | j);
                         ++cnt;
+                      }
                     }
                 }
             }

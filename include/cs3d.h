@@ -253,6 +253,7 @@ int cs3d_get_grid(cs3d_ctx *ctx, int inst, float minmax[6], int divs[3]);
 #define CS3D_OPT_RECORD_PAIRS  1   /* value 0/1: record the contact pairs used */
 #define CS3D_OPT_SKIN          2   /* value = skin length in units of 1e-6 */
 #define CS3D_OPT_PAIR_CAPACITY 3   /* value = max recorded pairs */
+#define CS3D_OPT_REBUILD       4   /* value ignored: rebuild every neighbour list at the next step */
 int cs3d_set_option(cs3d_ctx *ctx, int option, long long value);
 
 /* Contact pairs recorded during the last force evaluation (requires
