@@ -51,7 +51,7 @@ def build(verbose=False, force=False, extra_nvflags=()):
         _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", LIB, host_o, api_o], verbose)
     main_src = os.path.join(CSRC, "cs3d_main.cpp")
     if force or _stale(CLI, [main_src, LIB] + hdrs):
-        _run(["g++"] + CXXFLAGS + [main_src, "-o", CLI, "-L" + HERE, "-lcs3d",
+        _run(["g++"] + CXXFLAGS + ["-pthread", main_src, "-o", CLI, "-L" + HERE, "-lcs3d",
                                    "-Wl,-rpath,$ORIGIN"], verbose)
     return LIB
 

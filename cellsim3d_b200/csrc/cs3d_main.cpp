@@ -18,6 +18,7 @@
 #include <cstring>
 #include <ctime>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/cs3d.h"
@@ -149,12 +150,26 @@ int main(int argc, char **argv)
     int frame = 1;
     int step = 0;
     int n = n0;
+    // Frames are written by a second thread from one of two host buffers
+    // while the GPU steps on (the reference writes them on the step loop's
+    // thread, src/GPUbounce.cu:1430-1470).
+    std::vector<float> WB[2][3];
+    for (auto &b : WB)
+        for (auto &v : b) v.assign(cap_nodes, 0.f);
+    std::thread writer;
+    int wrc = 0;
+    int buf = 0;
+    auto join_writer = [&]() {
+        if (writer.joinable()) writer.join();
+        return wrc;
+    };
     while (step < total_steps) {
         int chunk = interval - step % interval;
         if (step + chunk > total_steps) chunk = total_steps - step;
         rc = cs3d_step(ctx, chunk);
         step += chunk;
         if (rc) {
+            join_writer();
             uint32_t bits = 0;
             cs3d_last_error(ctx, 0, &bits);
             fprintf(stderr, "cs3d: step %d: %s (error bits 0x%x)\n", step, cs3d_strerror(rc), bits);
@@ -170,13 +185,21 @@ int main(int argc, char **argv)
         }
         if (step % interval == 0) {
             ++frame;
-            if ((rc = cs3d_get_state(ctx, 0, &n, X.data(), Y.data(), Z.data(), nullptr, nullptr, nullptr, nullptr, nullptr)))
+            std::vector<float> *b = WB[buf];
+            if ((rc = cs3d_get_state(ctx, 0, &n, b[0].data(), b[1].data(), b[2].data(), nullptr, nullptr, nullptr,
+                                     nullptr, nullptr))) {
+                join_writer();
                 return fail("reading the state", rc);
-            if (traj) rc = cs3d_traj_write_frame(traj, step, frame, n, X.data(), Y.data(), Z.data(), nullptr);
-            else write_ascii_frame(ascii, step, interval, n, X.data(), Y.data(), Z.data());
-            if (rc) return fail("trajectory frame", rc);
+            }
+            if (join_writer()) return fail("trajectory frame", wrc);
+            writer = std::thread([&wrc, traj, ascii, b, step, frame, interval, nn = n]() {
+                if (traj) wrc = cs3d_traj_write_frame(traj, step, frame, nn, b[0].data(), b[1].data(), b[2].data(), nullptr);
+                else write_ascii_frame(ascii, step, interval, nn, b[0].data(), b[1].data(), b[2].data());
+            });
+            buf ^= 1;
         }
     }
+    if (join_writer()) return fail("trajectory frame", wrc);
     cs3d_get_state(ctx, 0, &n, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
     if (traj) cs3d_traj_close(traj, n);
     if (ascii) fclose(ascii);
