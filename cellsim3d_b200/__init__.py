@@ -251,6 +251,14 @@ class Ensemble:
         _lib.check(st, "cs3d_get_forces")
         return a
 
+    def random_force(self, inst=0):
+        """Langevin random force of the last step (192-stride SoA)."""
+        n = self.n_cells(inst)
+        a = {key: np.zeros(n * 192, dtype=np.float32) for key in ("FRX", "FRY", "FRZ")}
+        _lib.check(_lib.lib().cs3d_get_random_force(self.h, inst, _fp(a["FRX"]), _fp(a["FRY"]), _fp(a["FRZ"])),
+                   "cs3d_get_random_force")
+        return a
+
     def cells(self, inst=0):
         n = self.n_cells(inst)
         cm = np.zeros(3 * n, dtype=np.float32)

@@ -27,7 +27,8 @@ class Params(C.Structure):
         "gamma_visc", "division_vol", "time_interval", "max_pressure", "min_pressure",
         "growth_rate", "thresh_dist")] + [("box_len", C.c_float * 3)] + [(n, C.c_int32) for n in (
         "check_sphericity", "constrain_angles", "use_rigid_box", "daught_same_stiffness",
-        "div_time_steps", "rng_ij", "rng_kl")]
+        "div_time_steps", "rng_ij", "rng_kl", "add_rands")] + [("rand_scale_factor", C.c_float),
+                                                             ("rand_seed", C.c_int32)]
 
 
 class Topology(C.Structure):
@@ -77,7 +78,7 @@ EXPORTS = [
     "cs3d_topology_build", "cs3d_rng_init", "cs3d_rng_draw", "cs3d_rng_random_vector", "cs3d_seed_map",
     "cs3d_init_positions", "cs3d_traj_open", "cs3d_traj_write_frame", "cs3d_traj_close", "cs3d_create",
     "cs3d_create_ensemble", "cs3d_load_state", "cs3d_set_rng", "cs3d_get_rng", "cs3d_step", "cs3d_get_state",
-    "cs3d_get_forces", "cs3d_get_cells", "cs3d_get_grid", "cs3d_set_option", "cs3d_get_pairs",
+    "cs3d_get_forces", "cs3d_get_random_force", "cs3d_get_cells", "cs3d_get_grid", "cs3d_set_option", "cs3d_get_pairs",
     "cs3d_get_events", "cs3d_last_error", "cs3d_get_stats", "cs3d_profile_step", "cs3d_last_step_ms",
     "cs3d_destroy", "cs3d_forces_static",
 ]
@@ -131,6 +132,7 @@ def lib():
     L.cs3d_step.argtypes = [P, C.c_int]
     L.cs3d_get_state.argtypes = [P, C.c_int, ip, fp, fp, fp, fp, fp, fp, fp, fp]
     L.cs3d_get_forces.argtypes = [P, C.c_int, fp, fp, fp, fp, fp, fp]
+    L.cs3d_get_random_force.argtypes = [P, C.c_int, fp, fp, fp]
     L.cs3d_get_cells.argtypes = [P, C.c_int, fp, fp, fp, fp]
     L.cs3d_get_grid.argtypes = [P, C.c_int, fp, ip]
     L.cs3d_set_option.argtypes = [P, C.c_int, C.c_longlong]

@@ -193,6 +193,10 @@ InstParams make_inst(const cs3d_params &p, int base, int cap, float skin)
     q.div_steps = p.div_time_steps;
     q.base = base;
     q.cap = cap;
+    q.rands = p.add_rands ? 1 : 0;
+    q.rscale = p.rand_scale_factor;
+    q.rdt = sqrtf(p.time_interval);
+    q.rseed = (unsigned)p.rand_seed;
     return q;
 }
 
@@ -424,7 +428,7 @@ int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topol
 #define AL(ptr, cnt) if (!rc) rc = dalloc(c, &(ptr), (cnt))
     AL(d.prm, n_inst);
     AL(d.st, n_inst);
-    AL(d.X, nodes); AL(d.V, nodes); AL(d.Vb, nodes); AL(d.FC, nodes); AL(d.FD, nodes);
+    AL(d.X, nodes); AL(d.V, nodes); AL(d.Vb, nodes); AL(d.FC, nodes); AL(d.FD, nodes); AL(d.FR, nodes);
     AL(d.CM, c->cap_total);
     AL(d.press, c->cap_total); AL(d.E, c->cap_total); AL(d.vol, c->cap_total); AL(d.area, c->cap_total);
     AL(d.divflag, c->cap_total);
@@ -748,6 +752,20 @@ int cs3d_get_forces(cs3d_ctx *c, int inst, float *FCX, float *FCY, float *FCZ, f
     return CS3D_OK;
 }
 
+int cs3d_get_random_force(cs3d_ctx *c, int inst, float *FRX, float *FRY, float *FRZ)
+{
+    if (!c || inst < 0 || inst >= c->n_inst) return CS3D_E_ARG;
+    cudaSetDevice(c->device);
+    int rc = ensure_init(c);
+    if (rc) return rc;
+    int n = 0;
+    if ((rc = inst_count(c, inst, &n))) return rc;
+    std::vector<float4> buf;
+    if ((rc = fetch4(c, c->d.FR, inst, n, buf))) return rc;
+    to_soa(buf, n, FRX, FRY, FRZ);
+    return CS3D_OK;
+}
+
 int cs3d_get_cells(cs3d_ctx *c, int inst, float *cm, float *volume, float *area, float *aabb)
 {
     if (!c || inst < 0 || inst >= c->n_inst) return CS3D_E_ARG;
@@ -906,6 +924,7 @@ struct StaticScratch {
     InstParams prm;
     InstState st;
     float4 X[SCAP * SLOTS], V[SCAP * SLOTS], Vb[SCAP * SLOTS], FC[SCAP * SLOTS], FD[SCAP * SLOTS], Xb[SCAP * SLOTS];
+    float4 FR[SCAP * SLOTS];
     float4 CM[SCAP];
     float press[SCAP], E[SCAP], vol[SCAP], area[SCAP];
     uint8_t divflag[SCAP];
@@ -965,7 +984,7 @@ Dev static_dev(StaticScratch *s)
     d.topo.faces = s->faces;
     d.topo.cs0 = s->cs0;
     d.topo.r0i = s->r0i;
-    d.X = s->X; d.V = s->V; d.Vb = s->Vb; d.FC = s->FC; d.FD = s->FD; d.Xb = s->Xb;
+    d.X = s->X; d.V = s->V; d.Vb = s->Vb; d.FC = s->FC; d.FD = s->FD; d.Xb = s->Xb; d.FR = s->FR;
     d.CM = s->CM;
     d.press = s->press; d.E = s->E; d.vol = s->vol; d.area = s->area;
     d.divflag = s->divflag;

@@ -28,6 +28,10 @@ struct InstParams {
     float skin;
     int check_sph, angles, rigid, daught_same, div_steps;
     int base, cap;
+    int rands;      // Langevin random force on
+    float rscale;   // rand_scale_factor
+    float rdt;      // sqrtf(dt), the random force's weight in the kicks
+    unsigned rseed; // Philox key
 };
 
 // Per-instance mutable state (device resident).
@@ -80,6 +84,7 @@ struct Dev {
     float4 *V;          // velocities (state)
     float4 *Vb;         // velocities after the half kicks (v3), read by neighbours
     float4 *FC, *FD;    // forces
+    float4 *FR;         // Langevin random force of the last step (zero when off)
     float4 *CM;         // centre of mass
     float *press, *E, *vol, *area;
     uint8_t *divflag;

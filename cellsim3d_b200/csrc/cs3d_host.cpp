@@ -405,9 +405,12 @@ int cs3d_config_to_params(const cs3d_config *c, cs3d_params *p)
     p->daught_same_stiffness = c->daught_same_stiffness;
     p->div_time_steps = c->div_time_steps;
     cs3d_seed_map(c->rand_seed, &p->rng_ij, &p->rng_kl);
+    p->add_rands = c->add_rands ? 1 : 0;
+    p->rand_scale_factor = c->rand_scale_factor;
+    p->rand_seed = c->rand_seed;   // <= 0: the caller picks one (the reference seeds from time())
     // Features of the reference this build leaves out (all off in the
     // reference's shipped inp.json and in every benchmark configuration).
-    if (c->add_rands || c->correct_com || c->use_different_stiffnesses || c->do_pop_model ||
+    if (c->correct_com || c->use_different_stiffnesses || c->do_pop_model ||
         c->use_div_plane_basis || c->use_walls || c->use_pbcs || c->do_adaptive_dt)
         return CS3D_E_UNSUPPORTED;
     return CS3D_OK;

@@ -80,6 +80,40 @@ __device__ __forceinline__ float kick(float v, float fsum, double m)
     return (float)((double)v + 0.5 * (double)fsum / m);
 }
 
+// Langevin random force (src/propagate.cu:668-678): rand_scale_factor times
+// three standard normals per node and step.  The reference draws them from
+// per-node curand XORWOW states; here they come from the counter-based
+// Philox4x32-10 generator (Salmon, Moraes, Dror and Shaw, "Parallel random
+// numbers: as easy as 1, 2, 3", SC'11; round multipliers and Weyl key
+// increments as published there) keyed by the instance's rand_seed and
+// counted by (node, step), with the Box-Muller transform on 24-bit uniforms.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k)
+{
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const unsigned hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        const unsigned hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += 0x9E3779B9u;
+        k.y += 0xBB67AE85u;
+    }
+    return c;
+}
+
+__device__ __forceinline__ float unit_open(unsigned r)
+{
+    return ((float)(r >> 8) + 0.5f) * (1.0f / 16777216.0f);  // (0, 1), exact in float
+}
+
+__device__ __forceinline__ float3 random_force(const InstParams &P, int a, int i, int step)
+{
+    const unsigned node = (unsigned)((a - P.base) * SLOTS + i);
+    const uint4 r = philox4x32_10(make_uint4(node, (unsigned)step, 0u, 0u), make_uint2(P.rseed, 0x2545F491u));
+    const float ra = sqrtf(-2.0f * logf(unit_open(r.x))), ta = 6.28318531f * unit_open(r.y);
+    const float rb = sqrtf(-2.0f * logf(unit_open(r.z))), tb = 6.28318531f * unit_open(r.w);
+    return make_float3(P.rscale * (ra * cosf(ta)), P.rscale * (ra * sinf(ta)), P.rscale * (rb * cosf(tb)));
+}
+
 // sqrt(x) and 1/x of positive doubles: float hardware seeds refined by one
 // Newton step in FP64 (relative error ~1e-14, far below what the forces need,
 // and much cheaper than the correctly rounded FP64 sequences).
@@ -388,9 +422,18 @@ __global__ void __launch_bounds__(SLOTS) k_integrate(Dev d)
             float4 x = d.X[g], v = d.V[g], fc = d.FC[g], fd = d.FD[g];
             const float dt = P.dt;
             const double m = P.mass;
-            v.x = kick(v.x, __fadd_rn(__fmul_rn(dt, fc.x), __fmul_rn(dt, fd.x)), m);
-            v.y = kick(v.y, __fadd_rn(__fmul_rn(dt, fc.y), __fmul_rn(dt, fd.y)), m);
-            v.z = kick(v.z, __fadd_rn(__fmul_rn(dt, fc.z), __fmul_rn(dt, fd.z)), m);
+            float sx = __fadd_rn(__fmul_rn(dt, fc.x), __fmul_rn(dt, fd.x));
+            float sy = __fadd_rn(__fmul_rn(dt, fc.y), __fmul_rn(dt, fd.y));
+            float sz = __fadd_rn(__fmul_rn(dt, fc.z), __fmul_rn(dt, fd.z));
+            if (P.rands) {  // + sqrt(dt) Fr of the previous step
+                const float4 fr = d.FR[g];
+                sx = __fadd_rn(sx, __fmul_rn(P.rdt, fr.x));
+                sy = __fadd_rn(sy, __fmul_rn(P.rdt, fr.y));
+                sz = __fadd_rn(sz, __fmul_rn(P.rdt, fr.z));
+            }
+            v.x = kick(v.x, sx, m);
+            v.y = kick(v.y, sy, m);
+            v.z = kick(v.z, sz, m);
             float4 xn = make_float4(__fmaf_rn(v.x, dt, x.x), __fmaf_rn(v.y, dt, x.y), __fmaf_rn(v.z, dt, x.z), 0.0f);
             // displacement since the last neighbour-list build
             const float4 xb = d.Xb[g];
@@ -746,13 +789,21 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
             d.ndis[g] = (uint8_t)(nd < MAXD ? nd : MAXD);
             if (INIT) {
                 d.FD[g] = make_float4(fd.x, fd.y, fd.z, 0.f);
+                d.FR[g] = make_float4(0.f, 0.f, 0.f, 0.f);  // no random force before the first step
             } else {
                 const double m = P.mass;
                 const float dt = P.dt;
-                // VelocityUpdateA reads the stored (float) conservative force
-                float vx = kick(v.x, __fmul_rn(dt, (float)FX), m);
-                float vy = kick(v.y, __fmul_rn(dt, (float)FY), m);
-                float vz = kick(v.z, __fmul_rn(dt, (float)FZ), m);
+                // random force of this step (CalculateRanForce, GPUbounce.cu:1133-1137)
+                float3 fr = make_float3(0.f, 0.f, 0.f);
+                if (P.rands) {
+                    fr = random_force(P, a, i, d.st[inst].step);
+                    d.FR[g] = make_float4(fr.x, fr.y, fr.z, 0.f);
+                }
+                // VelocityUpdateA reads the stored (float) conservative force:
+                // 0.5 (dt Fc + sqrt(dt) Fr) / m
+                float vx = kick(v.x, __fadd_rn(__fmul_rn(dt, (float)FX), __fmul_rn(P.rdt, fr.x)), m);
+                float vy = kick(v.y, __fadd_rn(__fmul_rn(dt, (float)FY), __fmul_rn(P.rdt, fr.y)), m);
+                float vz = kick(v.z, __fadd_rn(__fmul_rn(dt, (float)FZ), __fmul_rn(P.rdt, fr.z)), m);
                 const double hdt = 0.5 * (double)dt;
                 vx = (float)((double)vx + hdt * (double)fd.x / m);
                 vy = (float)((double)vy + hdt * (double)fd.y / m);
@@ -827,10 +878,19 @@ __global__ void __launch_bounds__(SLOTS, 5) k_s2(Dev d, int par)
                 const float4 fc = d.FC[g];
                 const float dt = P.dt;
                 const double m = P.mass;
+                float sx = __fadd_rn(__fmul_rn(dt, fc.x), __fmul_rn(dt, fd.x));
+                float sy = __fadd_rn(__fmul_rn(dt, fc.y), __fmul_rn(dt, fd.y));
+                float sz = __fadd_rn(__fmul_rn(dt, fc.z), __fmul_rn(dt, fd.z));
+                if (P.rands) {
+                    const float4 fr = d.FR[g];
+                    sx = __fadd_rn(sx, __fmul_rn(P.rdt, fr.x));
+                    sy = __fadd_rn(sy, __fmul_rn(P.rdt, fr.y));
+                    sz = __fadd_rn(sz, __fmul_rn(P.rdt, fr.z));
+                }
                 float4 vn = v4;
-                vn.x = kick(v4.x, __fadd_rn(__fmul_rn(dt, fc.x), __fmul_rn(dt, fd.x)), m);
-                vn.y = kick(v4.y, __fadd_rn(__fmul_rn(dt, fc.y), __fmul_rn(dt, fd.y)), m);
-                vn.z = kick(v4.z, __fadd_rn(__fmul_rn(dt, fc.z), __fmul_rn(dt, fd.z)), m);
+                vn.x = kick(v4.x, sx, m);
+                vn.y = kick(v4.y, sy, m);
+                vn.z = kick(v4.z, sz, m);
                 const float4 xn = make_float4(__fmaf_rn(vn.x, dt, x4.x), __fmaf_rn(vn.y, dt, x4.y),
                                               __fmaf_rn(vn.z, dt, x4.z), 0.0f);
                 const float4 xb = d.Xb[g];

@@ -79,6 +79,15 @@ typedef struct cs3d_params {
     int32_t daught_same_stiffness; /* stiffnessParams.daughtSameStiffness */
     int32_t div_time_steps;     /* core.div_time_steps */
     int32_t rng_ij, rng_kl;     /* RANMAR seeds (see cs3d_seed_map) */
+    /* Langevin random force (rand_params.add_rands, src/propagate.cu:668-678):
+     * per node and step rand_scale_factor times three standard normals, used
+     * in VelocityUpdateA and the next Integrate with weight sqrt(dt).  The
+     * reference draws them from curand XORWOW states; this build draws them
+     * from Philox4x32-10 keyed by rand_seed and counted by (node, step), so
+     * only their distribution, not their values, matches the reference. */
+    int32_t add_rands;          /* rand_params.add_rands */
+    float rand_scale_factor;    /* rand_params.rand_scale_factor */
+    int32_t rand_seed;          /* rand_params.rand_seed */
 } cs3d_params;
 
 /* ---- static mesh data ------------------------------------------------- */
@@ -239,6 +248,11 @@ int cs3d_get_state(cs3d_ctx *ctx, int inst, int *n_cells, float *X, float *Y, fl
  * evaluation, 192-stride SoA. */
 int cs3d_get_forces(cs3d_ctx *ctx, int inst, float *FCX, float *FCY, float *FCZ,
                     float *FDX, float *FDY, float *FDZ);
+
+/* Langevin random force of the last step (zeros when add_rands is off or
+ * before the first step), 192-stride SoA.  No counterpart in the reference
+ * (its fRanList stays on the device). */
+int cs3d_get_random_force(cs3d_ctx *ctx, int inst, float *FRX, float *FRY, float *FRZ);
 
 /* Per-cell centre of mass (3*n), volume, area and bounding box (6*n:
  * minx maxx miny maxy minz maxz) as of the last step. */

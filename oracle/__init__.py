@@ -22,7 +22,8 @@ class OrcParams(C.Structure):
         "stiffness1", "gamma_int", "gamma_ext", "gamma_o", "div_vol", "dt", "max_p", "min_p",
         "growth_rate", "thresh_dist")] + [("box", C.c_float * 3)] + [(n, C.c_int) for n in (
         "check_sphericity", "constrain_angles", "use_rigid_box", "daught_same_stiffness",
-        "div_time_steps", "pad_")]
+        "div_time_steps", "pad_", "add_rands")] + [("rand_scale", C.c_float), ("rand_seed", C.c_uint),
+                                                   ("pad2_", C.c_int)]
 
 
 class OrcTopo(C.Structure):
@@ -158,7 +159,18 @@ def make_params(p):
     o.use_rigid_box = int(p["use_rigid_box"])
     o.daught_same_stiffness = int(p["daught_same_stiffness"])
     o.div_time_steps = int(p["div_time_steps"])
+    o.add_rands = int(p.get("add_rands", 0))
+    o.rand_scale = float(p.get("rand_scale_factor", 0.0))
+    o.rand_seed = int(p.get("rand_seed", 0)) & 0xffffffff
     return o
+
+
+def random_force(params, node, step):
+    """The oracle's Langevin random force of one node and step (3 floats)."""
+    P = make_params(params) if isinstance(params, dict) else params
+    out = np.zeros(3, dtype=np.float32)
+    lib().orc_random_force(C.byref(P), int(node), int(step), _fp(out))
+    return out
 
 
 def make_topo(nn, sign, r0, theta0, faces):
@@ -194,6 +206,7 @@ class System:
         self.vol, self.area = fv(9, capacity), fv(10, capacity)
         self.aabb = fv(11, 6 * capacity).reshape(capacity, 6)
         self.minmax = fv(12, 6)
+        self.FR = fv(13, 3 * nn).reshape(3, nn)
         self.FC = np.ctypeslib.as_array(L.orc_ptr_d(self.h, 0), shape=(3, nn))
         self.FD = np.ctypeslib.as_array(L.orc_ptr_d(self.h, 1), shape=(3, nn))
         self._n = np.ctypeslib.as_array(L.orc_ptr_i(self.h, 0), shape=(1,))

@@ -64,6 +64,10 @@ typedef struct {
     int daught_same_stiffness;
     int div_time_steps;       /* core.div_time_steps */
     int pad_;
+    int add_rands;            /* rand_params.add_rands */
+    float rand_scale;         /* rand_params.rand_scale_factor */
+    unsigned rand_seed;       /* Philox key (see orc_random_force) */
+    int pad2_;
 } orc_params;
 
 typedef struct {
@@ -87,6 +91,7 @@ typedef struct orc_sys {
     orc_topo T;
     float *X, *Y, *Z, *VX, *VY, *VZ;
     double *FC, *FD;           /* [3][cap*192] */
+    float *FR;                 /* [3][cap*192] random force of the last step */
     float *CM;                 /* [3][cap] */
     float *press, *E, *vol, *area;
     unsigned char *div_flag;
@@ -227,6 +232,7 @@ orc_sys *orc_create(int cap, const orc_params *P, const orc_topo *T)
     s->X = calloc(nn, 4); s->Y = calloc(nn, 4); s->Z = calloc(nn, 4);
     s->VX = calloc(nn, 4); s->VY = calloc(nn, 4); s->VZ = calloc(nn, 4);
     s->FC = calloc(3 * nn, 8); s->FD = calloc(3 * nn, 8);
+    s->FR = calloc(3 * nn, 4);
     s->CM = calloc(3 * (size_t)cap, 4);
     s->press = calloc(cap, 4); s->E = calloc(cap, 4);
     s->vol = calloc(cap, 4); s->area = calloc(cap, 4);
@@ -240,7 +246,7 @@ void orc_destroy(orc_sys *s)
 {
     if (!s) return;
     free(s->X); free(s->Y); free(s->Z); free(s->VX); free(s->VY); free(s->VZ);
-    free(s->FC); free(s->FD); free(s->CM); free(s->press); free(s->E);
+    free(s->FC); free(s->FD); free(s->FR); free(s->CM); free(s->press); free(s->E);
     free(s->vol); free(s->area); free(s->div_flag); free(s->aabb);
     free(s->bin_start); free(s->bin_cells); free(s->ev);
     free(s->rec[0]); free(s->rec[1]);
@@ -255,7 +261,7 @@ float *orc_ptr_f(orc_sys *s, int which)
     case 3: return s->VX; case 4: return s->VY; case 5: return s->VZ;
     case 6: return s->CM; case 7: return s->press; case 8: return s->E;
     case 9: return s->vol; case 10: return s->area; case 11: return s->aabb;
-    case 12: return s->minmax;
+    case 12: return s->minmax; case 13: return s->FR;
     default: return NULL;
     }
 }
@@ -855,8 +861,41 @@ void orc_init(orc_sys *s)
     orc_dis_force(s);
 }
 
+/* ------------------------------------------------------------------------ */
+/* Langevin random force, src/propagate.cu:668-678: rand_scale_factor times  */
+/* three standard normals per node and step.  The reference draws them from  */
+/* curand XORWOW states; the CUDA path (and this restatement of it) from     */
+/* Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) keyed by rand_seed and  */
+/* counted by (node, step), Box-Muller on 24-bit uniforms.                   */
+/* ------------------------------------------------------------------------ */
+static void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1)
+{
+    for (int r = 0; r < 10; ++r) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c[0], p1 = (uint64_t)0xCD9E8D57u * c[2];
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+        c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+}
+
+static float unit_open(uint32_t r) { return ((float)(r >> 8) + 0.5f) * (1.0f / 16777216.0f); }
+
+void orc_random_force(const orc_params *P, int node, int step, float out[3])
+{
+    uint32_t c[4] = {(uint32_t)node, (uint32_t)step, 0u, 0u};
+    philox4x32_10(c, P->rand_seed, 0x2545F491u);
+    float ra = sqrtf(-2.0f * logf(unit_open(c[0]))), ta = 6.28318531f * unit_open(c[1]);
+    float rb = sqrtf(-2.0f * logf(unit_open(c[2]))), tb = 6.28318531f * unit_open(c[3]);
+    out[0] = P->rand_scale * (ra * cosf(ta));
+    out[1] = P->rand_scale * (ra * sinf(ta));
+    out[2] = P->rand_scale * (rb * cosf(tb));
+}
+
 /* One timestep, src/GPUbounce.cu:1055-1338 (population model, variable
- * stiffness, random forces and CoM correction disabled).                    */
+ * stiffness and CoM correction disabled).                                    */
 void orc_step(orc_sys *s)
 {
     const orc_params *P = &s->P;
@@ -870,6 +909,7 @@ void orc_step(orc_sys *s)
      * one float multiply-add.  Transcribed exactly, so that from the same float
      * state the oracle's positions after the drift are the reference's. */
     const float dtf = P->dt;
+    const float rdt = sqrtf(dtf);
     #pragma omp parallel for schedule(static)
     for (int c = 0; c < N; ++c)
         for (int i = 0; i < 180; ++i) {
@@ -879,6 +919,7 @@ void orc_step(orc_sys *s)
             for (int q = 0; q < 3; ++q) {
                 float fc = (float)s->FC[q * cap192 + g], fd = (float)s->FD[q * cap192 + g];
                 float sum = dtf * fc + dtf * fd;
+                if (P->add_rands) sum = sum + rdt * s->FR[q * cap192 + g];
                 V[q][g] = (float)((double)V[q][g] + 0.5 * (double)sum / m);
                 X[q][g] = fmaf(V[q][g], dtf, X[q][g]);
             }
@@ -889,6 +930,16 @@ void orc_step(orc_sys *s)
     record_pairs(s);
     orc_con_force(s);
     orc_dis_force(s);
+    /* CalculateRanForce, src/GPUbounce.cu:1133-1137 */
+    if (P->add_rands) {
+        #pragma omp parallel for schedule(static)
+        for (int c = 0; c < N; ++c)
+            for (int i = 0; i < 180; ++i) {
+                float fr[3];
+                orc_random_force(P, c * 192 + i, step, fr);
+                for (int q = 0; q < 3; ++q) s->FR[q * cap192 + c * 192 + i] = fr[q];
+            }
+    }
     /* VelocityUpdateA/B, src/propagate.cu:714-736 (float forces, double scale) */
     #pragma omp parallel for schedule(static)
     for (int c = 0; c < N; ++c)
@@ -897,7 +948,9 @@ void orc_step(orc_sys *s)
             float *V[3] = {s->VX, s->VY, s->VZ};
             for (int q = 0; q < 3; ++q) {
                 float fc = (float)s->FC[q * cap192 + g], fd = (float)s->FD[q * cap192 + g];
-                V[q][g] = (float)((double)V[q][g] + 0.5 * (double)(dtf * fc) / m);
+                float sa = dtf * fc;
+                if (P->add_rands) sa = sa + rdt * s->FR[q * cap192 + g];
+                V[q][g] = (float)((double)V[q][g] + 0.5 * (double)sa / m);
                 V[q][g] = (float)((double)V[q][g] + 0.5 * (double)dtf * (double)fd / m);
             }
         }

@@ -87,6 +87,7 @@ def sorted_pairs(a):
 def snapshot(sim):
     st = sim.state()
     st.update(sim.forces())
+    st.update(sim.random_force())
     st["cm"] = sim.cells()["cm"]
     st["rng"] = sim.get_rng()
     st["step"] = sim.stats()["steps"]
@@ -100,6 +101,8 @@ def oracle_from(snap, p, otopo, capacity, record=True):
     O.load(snap["X"], snap["Y"], snap["Z"], snap["VX"], snap["VY"], snap["VZ"],
            pressure=snap["pressure"], youngs=snap["youngs"], n=n)
     O.load_forces(snap["FCX"], snap["FCY"], snap["FCZ"], snap["FDX"], snap["FDY"], snap["FDZ"])
+    k = n * 192
+    O.FR[0][:k], O.FR[1][:k], O.FR[2][:k] = snap["FRX"][:k], snap["FRY"][:k], snap["FRZ"][:k]
     O.load_cm(snap["cm"])
     O.set_rng_from(snap["rng"].state)
     O.set_step(snap["step"])

@@ -127,6 +127,7 @@ def test_ensemble_instances_single_step(mesh):
     for k in range(3):
         s = ens.state(k)
         s.update(ens.forces(k))
+        s.update(ens.random_force(k))
         s["cm"] = ens.cells(k)["cm"]
         s["rng"] = ens.get_rng(k)
         s["step"] = 30
