@@ -28,7 +28,7 @@ class Params(C.Structure):
         "growth_rate", "thresh_dist")] + [("box_len", C.c_float * 3)] + [(n, C.c_int32) for n in (
         "check_sphericity", "constrain_angles", "use_rigid_box", "daught_same_stiffness",
         "div_time_steps", "rng_ij", "rng_kl", "add_rands")] + [("rand_scale_factor", C.c_float),
-                                                             ("rand_seed", C.c_int32)]
+                                                             ("rand_seed", C.c_int32), ("correct_com", C.c_int32)]
 
 
 class Topology(C.Structure):

@@ -30,6 +30,7 @@ struct cs3d_ctx {
     long long host_step = 0;
     int max_div_steps = 0;
     bool any_growth = false;
+    bool any_com = false;          // some instance corrects its centre-of-mass motion
     float skin = 0.1f;
     int grid_cells = 0;            // blocks of the per-cell kernels
     int grid_flat = 0;             // blocks of the per-thread kernels
@@ -197,6 +198,7 @@ InstParams make_inst(const cs3d_params &p, int base, int cap, float skin)
     q.rscale = p.rand_scale_factor;
     q.rdt = sqrtf(p.time_interval);
     q.rseed = (unsigned)p.rand_seed;
+    q.correct_com = p.correct_com ? 1 : 0;
     return q;
 }
 
@@ -277,6 +279,9 @@ int run_init(cs3d_ctx *c)
     k_build_work<<<1, 256, 0, s>>>(d);
     k_init_begin<<<1, 256, 0, s>>>(d);
     k_geom<<<c->grid_cells, SLOTS, 0, s>>>(d, 0);
+    // correct_com at set-up (src/GPUbounce.cu:785-805): after the first grid,
+    // before the first force evaluation
+    if (c->any_com) k_com_shift<<<c->n_inst, 256, 0, s>>>(d);
     CK(cudaGetLastError());
     int rc = launch_nl_build(c);
     if (rc) return rc;
@@ -311,6 +316,7 @@ int launch_step(cs3d_ctx *c, int par, bool div, bool k1 = true, bool fuse = fals
         k_div_apply<<<c->grid_cells, SLOTS, 0, s>>>(d, par); ++n; pf.mark(s, "div_apply");
         k_grid_fix<<<c->grid_flat, 256, 0, s>>>(d, par); ++n; pf.mark(s, "grid_fix");
     }
+    if (c->any_com) { k_com_shift<<<c->n_inst, 256, 0, s>>>(d); ++n; pf.mark(s, "com_shift"); }
     CK(cudaGetLastError());
     c->launches_per_step = n;
     return CS3D_OK;
@@ -417,6 +423,7 @@ int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topol
         c->hprm.push_back(make_inst(params[k], base, capacity[k], c->skin));
         base += capacity[k];
         if (params[k].growth_rate > 0) c->any_growth = true;
+        if (params[k].correct_com) c->any_com = true;
         c->max_div_steps = std::max(c->max_div_steps, params[k].div_time_steps);
     }
     Dev &d = c->d;
@@ -633,7 +640,7 @@ int cs3d_step(cs3d_ctx *c, int n_steps)
         long long s = c->host_step + 1;
         int par = (int)((s - 1) & 1);
         bool div = c->any_growth && s <= c->max_div_steps;
-        bool fuse = !div && k + 1 < n_steps;
+        bool fuse = !div && !c->any_com && k + 1 < n_steps;
         cudaGraphExec_t g;
         if ((rc = get_graph(c, par, div, k1, fuse, &g))) return rc;
         CK(cudaGraphLaunch(g, c->stream));

@@ -32,6 +32,7 @@ struct InstParams {
     float rscale;   // rand_scale_factor
     float rdt;      // sqrtf(dt), the random force's weight in the kicks
     unsigned rseed; // Philox key
+    int correct_com;
 };
 
 // Per-instance mutable state (device resident).

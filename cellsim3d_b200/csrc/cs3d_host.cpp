@@ -408,9 +408,10 @@ int cs3d_config_to_params(const cs3d_config *c, cs3d_params *p)
     p->add_rands = c->add_rands ? 1 : 0;
     p->rand_scale_factor = c->rand_scale_factor;
     p->rand_seed = c->rand_seed;   // <= 0: the caller picks one (the reference seeds from time())
+    p->correct_com = c->correct_com ? 1 : 0;
     // Features of the reference this build leaves out (all off in the
     // reference's shipped inp.json and in every benchmark configuration).
-    if (c->correct_com || c->use_different_stiffnesses || c->do_pop_model ||
+    if (c->use_different_stiffnesses || c->do_pop_model ||
         c->use_div_plane_basis || c->use_walls || c->use_pbcs || c->do_adaptive_dt)
         return CS3D_E_UNSUPPORTED;
     return CS3D_OK;

@@ -1164,6 +1164,46 @@ __global__ void __launch_bounds__(SLOTS) k_div_apply(Dev d, int par)
     }
 }
 
+// CoM correction at the end of a step (correct_com, src/GPUbounce.cu:1430-1440
+// with calc_sys_CM :2504-2520 and CorrectCoMMotion, src/propagate.cu:766-776):
+// the mean of the cells' centres of mass (a float sum in cell order, as the
+// host loop does; a daughter's entry is still 0 in its first step) is
+// subtracted from every node.  The centres of mass, boxes and grid of this
+// step keep their unshifted values, as in the reference; the list anchors
+// move with the nodes (a uniform shift changes no distance).  One block per
+// instance.
+__global__ void __launch_bounds__(256) k_com_shift(Dev d)
+{
+    const int k = blockIdx.x;
+    if (k >= d.n_inst) return;
+    const InstParams &P = d.prm[k];
+    if (!P.correct_com) return;
+    __shared__ float sys[3];
+    const int n = d.st[k].n;
+    if (threadIdx.x == 0) {
+        float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+        for (int c = 0; c < n; ++c) {
+            const float4 cm = d.CM[P.base + c];
+            sx = __fadd_rn(sx, cm.x);
+            sy = __fadd_rn(sy, cm.y);
+            sz = __fadd_rn(sz, cm.z);
+        }
+        sys[0] = __fdiv_rn(sx, (float)n);
+        sys[1] = __fdiv_rn(sy, (float)n);
+        sys[2] = __fdiv_rn(sz, (float)n);
+    }
+    __syncthreads();
+    const float ox = sys[0], oy = sys[1], oz = sys[2];
+    for (int q = threadIdx.x; q < n * SLOTS; q += blockDim.x) {
+        const size_t g = (size_t)P.base * SLOTS + q;
+        float4 x = d.X[g], b = d.Xb[g];
+        x.x = __fsub_rn(x.x, ox); x.y = __fsub_rn(x.y, oy); x.z = __fsub_rn(x.z, oz);
+        b.x = __fsub_rn(b.x, ox); b.y = __fsub_rn(b.y, oy); b.z = __fsub_rn(b.z, oz);
+        d.X[g] = x;
+        d.Xb[g] = b;
+    }
+}
+
 // G: grid extents of instances that divided this step, from all boxes.
 __global__ void k_grid_fix(Dev d, int par)
 {

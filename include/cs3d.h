@@ -88,6 +88,8 @@ typedef struct cs3d_params {
     int32_t add_rands;          /* rand_params.add_rands */
     float rand_scale_factor;    /* rand_params.rand_scale_factor */
     int32_t rand_seed;          /* rand_params.rand_seed */
+    int32_t correct_com;        /* core.correct_com: shift all nodes by minus the mean of the
+                                   cells' centres of mass after every step, src/GPUbounce.cu:1430-1440 */
 } cs3d_params;
 
 /* ---- static mesh data ------------------------------------------------- */

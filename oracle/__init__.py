@@ -23,7 +23,7 @@ class OrcParams(C.Structure):
         "growth_rate", "thresh_dist")] + [("box", C.c_float * 3)] + [(n, C.c_int) for n in (
         "check_sphericity", "constrain_angles", "use_rigid_box", "daught_same_stiffness",
         "div_time_steps", "pad_", "add_rands")] + [("rand_scale", C.c_float), ("rand_seed", C.c_uint),
-                                                   ("pad2_", C.c_int)]
+                                                   ("correct_com", C.c_int)]
 
 
 class OrcTopo(C.Structure):
@@ -61,7 +61,7 @@ def lib():
         L.orc_rng.restype = C.POINTER(OrcRanmar)
         L.orc_rng.argtypes = [P]
         for fn in ("orc_init", "orc_center_of_mass", "orc_build_grid", "orc_con_force",
-                   "orc_dis_force", "orc_volumes", "orc_step"):
+                   "orc_dis_force", "orc_volumes", "orc_step", "orc_rebuild_bins"):
             getattr(L, fn).argtypes = [P]
         L.orc_run.argtypes = [P, C.c_int]
         L.orc_pairs.restype = C.c_long
@@ -77,6 +77,7 @@ def lib():
         L.orc_ranmar_draw.argtypes = [C.POINTER(OrcRanmar), C.POINTER(C.c_float), C.c_int]
         L.orc_random_vector.argtypes = [C.POINTER(OrcRanmar), C.POINTER(C.c_float)]
         L.orc_seed_map.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.orc_random_force.argtypes = [C.POINTER(OrcParams), C.c_int, C.c_int, C.POINTER(C.c_float)]
         L.orc_r0_theta0.argtypes = [C.POINTER(C.c_float)] * 3 + [C.POINTER(C.c_int),
                                                                  C.POINTER(C.c_float), C.POINTER(C.c_float)]
         L.orc_divide_cell.restype = C.c_int
@@ -162,6 +163,7 @@ def make_params(p):
     o.add_rands = int(p.get("add_rands", 0))
     o.rand_scale = float(p.get("rand_scale_factor", 0.0))
     o.rand_seed = int(p.get("rand_seed", 0)) & 0xffffffff
+    o.correct_com = int(p.get("correct_com", 0))
     return o
 
 
@@ -316,6 +318,13 @@ class System:
 
     def compute_grid(self):
         lib().orc_build_grid(self.h)
+
+    def load_grid(self, aabb, minmax):
+        """Boxes (n, 6) and grid extents (6) of a handed-over state; bins rebuilt."""
+        n = self.n
+        self.aabb[:n] = np.asarray(aabb, dtype=np.float32).reshape(n, 6)
+        self.minmax[:] = np.asarray(minmax, dtype=np.float32).reshape(6)
+        lib().orc_rebuild_bins(self.h)
 
     def compute_cm(self):
         lib().orc_center_of_mass(self.h)

@@ -67,7 +67,7 @@ typedef struct {
     int add_rands;            /* rand_params.add_rands */
     float rand_scale;         /* rand_params.rand_scale_factor */
     unsigned rand_seed;       /* Philox key (see orc_random_force) */
-    int pad2_;
+    int correct_com;          /* core.correct_com */
 } orc_params;
 
 typedef struct {
@@ -355,6 +355,18 @@ void orc_build_grid(orc_sys *s)
         }
     }
     for (int d = 0; d < 3; ++d) { s->minmax[2 * d] = mn[d]; s->minmax[2 * d + 1] = mx[d]; }
+    s->xdiv = (int)((s->minmax[1] - s->minmax[0]) / ORC_DL + 1);
+    s->ydiv = (int)((s->minmax[3] - s->minmax[2]) / ORC_DL + 1);
+    s->zdiv = (int)((s->minmax[5] - s->minmax[4]) / ORC_DL + 1);
+    build_bins(s);
+}
+
+static void build_bins(orc_sys *s);
+
+/* Grid divisions and bins from boxes and extents already in place (a state
+ * handed over from the CUDA path, whose stale grid is part of the state). */
+void orc_rebuild_bins(orc_sys *s)
+{
     s->xdiv = (int)((s->minmax[1] - s->minmax[0]) / ORC_DL + 1);
     s->ydiv = (int)((s->minmax[3] - s->minmax[2]) / ORC_DL + 1);
     s->zdiv = (int)((s->minmax[5] - s->minmax[4]) / ORC_DL + 1);
@@ -851,11 +863,34 @@ long orc_recorded_pairs(orc_sys *s, int kind, int *out, long maxout)
 /* Initialisation up to the first force evaluation, src/GPUbounce.cu:739-763 */
 /* and :978-1004 (pressures set to minPressure at :867-871 by the caller).   */
 /* ------------------------------------------------------------------------ */
+/* CoM correction, src/GPUbounce.cu:1430-1440 (calc_sys_CM :2504-2520 sums
+ * the float centres of mass in cell order on the host; CorrectCoMMotion,
+ * src/propagate.cu:766-776, shifts the positions only).                     */
+static void correct_com(orc_sys *s)
+{
+    float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+    const int n = s->n, cap = s->cap;
+    for (int c = 0; c < n; ++c) {
+        sx += s->CM[c];
+        sy += s->CM[cap + c];
+        sz += s->CM[2 * cap + c];
+    }
+    sx = sx / (float)n;
+    sy = sy / (float)n;
+    sz = sz / (float)n;
+    for (int g = 0; g < n * 192; ++g) {
+        s->X[g] -= sx;
+        s->Y[g] -= sy;
+        s->Z[g] -= sz;
+    }
+}
+
 void orc_init(orc_sys *s)
 {
     s->err = 0;
     orc_center_of_mass(s);
     orc_build_grid(s);
+    if (s->P.correct_com) correct_com(s);   /* src/GPUbounce.cu:785-805 */
     record_pairs(s);
     orc_con_force(s);
     orc_dis_force(s);
@@ -967,6 +1002,7 @@ void orc_step(orc_sys *s)
         }
     }
     orc_build_grid(s);
+    if (P->correct_com) correct_com(s);
 }
 
 void orc_run(orc_sys *s, int nsteps)

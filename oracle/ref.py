@@ -7,7 +7,8 @@ restatement against the reference's own arithmetic, and the benchmark uses it
 to time the reference on the same GPU.  Nothing in the product imports it.
 
 File formats (little-endian):
-  input   "CS3DREF1", cs3d_params, cs3d_topology (include/cs3d.h),
+  input   "CS3DREF2", int32 sizeof(cs3d_params), sizeof(cs3d_topology),
+          cs3d_params, cs3d_topology (include/cs3d.h),
           int32 n, capacity, steps, flags (bit 0: dump the initial forces),
           warmup (steps before the timed region),
           float32 X, Y, Z, VX, VY, VZ [n*192], pressure [n], youngs [n]
@@ -22,10 +23,13 @@ import struct
 import subprocess
 import tempfile
 
+import ctypes as C
+
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 BIN = os.path.join(HERE, "_ref", "cs3d_ref")
+_DEPS = [os.path.join(HERE, "ref_harness.cu"), os.path.join(HERE, "..", "include", "cs3d.h")]
 
 STATUS = {0: "ok", 1: "a grid bin held more than 32 cells (clamped)",
           2: "more than 10 cells passed the box filter for a node (bin cut)",
@@ -33,7 +37,12 @@ STATUS = {0: "ok", 1: "a grid bin held more than 32 cells (clamped)",
 
 
 def available():
-    return os.path.exists(BIN)
+    """The harness is built and not older than its sources (a stale build
+    would read a different parameter layout; it rejects such input)."""
+    if not os.path.exists(BIN):
+        return False
+    t = os.path.getmtime(BIN)
+    return all(not os.path.exists(dep) or os.path.getmtime(dep) <= t for dep in _DEPS)
 
 
 def build(ref_root="/root/reference"):
@@ -68,7 +77,8 @@ def run(params, topo, state, capacity, steps, dump_init=False, warmup=0, timeout
     with tempfile.TemporaryDirectory(dir=workdir) as tmp:
         fin, fout = os.path.join(tmp, "in.bin"), os.path.join(tmp, "out.bin")
         with open(fin, "wb") as f:
-            f.write(b"CS3DREF1")
+            f.write(b"CS3DREF2")
+            f.write(struct.pack("<2i", C.sizeof(params), C.sizeof(topo)))
             f.write(bytes(params))
             f.write(bytes(topo))
             f.write(struct.pack("<5i", n, int(capacity), int(steps), 1 if dump_init else 0, int(warmup)))

@@ -124,29 +124,90 @@ struct Input {
     std::vector<float> X, Y, Z, VX, VY, VZ, press, youngs;
 };
 
+// The input file must match this build's layout exactly (sizes written by
+// the caller and checked here), and every value the reference kernels index
+// with or trap on is validated on the host before any launch: neighbour and
+// face indices in range, symmetric neighbour table, positive finite lengths
+// and angles, finite state, sane sizes.  A mismatched or corrupt file is
+// rejected instead of reaching the GPU.
+static bool fail_input(const char *why)
+{
+    fprintf(stderr, "cs3d_ref: input rejected: %s\n", why);
+    return false;
+}
+
+static bool finite_all(const std::vector<float> &v)
+{
+    for (float x : v)
+        if (!std::isfinite(x)) return false;
+    return true;
+}
+
 static bool read_input(const char *path, Input &in)
 {
     FILE *f = fopen(path, "rb");
-    if (!f) return false;
+    if (!f) return fail_input("cannot open");
+    fseek(f, 0, SEEK_END);
+    const long fsize = ftell(f);
+    fseek(f, 0, SEEK_SET);
     char magic[8];
-    bool ok = fread(magic, 1, 8, f) == 8 && memcmp(magic, "CS3DREF1", 8) == 0;
-    ok = ok && fread(&in.p, sizeof in.p, 1, f) == 1 && fread(&in.t, sizeof in.t, 1, f) == 1;
+    int sizes[2] = {0, 0};
+    bool ok = fread(magic, 1, 8, f) == 8 && memcmp(magic, "CS3DREF2", 8) == 0;
+    if (!ok) { fclose(f); return fail_input("bad magic (stale writer or build)"); }
+    ok = fread(sizes, sizeof(int), 2, f) == 2 && sizes[0] == (int)sizeof(cs3d_params) &&
+         sizes[1] == (int)sizeof(cs3d_topology);
+    if (!ok) { fclose(f); return fail_input("parameter/topology layout differs from this build (rebuild oracle/_ref)"); }
+    ok = fread(&in.p, sizeof in.p, 1, f) == 1 && fread(&in.t, sizeof in.t, 1, f) == 1;
     int hdr[5];
     ok = ok && fread(hdr, sizeof(int), 5, f) == 5;
-    if (ok) {
-        in.n = hdr[0]; in.cap = hdr[1]; in.steps = hdr[2]; in.flags = hdr[3]; in.warmup = hdr[4];
-        ok = in.n >= 1 && in.cap >= in.n && in.steps >= 0 && in.warmup >= 0 && in.warmup <= in.steps;
+    if (!ok) { fclose(f); return fail_input("truncated header"); }
+    in.n = hdr[0]; in.cap = hdr[1]; in.steps = hdr[2]; in.flags = hdr[3]; in.warmup = hdr[4];
+    if (!(in.n >= 1 && in.cap >= in.n && in.cap <= (1 << 22) && in.steps >= 0 && in.steps <= 10000000 &&
+          in.warmup >= 0 && in.warmup <= in.steps)) {
+        fclose(f);
+        return fail_input("sizes out of range");
     }
-    if (ok) {
-        const size_t k = (size_t)in.n * 192;
-        std::vector<float> *arr[6] = {&in.X, &in.Y, &in.Z, &in.VX, &in.VY, &in.VZ};
-        for (auto *a : arr) { a->resize(k); ok = ok && fread(a->data(), sizeof(float), k, f) == k; }
-        in.press.resize(in.n); in.youngs.resize(in.n);
-        ok = ok && fread(in.press.data(), sizeof(float), in.n, f) == (size_t)in.n;
-        ok = ok && fread(in.youngs.data(), sizeof(float), in.n, f) == (size_t)in.n;
-    }
+    const size_t k = (size_t)in.n * 192;
+    const long expect = 8 + 8 + (long)sizeof(cs3d_params) + (long)sizeof(cs3d_topology) + 20 +
+                        (long)(6 * k + 2 * (size_t)in.n) * 4;
+    if (fsize != expect) { fclose(f); return fail_input("file length does not match its header"); }
+    std::vector<float> *arr[6] = {&in.X, &in.Y, &in.Z, &in.VX, &in.VY, &in.VZ};
+    for (auto *a : arr) { a->resize(k); ok = ok && fread(a->data(), sizeof(float), k, f) == k; }
+    in.press.resize(in.n); in.youngs.resize(in.n);
+    ok = ok && fread(in.press.data(), sizeof(float), in.n, f) == (size_t)in.n;
+    ok = ok && fread(in.youngs.data(), sizeof(float), in.n, f) == (size_t)in.n;
     fclose(f);
-    return ok;
+    if (!ok) return fail_input("truncated arrays");
+    for (auto *a : arr)
+        if (!finite_all(*a)) return fail_input("non-finite position or velocity");
+    if (!finite_all(in.press) || !finite_all(in.youngs)) return fail_input("non-finite pressure or stiffness");
+    const cs3d_params &p = in.p;
+    if (!(p.particle_mass > 0 && p.time_interval > 0 && p.time_interval < 1 && p.attraction_range > 0 &&
+          p.attraction_range < 10 && p.repulsion_range >= 0 && std::isfinite(p.youngs_mod) &&
+          std::isfinite(p.stiffness1) && std::isfinite(p.max_pressure) && std::isfinite(p.min_pressure) &&
+          std::isfinite(p.growth_rate) && std::isfinite(p.division_vol)))
+        return fail_input("parameters out of range");
+    if (p.add_rands || p.correct_com) return fail_input("random forces / CoM correction are not driven by this harness");
+    for (int q = 0; q < 3; ++q)
+        for (int i = 0; i < 180; ++i) {
+            const int nb = in.t.nn[q * 192 + i];
+            if (nb < 0 || nb >= 180) return fail_input("neighbour index out of range");
+            bool back = false;
+            for (int m = 0; m < 3; ++m) back = back || in.t.nn[m * 192 + nb] == i;
+            if (!back) return fail_input("neighbour table not symmetric");
+            const float r0 = in.t.r0[q * 192 + i];
+            if (!(r0 > 0 && r0 < 10)) return fail_input("bond length out of range");
+        }
+    for (int i = 0; i < 3 * 180; ++i)
+        if (!(in.t.theta0[i] > 0 && in.t.theta0[i] < 3.1416f)) return fail_input("angle out of range");
+    for (int i = 0; i < 180; ++i)
+        if (in.t.sign[i] != 1 && in.t.sign[i] != -1) return fail_input("bad orientation sign");
+    for (int fc = 0; fc < 92; ++fc)
+        for (int m = 0; m < (fc < 12 ? 5 : 6); ++m) {
+            const int v = in.t.faces[fc * 7 + m];
+            if (v < 0 || v >= 180) return fail_input("face index out of range");
+        }
+    return true;
 }
 
 template <typename T> static T *dev(size_t n)

@@ -88,7 +88,10 @@ def snapshot(sim):
     st = sim.state()
     st.update(sim.forces())
     st.update(sim.random_force())
-    st["cm"] = sim.cells()["cm"]
+    cells = sim.cells()
+    st["cm"] = cells["cm"]
+    st["aabb"] = cells["aabb"]
+    st["minmax"] = sim.grid()[0]
     st["rng"] = sim.get_rng()
     st["step"] = sim.stats()["steps"]
     return st
@@ -106,7 +109,10 @@ def oracle_from(snap, p, otopo, capacity, record=True):
     O.load_cm(snap["cm"])
     O.set_rng_from(snap["rng"].state)
     O.set_step(snap["step"])
-    O.compute_grid()
+    if "aabb" in snap:
+        O.load_grid(snap["aabb"], snap["minmax"])   # the stale grid is part of the state
+    else:
+        O.compute_grid()
     O.set_record(record)
     return O
 
@@ -148,12 +154,20 @@ def single_step_check(sim, tag="", tol=TOL, check_pairs=True):
     # dissipative force on identical inputs: the CUDA path's own v3 and x,
     # stale grid of the previous step (cells that divided this step excluded:
     # their positions changed after the force evaluation)
+    # (with correct_com the positions after the step were shifted after the
+    # force evaluation: the positions at the evaluation are rebuilt from the
+    # state before the step by the integrator's float arithmetic)
     O2 = oracle_from(before, p, otopo, cap, record=False)
-    O2.X[:k], O2.Y[:k], O2.Z[:k] = after["X"][:k], after["Y"][:k], after["Z"][:k]
+    if p.get("correct_com"):
+        xs = drift_positions(before, p)
+        O2.X[:k], O2.Y[:k], O2.Z[:k] = xs[0][:k], xs[1][:k], xs[2][:k]
+    else:
+        O2.X[:k], O2.Y[:k], O2.Z[:k] = after["X"][:k], after["Y"][:k], after["Z"][:k]
     O2.VX[:k], O2.VY[:k], O2.VZ[:k] = after["VX"][:k], after["VY"][:k], after["VZ"][:k]
     O2._n[0] = n
     O2.dis_force()
-    ed = rel_err([after["FDX"], after["FDY"], after["FDZ"]], [O2.FD[0], O2.FD[1], O2.FD[2]], n,
+    fd_ref = O2.FD
+    ed = rel_err([after["FDX"], after["FDY"], after["FDZ"]], [fd_ref[0], fd_ref[1], fd_ref[2]], n,
                  exclude_cells=sorted(divided))
     res.update(fc=ec, fd=ed, v=ev, cm_exact=bool(np.array_equal(after["cm"].view(np.uint32), cm_o.view(np.uint32))))
     print("%-26s n=%5d Fc max %.2e glob %.2e | Fd max %.2e glob %.2e | V max %.2e glob %.2e"
@@ -164,6 +178,25 @@ def single_step_check(sim, tag="", tol=TOL, check_pairs=True):
     O.close()
     O2.close()
     return res
+
+
+def drift_positions(snap, p):
+    """Positions after the first half kick and drift of a step from the state
+    `snap` (Integrate + ForwardTime: float sums, the kick scaled in double,
+    x + v dt rounded once)."""
+    f32, f64 = np.float32, np.float64
+    dt = f32(p["time_interval"])
+    m = f64(p["particle_mass"])
+    rdt = np.sqrt(dt, dtype=np.float32)
+    out = []
+    for a, fc, fd, fr, v in (("X", "FCX", "FDX", "FRX", "VX"), ("Y", "FCY", "FDY", "FRY", "VY"),
+                             ("Z", "FCZ", "FDZ", "FRZ", "VZ")):
+        s = (dt * snap[fc].astype(f32)).astype(f32) + (dt * snap[fd].astype(f32)).astype(f32)
+        if p.get("add_rands"):
+            s = s + (rdt * snap[fr].astype(f32)).astype(f32)
+        v1 = (snap[v].astype(f64) + 0.5 * s.astype(f64) / m).astype(f32)
+        out.append((snap[a].astype(f64) + v1.astype(f64) * f64(dt)).astype(f32))
+    return out
 
 
 def write_mesh_files(d, mesh):

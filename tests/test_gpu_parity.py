@@ -197,3 +197,25 @@ def test_multi_step_launch_equals_single_steps(mesh):
     assert sims[0].stats()["rebuilds"] == sims[1].stats()["rebuilds"]
     for sim in sims:
         sim.close()
+
+
+def test_correct_com_single_steps(mesh):
+    """correct_com: all nodes shifted by minus the mean centre of mass after
+    every step (and at set-up), the step's grid and centres of mass left
+    unshifted, as in the reference."""
+    c, vel, L = W.packed_fcc(64, phi=0.5, seed=13)
+    c = c + np.float32(3.0)   # off-centre, so the correction moves the nodes
+    p = W.base_params(box_len=(L + 6, L + 6, L + 6), growth_rate=0.0, min_pressure=200.0, max_pressure=200.0,
+                      div_time_steps=5000, correct_com=1)
+    st = W.state(c, velocities=vel)
+    sim, orc = make_pair(p, st, mesh, capacity=64)
+    _check_init("correct_com init", sim, orc)
+    for target in (1, 2, 5):
+        cur = sim.stats()["steps"]
+        if target - 1 > cur:
+            sim.step(target - 1 - cur)
+        single_step_check(sim, "correct_com step %d" % target)
+    s = sim.state()
+    assert abs(float(np.mean(s["X"].reshape(-1, 192)[:, :180]))) < 0.5
+    sim.close()
+    orc.close()
