@@ -229,12 +229,24 @@ class Ensemble:
         _lib.check(_lib.lib().cs3d_get_state(self.h, inst, C.byref(n), *([None] * 8)), "cs3d_get_state")
         return n.value
 
-    def state(self, inst=0):
+    def state(self, inst=0, out=None):
+        """Positions, velocities (192-stride SoA), pressures and stiffnesses.
+        out: optional dict of preallocated float32 arrays (e.g. pinned host
+        memory) with room for the current cells, filled in place."""
         n = self.n_cells(inst)
         k = n * 192
-        a = {key: np.zeros(k, dtype=np.float32) for key in ("X", "Y", "Z", "VX", "VY", "VZ")}
-        a["pressure"] = np.zeros(n, dtype=np.float32)
-        a["youngs"] = np.zeros(n, dtype=np.float32)
+        if out is not None:
+            a = dict(out)
+            for key in ("X", "Y", "Z", "VX", "VY", "VZ"):
+                if a[key].dtype != np.float32 or not a[key].flags.c_contiguous or a[key].size < k:
+                    raise ValueError("out[%s]: contiguous float32 with room for %d values needed" % (key, k))
+            for key in ("pressure", "youngs"):
+                if key not in a or a[key].size < n:
+                    a[key] = np.zeros(n, dtype=np.float32)
+        else:
+            a = {key: np.zeros(k, dtype=np.float32) for key in ("X", "Y", "Z", "VX", "VY", "VZ")}
+            a["pressure"] = np.zeros(n, dtype=np.float32)
+            a["youngs"] = np.zeros(n, dtype=np.float32)
         nn = C.c_int32()
         st = _lib.lib().cs3d_get_state(self.h, inst, C.byref(nn), _fp(a["X"]), _fp(a["Y"]), _fp(a["Z"]),
                                        _fp(a["VX"]), _fp(a["VY"]), _fp(a["VZ"]), _fp(a["pressure"]),

@@ -210,6 +210,26 @@ int check_params(const cs3d_params &p)
     return CS3D_OK;
 }
 
+// Staged SoA (6 arrays of k floats) -> float4 positions (and velocities);
+// padding nodes (180..191 of each cell) are left zero.
+__global__ void k_pack(const float *stage, float4 *X, float4 *V, size_t k)
+{
+    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < k; g += (size_t)gridDim.x * blockDim.x) {
+        if (g % SLOTS >= NODES) continue;
+        X[g] = make_float4(stage[g], stage[k + g], stage[2 * k + g], 0.f);
+        if (V) V[g] = make_float4(stage[3 * k + g], stage[4 * k + g], stage[5 * k + g], 0.f);
+    }
+}
+
+// float4 arrays a, b -> staged SoA components (a.xyz, b.xyz).
+__global__ void k_unpack(float *stage, const float4 *a, const float4 *b, size_t k)
+{
+    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < k; g += (size_t)gridDim.x * blockDim.x) {
+        if (a) { const float4 v = a[g]; stage[g] = v.x; stage[k + g] = v.y; stage[2 * k + g] = v.z; }
+        if (b) { const float4 v = b[g]; stage[3 * k + g] = v.x; stage[4 * k + g] = v.y; stage[5 * k + g] = v.z; }
+    }
+}
+
 // Rebuild the active-cell work table from the device cell counts.
 __global__ void k_build_work(Dev d)
 {
@@ -358,17 +378,6 @@ int read_errors(cs3d_ctx *c, unsigned *any)
     return CS3D_OK;
 }
 
-void to_soa(const std::vector<float4> &src, int n, float *X, float *Y, float *Z)
-{
-    for (int c = 0; c < n; ++c)
-        for (int i = 0; i < SLOTS; ++i) {
-            const float4 &v = src[(size_t)c * SLOTS + i];
-            if (X) X[(size_t)c * SLOTS + i] = v.x;
-            if (Y) Y[(size_t)c * SLOTS + i] = v.y;
-            if (Z) Z[(size_t)c * SLOTS + i] = v.z;
-        }
-}
-
 int inst_count(cs3d_ctx *c, int inst, int *n)
 {
     int v = 0;
@@ -378,12 +387,25 @@ int inst_count(cs3d_ctx *c, int inst, int *n)
     return CS3D_OK;
 }
 
-int fetch4(cs3d_ctx *c, const float4 *src, int inst, int n, std::vector<float4> &out)
+// Host <-> device transfers of 192-stride SoA node arrays go through a
+// device staging area (c->d.stage, 6 arrays of cap*192 floats): the host
+// copies move the caller's arrays as they are (at full PCIe speed when the
+// caller's memory is pinned) and kernels convert to and from the float4
+// layout.
+
+// Gather up to two float4 arrays of instance inst (n cells) into staged
+// SoA components (k = 0..5 -> a.x, a.y, a.z, b.x, b.y, b.z), then copy the
+// requested ones to the host.
+int fetch_soa(cs3d_ctx *c, int inst, int n, const float4 *a, const float4 *b, float *const out[6])
 {
-    out.resize((size_t)n * SLOTS);
     if (n == 0) return CS3D_OK;
-    CK(cudaMemcpyAsync(out.data(), src + (size_t)c->hprm[inst].base * SLOTS, sizeof(float4) * out.size(),
-                       cudaMemcpyDeviceToHost, c->stream));
+    const size_t k = (size_t)n * SLOTS;
+    const size_t off = (size_t)c->hprm[inst].base * SLOTS;
+    k_unpack<<<c->grid_flat, 256, 0, c->stream>>>(c->d.stage, a ? a + off : nullptr, b ? b + off : nullptr, k);
+    CK(cudaGetLastError());
+    for (int q = 0; q < 6; ++q)
+        if (out[q]) CK(cudaMemcpyAsync(out[q], c->d.stage + (size_t)q * k, sizeof(float) * k, cudaMemcpyDeviceToHost,
+                                       c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return CS3D_OK;
 }
@@ -436,6 +458,7 @@ int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topol
     AL(d.prm, n_inst);
     AL(d.st, n_inst);
     AL(d.X, nodes); AL(d.V, nodes); AL(d.Vb, nodes); AL(d.FC, nodes); AL(d.FD, nodes); AL(d.FR, nodes);
+    AL(d.stage, 6 * nodes);
     AL(d.CM, c->cap_total);
     AL(d.press, c->cap_total); AL(d.E, c->cap_total); AL(d.vol, c->cap_total); AL(d.area, c->cap_total);
     AL(d.divflag, c->cap_total);
@@ -565,22 +588,25 @@ int cs3d_load_state(cs3d_ctx *c, int inst, int n, const float *X, const float *Y
     if (n > P.cap) return CS3D_E_CAPACITY;
     cudaSetDevice(c->device);
     const size_t slots = (size_t)P.cap * SLOTS;
-    std::vector<float4> x(slots, make_float4(0, 0, 0, 0)), v(slots, make_float4(0, 0, 0, 0));
-    for (size_t g = 0; g < (size_t)n * SLOTS; ++g) {
-        int node = (int)(g % SLOTS);
-        if (node >= NODES) continue;
-        x[g] = make_float4(X[g], Y[g], Z[g], 0.f);
-        if (VX && VY && VZ) v[g] = make_float4(VX[g], VY[g], VZ[g], 0.f);
-    }
+    const size_t k = (size_t)n * SLOTS;
+    const size_t off0 = (size_t)P.base * SLOTS;
+    const Dev &d0 = c->d;
+    // the caller's SoA arrays into the staging area, packed on the device
+    const float *in[6] = {X, Y, Z, VX, VY, VZ};
+    const bool with_v = VX && VY && VZ;
+    for (int q = 0; q < (with_v ? 6 : 3); ++q)
+        if (k) CK(cudaMemcpyAsync(d0.stage + (size_t)q * k, in[q], sizeof(float) * k, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(d0.X + off0, 0, sizeof(float4) * slots, c->stream));
+    CK(cudaMemsetAsync(d0.V + off0, 0, sizeof(float4) * slots, c->stream));
+    if (k) k_pack<<<c->grid_flat, 256, 0, c->stream>>>(d0.stage, d0.X + off0, with_v ? d0.V + off0 : nullptr, k);
+    CK(cudaGetLastError());
     std::vector<float> p(P.cap, 0.f), e(P.cap, 0.f);
     for (int k = 0; k < n; ++k) {
         p[k] = pressure ? pressure[k] : P.minp;
         e[k] = youngs ? youngs[k] : P.stiff1;
     }
-    const size_t off = (size_t)P.base * SLOTS;
+    const size_t off = off0;
     const Dev &d = c->d;
-    CK(cudaMemcpyAsync(d.X + off, x.data(), sizeof(float4) * slots, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(d.V + off, v.data(), sizeof(float4) * slots, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemsetAsync(d.Vb + off, 0, sizeof(float4) * slots, c->stream));
     CK(cudaMemsetAsync(d.FC + off, 0, sizeof(float4) * slots, c->stream));
     CK(cudaMemsetAsync(d.FD + off, 0, sizeof(float4) * slots, c->stream));
@@ -723,14 +749,10 @@ int cs3d_get_state(cs3d_ctx *c, int inst, int *n_cells, float *X, float *Y, floa
     int n = 0;
     if ((rc = inst_count(c, inst, &n))) return rc;
     if (n_cells) *n_cells = n;
-    std::vector<float4> buf;
-    if (X || Y || Z) {
-        if ((rc = fetch4(c, c->d.X, inst, n, buf))) return rc;
-        to_soa(buf, n, X, Y, Z);
-    }
-    if (VX || VY || VZ) {
-        if ((rc = fetch4(c, c->d.V, inst, n, buf))) return rc;
-        to_soa(buf, n, VX, VY, VZ);
+    if (X || Y || Z || VX || VY || VZ) {
+        float *const out[6] = {X, Y, Z, VX, VY, VZ};
+        if ((rc = fetch_soa(c, inst, n, (X || Y || Z) ? c->d.X : nullptr, (VX || VY || VZ) ? c->d.V : nullptr, out)))
+            return rc;
     }
     const int base = c->hprm[inst].base;
     if (pressure && n) CK(cudaMemcpyAsync(pressure, c->d.press + base, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
@@ -747,16 +769,9 @@ int cs3d_get_forces(cs3d_ctx *c, int inst, float *FCX, float *FCY, float *FCZ, f
     if (rc) return rc;
     int n = 0;
     if ((rc = inst_count(c, inst, &n))) return rc;
-    std::vector<float4> buf;
-    if (FCX || FCY || FCZ) {
-        if ((rc = fetch4(c, c->d.FC, inst, n, buf))) return rc;
-        to_soa(buf, n, FCX, FCY, FCZ);
-    }
-    if (FDX || FDY || FDZ) {
-        if ((rc = fetch4(c, c->d.FD, inst, n, buf))) return rc;
-        to_soa(buf, n, FDX, FDY, FDZ);
-    }
-    return CS3D_OK;
+    float *const out[6] = {FCX, FCY, FCZ, FDX, FDY, FDZ};
+    return fetch_soa(c, inst, n, (FCX || FCY || FCZ) ? c->d.FC : nullptr, (FDX || FDY || FDZ) ? c->d.FD : nullptr,
+                     out);
 }
 
 int cs3d_get_random_force(cs3d_ctx *c, int inst, float *FRX, float *FRY, float *FRZ)
@@ -767,10 +782,8 @@ int cs3d_get_random_force(cs3d_ctx *c, int inst, float *FRX, float *FRY, float *
     if (rc) return rc;
     int n = 0;
     if ((rc = inst_count(c, inst, &n))) return rc;
-    std::vector<float4> buf;
-    if ((rc = fetch4(c, c->d.FR, inst, n, buf))) return rc;
-    to_soa(buf, n, FRX, FRY, FRZ);
-    return CS3D_OK;
+    float *const out[6] = {FRX, FRY, FRZ, nullptr, nullptr, nullptr};
+    return fetch_soa(c, inst, n, c->d.FR, nullptr, out);
 }
 
 int cs3d_get_cells(cs3d_ctx *c, int inst, float *cm, float *volume, float *area, float *aabb)

@@ -86,6 +86,7 @@ struct Dev {
     float4 *Vb;         // velocities after the half kicks (v3), read by neighbours
     float4 *FC, *FD;    // forces
     float4 *FR;         // Langevin random force of the last step (zero when off)
+    float *stage;       // [6 * cap_total*192] host transfer staging (SoA)
     float4 *CM;         // centre of mass
     float *press, *E, *vol, *area;
     uint8_t *divflag;
