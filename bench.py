@@ -1,7 +1,7 @@
 """Benchmark of the CellSim3D timestep on B200 (node-steps/s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cs3d|reference]
-                    [--workload packed100k|colony|ensemble256] [--cells C]
+                    [--workload packed100k|colony|ensemble256|small8] [--cells C]
 
 Default workload: the packed large system (100,000 non-dividing cells, FCC
 packing at volume fraction 0.5, pressure 200, Gaussian node velocities
@@ -119,6 +119,10 @@ def build_workload(name, cells, seed=123, steps=0, instances=0):
     if name == "colony":
         p, st, cap = W.config2()
         return [(p, st, cap)]
+    if name == "small8":
+        # 8 cells on a 2x2x2 lattice, pressure ramp, all divide at step 1
+        p, st, _ = W.config1()
+        return [(p, st, 4096)]
     if name == "ensemble256":
         # capacity per instance: 10k steps grow the largest instance to ~4500 cells
         cap = 1024 if steps <= 500 else 6000
@@ -157,6 +161,8 @@ def run_cs3d(args, world, rank, local):
         insts = [insts[k] for k in mine]
     topo = make_topology(insts)
     ens = cs.Ensemble([p for p, _, _ in insts], topo, [cap for _, _, cap in insts], device=local)
+    if args.skin is not None:
+        ens.set_option(cs.OPT_SKIN, int(round(args.skin * 1e6)))
     for k, (p, st, cap) in enumerate(insts):
         ens.load_state(k, st["X"], st["Y"], st["Z"], st.get("VX"), st.get("VY"), st.get("VZ"), n_cells=st["n"])
     n_nodes0 = sum(st["n"] for _, st, _ in insts) * 180
@@ -385,12 +391,14 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="cs3d", choices=["cs3d", "reference"])
-    ap.add_argument("--workload", default="packed100k", choices=["packed100k", "colony", "ensemble256"])
+    ap.add_argument("--workload", default="packed100k", choices=["packed100k", "colony", "ensemble256", "small8"])
     ap.add_argument("--cells", type=int, default=100_000)
     ap.add_argument("--cpu-cells", type=int, default=10_000)
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--skin", type=float, default=None,
+                    help="neighbour-list skin (default: the library's, 0.1)")
     ap.add_argument("--instances", type=int, default=0,
                     help="ensemble256: a stratified subset of this many instances (0: all 256)")
     ap.add_argument("--ref-sample", type=int, default=0,
