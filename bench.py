@@ -1,7 +1,7 @@
 """Benchmark of the CellSim3D timestep on B200 (node-steps/s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cs3d|reference]
-                    [--workload packed100k|colony|ensemble256|small8] [--cells C]
+                    [--workload packed100k|colony|ensemble256|het64|small8] [--cells C]
 
 Default workload: the packed large system (100,000 non-dividing cells, FCC
 packing at volume fraction 0.5, pressure 200, Gaussian node velocities
@@ -37,6 +37,8 @@ NODE_BYTES = 48  # algorithmic bytes per node-step: float32 x and v, read and wr
 # profiles/k_s1_packed30k.md (30k cells, 5.4M nodes: 334.8 MB + 194.0 MB), scaled
 # by the nodes of the launch
 S1_TRAFFIC_PER_NODE = 97.9
+ENSEMBLES = ("ensemble256", "het64")
+_WORKLOADS = {}
 
 
 def _peaks():
@@ -109,7 +111,30 @@ def dist_env():
     return world, rank, local
 
 
+def _subset(insts, k):
+    """A stratified subset by initial cell count: every (n / k)-th instance in size order."""
+    if not k or k >= len(insts):
+        return insts
+    order = sorted(range(len(insts)), key=lambda q: (insts[q][1]["n"], q))
+    pick = sorted({order[int(round(q * (len(insts) - 1) / max(k - 1, 1)))] for q in range(k)})
+    return [insts[q] for q in pick]
+
+
+def _config(gen):
+    """The instances of an ensemble generator, generated once per process."""
+    if gen.__name__ not in _WORKLOADS:
+        _WORKLOADS[gen.__name__] = gen()
+    return _WORKLOADS[gen.__name__]
+
+
 def build_workload(name, cells, seed=123, steps=0, instances=0):
+    key = (name, cells, seed, steps, instances)
+    if key not in _WORKLOADS:
+        _WORKLOADS[key] = _build_workload(name, cells, seed, steps, instances)
+    return _WORKLOADS[key]
+
+
+def _build_workload(name, cells, seed, steps, instances):
     from cellsim3d_b200 import workloads as W
     if name == "packed100k":
         c, vel, L = W.packed_fcc(cells, phi=0.5, seed=seed)
@@ -126,13 +151,12 @@ def build_workload(name, cells, seed=123, steps=0, instances=0):
     if name == "ensemble256":
         # capacity per instance: 10k steps grow the largest instance to ~4500 cells
         cap = 1024 if steps <= 500 else 6000
-        insts = [(p, st, cap) for p, st in W.config4()]
-        if instances and instances < len(insts):
-            # a stratified subset (by initial cell count) for small profiling runs
-            order = sorted(range(len(insts)), key=lambda k: (insts[k][1]["n"], k))
-            pick = sorted({order[int(round(q * (len(insts) - 1) / max(instances - 1, 1)))] for q in range(instances)})
-            insts = [insts[k] for k in pick]
-        return insts
+        return _subset([(p, st, cap) for p, st in _config(W.config4)], instances)
+    if name == "het64":
+        # 64 instances of 256..8192 cells at packing 0.4, own bond stiffness;
+        # every cell divides at step 1, so the capacity is a multiple of N0
+        grow = 4 if steps > 500 else 2
+        return _subset([(p, st, grow * st["n"] + 64) for p, st in _config(W.config5)], instances)
     raise ValueError(name)
 
 
@@ -154,7 +178,7 @@ def run_cs3d(args, world, rank, local):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
     insts = build_workload(args.workload, args.cells, steps=args.warmup + args.steps, instances=args.instances)
     n_total = len(insts)
-    if args.workload == "ensemble256" and world > 1:
+    if args.workload in ENSEMBLES and world > 1:
         # instances shard across ranks by predicted cost, no data-path collective
         from cellsim3d_b200 import shard
         mine = shard.partition([shard.predicted_cost(st) for _, st, _ in insts], world)[rank]
@@ -185,22 +209,28 @@ def run_cs3d(args, world, rank, local):
     # final state back
     e2e = None
     if not args.no_e2e:
-        st0 = ens.state(0)
+        # every instance's state from pinned host memory, K steps, every
+        # instance's state back into pinned buffers with room for the capacity
         keys = ("X", "Y", "Z", "VX", "VY", "VZ")
-        host = {k: torch.from_numpy(st0[k]).pin_memory().numpy() for k in keys}
-        # pinned result buffers with room for the capacity (cells may divide)
-        cap_nodes = int(sum(cap for _, _, cap in insts)) * 192
-        res = {k: torch.empty(cap_nodes, dtype=torch.float32).pin_memory().numpy() for k in keys}
+        host, res = [], []
+        for k, (_, _, cap) in enumerate(insts):
+            s = ens.state(k)
+            host.append((s["n"], {q: torch.from_numpy(s[q]).pin_memory().numpy() for q in keys}))
+            res.append({q: torch.empty(cap * 192, dtype=torch.float32).pin_memory().numpy() for q in keys})
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        ens.load_state(0, host["X"], host["Y"], host["Z"], host["VX"], host["VY"], host["VZ"], n_cells=st0["n"])
+        for k, (n, h) in enumerate(host):
+            ens.load_state(k, h["X"], h["Y"], h["Z"], h["VX"], h["VY"], h["VZ"], n_cells=n)
         for _ in range(args.steps):
             ens.step(1)
-        out = ens.state(0, out=res)
+        outs = [ens.state(k, out=res[k]) for k in range(len(insts))]
         t1 = time.perf_counter()
-        state_bytes = 6 * 4 * out["n"] * 192
-        e2e = {"seconds": t1 - t0, "node_steps": st0["n"] * 180 * args.steps,
-               "h2d": state_bytes / args.steps, "d2h": state_bytes / args.steps + 4 * len(insts)}
+        n_in = sum(n for n, _ in host)
+        n_out = sum(o["n"] for o in outs)
+        # node-steps at the starting cell counts (divisions during the K steps not counted)
+        e2e = {"seconds": t1 - t0, "node_steps": n_in * 180 * args.steps,
+               "h2d": 6 * 4 * n_in * 192 / args.steps,
+               "d2h": (6 * 4 * n_out * 192 + 4 * len(insts)) / args.steps + 4 * len(insts)}
     t = torch.tensor([ms], dtype=torch.float64, device="cuda")
     ns = torch.tensor([node_steps], dtype=torch.float64, device="cuda")
     if dist:
@@ -231,7 +261,7 @@ def run_cs3d(args, world, rank, local):
             "dtype": "f32",
             "data": "synthetic (seeded generator, cellsim3d_b200/workloads.py)",
             "config": {"workload": args.workload, "cells": cells_before, "nodes": int(n_nodes),
-                       "parallelism": "replicas" if args.workload != "ensemble256" else "instances sharded",
+                       "parallelism": "instances sharded" if args.workload in ENSEMBLES else "replicas",
                        "l2": "inputs larger than L2 (no flush)" if n_nodes * 32 > 126e6 else "L2 resident",
                        "precision": "FP32 forces/integration, FP64 CoM/volume/division"},
             "roofline": {"bound": "hbm", "kernel": "s1_con_dis", "achieved": achieved, "peak": peak,
@@ -252,13 +282,17 @@ def run_cs3d(args, world, rank, local):
             "max_halo": stats["max_halo"],
             "clocks": clk.summary(),
         }
-        if args.workload == "ensemble256":
+        if args.workload in ENSEMBLES:
             # whole simulations per hour: the timed steps stand for the run of
-            # warmup + steps steps of every instance
+            # warmup + steps steps of every instance.  Every instance advances
+            # one step per ensemble step, so each instance's step time is the
+            # ensemble's step time (p50 = p99).
             secs = ms_max * 1e-3 * (args.warmup + args.steps) / args.steps
             result["ensemble"] = {"instances": n_total, "steps_per_sim": args.warmup + args.steps,
                                   "cells_start": cells_before, "cells_end": cells_after,
-                                  "sims_per_hour": n_total * 3600.0 / secs}
+                                  "sims_per_hour": n_total * 3600.0 / secs,
+                                  "instance_step_ms_p50": ms_max / args.steps,
+                                  "instance_step_ms_p99": ms_max / args.steps}
         if e2e:
             result["e2e"] = {"value": e2e["node_steps"] * world / e2e["seconds"] if world == 1 else
                              e2e["node_steps"] / e2e["seconds"] * world,
@@ -278,9 +312,9 @@ def cpu_baseline(args, steps=None, cells=None):
     import oracle
     from cellsim3d_b200 import workloads as W
     cells = cells or args.cpu_cells
-    insts = build_workload(args.workload, cells) if args.workload == "packed100k" else \
-        build_workload(args.workload, cells)
-    p, st, cap = insts[0]
+    insts = build_workload(args.workload, cells)
+    # ensembles: the instance of median initial size
+    p, st, cap = sorted(insts, key=lambda t: t[1]["n"])[len(insts) // 2]
     mesh = W.load_mesh()
     r0, th = oracle.r0_theta0(st["X"][:192], st["Y"][:192], st["Z"][:192], mesh["nn"])
     topo = oracle.make_topo(mesh["nn"], mesh["sign"], r0, th, mesh["faces"])
@@ -322,13 +356,10 @@ def run_reference(args):
     insts = build_workload(args.workload, args.cells, steps=args.warmup + args.steps)
     topo = make_topology(insts)
     n_all = len(insts)
-    if args.ref_sample and args.ref_sample < n_all:
-        # stratified by initial cell count: every (n_all / k)-th instance in size order
-        order = sorted(range(n_all), key=lambda k: (insts[k][1]["n"], k))
-        pick = sorted({order[int(round(q * (n_all - 1) / (args.ref_sample - 1)))] for q in range(args.ref_sample)})
-        insts = [insts[k] for k in pick]
+    insts = _subset(insts, args.ref_sample)
     total_ms, node_steps, cells0 = 0.0, 0.0, 0
     statuses, max_bin, max_nn, guard = set(), 0, 0, 0.0
+    inst_ms = []
 
     def one(inst):
         p, st, cap = inst
@@ -341,6 +372,7 @@ def run_reference(args):
             if timed <= 0:
                 raise RuntimeError("reference stopped in the warm-up: " + r["status_text"])
             total_ms += r["total_ms"] - r["guard_ms"]
+            inst_ms.append((r["total_ms"] - r["guard_ms"]) / timed)
             node_steps += 0.5 * (st["n"] + r["n"]) * 180 * timed   # cell count grows by division
             cells0 += st["n"]
             statuses.add(r["status_text"])
@@ -362,6 +394,9 @@ def run_reference(args):
                  "sims_per_hour_sequential": len(insts) * 3600.0 / (total_ms * 1e-3),
                  "sims_per_hour_concurrent": len(insts) * 3600.0 / conc}
         value = max(value, node_steps / conc)
+    if len(inst_ms) > 1:
+        extra["instance_step_ms_p50"] = float(np.percentile(inst_ms, 50))
+        extra["instance_step_ms_p99"] = float(np.percentile(inst_ms, 99))
     line.update({
         "value": value, "ms_per_step": total_ms / args.steps, "dtype": "f32",
         "config": {"workload": args.workload, "cells": cells0, "instances": len(insts), "instances_total": n_all,
@@ -391,7 +426,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="cs3d", choices=["cs3d", "reference"])
-    ap.add_argument("--workload", default="packed100k", choices=["packed100k", "colony", "ensemble256", "small8"])
+    ap.add_argument("--workload", default="packed100k", choices=["packed100k", "colony", "ensemble256", "het64", "small8"])
     ap.add_argument("--cells", type=int, default=100_000)
     ap.add_argument("--cpu-cells", type=int, default=10_000)
     ap.add_argument("--cpu-steps", type=int, default=10)
@@ -400,7 +435,7 @@ def main():
     ap.add_argument("--skin", type=float, default=None,
                     help="neighbour-list skin (default: the library's, 0.1)")
     ap.add_argument("--instances", type=int, default=0,
-                    help="ensemble256: a stratified subset of this many instances (0: all 256)")
+                    help="ensembles: a stratified subset of this many instances (0: all)")
     ap.add_argument("--ref-sample", type=int, default=0,
                     help="reference arm, ensembles: run a stratified sample of this many instances (0: all)")
     ap.add_argument("--ref-concurrency", type=int, default=8,

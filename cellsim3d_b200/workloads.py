@@ -211,16 +211,53 @@ def config4(n_inst=256, master_seed=2024):
     return inst
 
 
+def rsa_centres(n, box, rng, min_dist=1.9, margin=1.05):
+    """Random sequential insertion in [margin, box - margin]^3, vectorised:
+    candidates come in batches from the numpy generator `rng`; a candidate is
+    kept if no earlier kept centre (earlier batches, then earlier candidates
+    of its own batch, in order) lies within min_dist, which is sequential
+    insertion of the same candidate stream."""
+    from scipy.spatial import cKDTree
+    pts = np.empty((0, 3))
+    tries = 0
+    while len(pts) < n:
+        m = max(4096, 8 * (n - len(pts)))
+        cand = margin + rng.random((m, 3)) * (box - 2 * margin)
+        tries += m
+        if tries > 50_000_000:
+            raise RuntimeError("random insertion did not converge")
+        if len(pts):
+            d, _ = cKDTree(pts).query(cand, k=1, distance_upper_bound=min_dist)
+            cand = cand[~(d < min_dist)]
+        if len(cand) == 0:
+            continue
+        earlier = [[] for _ in range(len(cand))]
+        for i, j in cKDTree(cand).query_pairs(min_dist, output_type="ndarray"):
+            earlier[max(i, j)].append(min(i, j))
+        keep = np.zeros(len(cand), bool)
+        need, taken = n - len(pts), 0
+        for i in range(len(cand)):
+            if not any(keep[j] for j in earlier[i]):
+                keep[i] = True
+                taken += 1
+                if taken == need:
+                    break
+        pts = np.concatenate([pts, cand[keep]])
+    return pts.astype(np.float32)
+
+
 def config5(n_inst=64, master_seed=2025):
-    """64 instances: N0 ~ U{256..8192}, random centres at packing 0.4, bond
-    stiffness U[500, 2000] (stiffFactor1 = k/1000), seeds 1000..1063."""
+    """64 instances: N0 ~ U{256..8192}, random centres at packing 0.4 of the
+    region the centres occupy (box side (N0 (4/3) pi / 0.4)^(1/3) + 2 x 1.05,
+    centres at least 1.05 from each wall and 1.9 apart), bond stiffness
+    U[500, 2000] (stiffFactor1 = k/1000), dividing, seeds 1000..1063."""
     sm = SplitMix(master_seed)
     inst = []
     for i in range(n_inst):
         n0 = 256 + int(sm.uniform() * (8192 - 256 + 1))
         k = 500 + 1500 * sm.uniform()
-        box = (n0 * (4.0 / 3.0) * math.pi / 0.4) ** (1.0 / 3.0)
-        c = random_centres(n0, box, sm)
+        box = (n0 * (4.0 / 3.0) * math.pi / 0.4) ** (1.0 / 3.0) + 2 * 1.05
+        c = rsa_centres(n0, box, np.random.default_rng([master_seed, i]))
         ij, kl = seed_pair(1000 + i)
         p = base_params(box_len=(box, box, box), stiffness1=float(np.float32(k)),
                         div_time_steps=10 ** 9, rng_ij=ij, rng_kl=kl)

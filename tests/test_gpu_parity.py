@@ -96,19 +96,17 @@ def test_colony_growth_single_steps(mesh):
         single_step_check(sim, "colony step %d" % sim.stats()["steps"])
 
 
-def test_ensemble_instances_single_step(mesh):
-    insts = []
-    for k, (n, gr) in enumerate([(3, 0.002), (1, 0.004), (8, 0.001)]):
-        c = W.random_centres(n, 12.0, W.SplitMix(100 + k))
-        p = W.base_params(box_len=(12.0, 12.0, 12.0), growth_rate=gr, division_vol=2.9 - 0.1 * k,
-                          rng_ij=k, rng_kl=100 * k)
-        insts.append((p, W.state(c)))
+def _ensemble_check(mesh, insts, cap, steps):
+    """Instances of one ensemble against one oracle each: initial forces,
+    `steps` steps (cell counts and division events exact), then one step of
+    every instance from the ensemble's own state (positions bit-exact, forces
+    and velocities within the bar)."""
     topo, otopo = topo_for(insts[0][1], mesh)
-    ens = cs.Ensemble([p for p, _ in insts], topo, [32, 32, 32])
+    ens = cs.Ensemble([p for p, _ in insts], topo, [cap] * len(insts))
     orcs = []
     for k, (p, st) in enumerate(insts):
         ens.load_state(k, st["X"], st["Y"], st["Z"], n_cells=st["n"])
-        o = oracle.System(32, p, otopo)
+        o = oracle.System(cap, p, otopo)
         o.load(st["X"], st["Y"], st["Z"], n=st["n"])
         o.seed(p["rng_ij"], p["rng_kl"])
         o.init()
@@ -117,22 +115,22 @@ def test_ensemble_instances_single_step(mesh):
         f = ens.forces(k)
         ec = rel_err([f["FCX"], f["FCY"], f["FCZ"]], [o.FC[0], o.FC[1], o.FC[2]], o.n)
         assert ec[0] < TOL, (k, ec)
-    ens.step(30)
+    ens.step(steps)
     for k, o in enumerate(orcs):
-        o.step(30)
+        o.step(steps)
         assert ens.n_cells(k) == o.n
         assert np.array_equal(ens.events(k), o.events())
     # single step of every instance from the ensemble's own state
     snaps = []
-    for k in range(3):
+    for k in range(len(insts)):
         s = ens.state(k)
         s.update(ens.forces(k))
         s.update(ens.random_force(k))
         s["cm"] = ens.cells(k)["cm"]
         s["rng"] = ens.get_rng(k)
-        s["step"] = 30
+        s["step"] = steps
         snaps.append(s)
-    Os = [oracle_from(snaps[k], insts[k][0], otopo, 32, record=False) for k in range(3)]
+    Os = [oracle_from(snaps[k], insts[k][0], otopo, cap, record=False) for k in range(len(insts))]
     ens.step(1)
     for k, O in enumerate(Os):
         O.step(1)
@@ -145,6 +143,36 @@ def test_ensemble_instances_single_step(mesh):
         ev = rel_err([s["VX"], s["VY"], s["VZ"]], [O.VX, O.VY, O.VZ], n)
         print("ensemble inst %d n %d Fc %s V %s" % (k, n, ec, ev))
         assert ec[0] < TOL and ev[0] < TOL
+    for o in orcs + Os:
+        o.close()
+    ens.close()
+
+
+def test_ensemble_instances_single_step(mesh):
+    """Instances in the manner of the 256-instance ensemble: own cell counts,
+    growth rates, division volumes and seeds."""
+    insts = []
+    for k, (n, gr) in enumerate([(3, 0.002), (1, 0.004), (8, 0.001)]):
+        c = W.random_centres(n, 12.0, W.SplitMix(100 + k))
+        p = W.base_params(box_len=(12.0, 12.0, 12.0), growth_rate=gr, division_vol=2.9 - 0.1 * k,
+                          rng_ij=k, rng_kl=100 * k)
+        insts.append((p, W.state(c)))
+    _ensemble_check(mesh, insts, 32, 30)
+
+
+def test_ensemble_packed_stiffness_instances(mesh):
+    """Instances in the manner of the 64-instance heterogeneous ensemble:
+    packing 0.4, own bond stiffness (stiffFactor1 = k/1000, contact stays at
+    Young's modulus), own boxes, seeds above 300 folded into RANMAR's range;
+    every cell divides at step 1."""
+    insts = []
+    for k, (n, stiff, seed) in enumerate([(12, 500.0, 1000), (20, 1250.0, 1031), (30, 2000.0, 1063)]):
+        box = (n * (4.0 / 3.0) * np.pi / 0.4) ** (1.0 / 3.0) + 2.1
+        c = W.rsa_centres(n, box, np.random.default_rng([7, k]))
+        ij, kl = W.seed_pair(seed)
+        p = W.base_params(box_len=(box, box, box), stiffness1=stiff, div_time_steps=10 ** 9, rng_ij=ij, rng_kl=kl)
+        insts.append((p, W.state(c)))
+    _ensemble_check(mesh, insts, 96, 40)
 
 
 def test_nan_input_raises_error_bit(mesh):
