@@ -139,6 +139,17 @@ def initialize_C180s(cfg, mesh, n_cells, rng=None):
     return X, Y, Z
 
 
+def initial_stiffness(cfg, X, Y, Z, n_cells, rng=None):
+    """Bond stiffness of the initial cells (src/GPUbounce.cu:616-692): stiffness1,
+    or stiffness2 for the softer cells the config selects."""
+    out = np.zeros(max(n_cells, 1), dtype=np.float32)
+    X, Y, Z = _f32(X), _f32(Y), _f32(Z)
+    st = _lib.lib().cs3d_initial_stiffness(C.byref(cfg), int(n_cells), _fp(X), _fp(Y), _fp(Z),
+                                           C.byref(rng.state) if rng is not None else None, _fp(out))
+    _lib.check(st, "initial_stiffness")
+    return out[:n_cells]
+
+
 class Ensemble:
     """Independent simulations stepped together on one GPU.
 
@@ -300,6 +311,16 @@ class Ensemble:
         _lib.check(L.cs3d_get_events(self.h, inst, None, 0, C.byref(cnt)), "cs3d_get_events")
         out = np.zeros((max(cnt.value, 1), 3), dtype=np.int32)
         _lib.check(L.cs3d_get_events(self.h, inst, _ip(out), cnt.value, C.byref(cnt)), "cs3d_get_events")
+        return out[:cnt.value]
+
+    def far_counts(self, inst=0):
+        """(step, cells) of the division steps whose far cells the internal-cells
+        mitotic count left out."""
+        cnt = C.c_int32()
+        L = _lib.lib()
+        _lib.check(L.cs3d_get_far_counts(self.h, inst, None, 0, C.byref(cnt)), "cs3d_get_far_counts")
+        out = np.zeros((max(cnt.value, 1), 2), dtype=np.int32)
+        _lib.check(L.cs3d_get_far_counts(self.h, inst, _ip(out), cnt.value, C.byref(cnt)), "cs3d_get_far_counts")
         return out[:cnt.value]
 
     def last_error(self, inst=0):

@@ -15,7 +15,7 @@ E_CAPACITY = -69
 
 ERRBITS = {0x001: "NAN", 0x002: "CAPACITY", 0x004: "CAND_OVERFLOW", 0x008: "ENTRY_OVERFLOW",
            0x010: "NONFINITE_VOL", 0x020: "BAD_NORMAL", 0x040: "GRID_OVERFLOW", 0x080: "PAIR_OVERFLOW",
-           0x100: "HALO_OVERFLOW"}
+           0x100: "HALO_OVERFLOW", 0x200: "SOFT_CELLS"}
 
 OPT_RECORD_PAIRS, OPT_SKIN, OPT_PAIR_CAPACITY, OPT_REBUILD = 1, 2, 3, 4
 
@@ -28,7 +28,11 @@ class Params(C.Structure):
         "growth_rate", "thresh_dist")] + [("box_len", C.c_float * 3)] + [(n, C.c_int32) for n in (
         "check_sphericity", "constrain_angles", "use_rigid_box", "daught_same_stiffness",
         "div_time_steps", "rng_ij", "rng_kl", "add_rands")] + [("rand_scale_factor", C.c_float),
-                                                             ("rand_seed", C.c_int32), ("correct_com", C.c_int32)]
+                                                             ("rand_seed", C.c_int32), ("correct_com", C.c_int32),
+        ("use_different_stiffnesses", C.c_int32), ("stiffness2", C.c_float), ("phase_count", C.c_int32),
+        ("soften_after_growth", C.c_int32), ("number_of_softer_cells", C.c_int32),
+        ("fraction_of_softer_cells", C.c_float), ("choose_random_cell_indices", C.c_int32),
+        ("closeness_to_center", C.c_float), ("count_internal_radius", C.c_float)]
 
 
 class Topology(C.Structure):
@@ -76,10 +80,10 @@ Config = type("Config", (C.Structure,), {"_fields_": [
 EXPORTS = [
     "cs3d_version", "cs3d_strerror", "cs3d_config_read_json", "cs3d_config_to_params", "cs3d_mesh_read",
     "cs3d_topology_build", "cs3d_rng_init", "cs3d_rng_draw", "cs3d_rng_random_vector", "cs3d_seed_map",
-    "cs3d_init_positions", "cs3d_traj_open", "cs3d_traj_write_frame", "cs3d_traj_close", "cs3d_create",
+    "cs3d_initial_stiffness", "cs3d_init_positions", "cs3d_traj_open", "cs3d_traj_write_frame", "cs3d_traj_close", "cs3d_create",
     "cs3d_create_ensemble", "cs3d_load_state", "cs3d_set_rng", "cs3d_get_rng", "cs3d_step", "cs3d_get_state",
     "cs3d_get_forces", "cs3d_get_random_force", "cs3d_get_cells", "cs3d_get_grid", "cs3d_set_option", "cs3d_get_pairs",
-    "cs3d_get_events", "cs3d_last_error", "cs3d_get_stats", "cs3d_profile_step", "cs3d_last_step_ms",
+    "cs3d_get_events", "cs3d_get_far_counts", "cs3d_last_error", "cs3d_get_stats", "cs3d_profile_step", "cs3d_last_step_ms",
     "cs3d_destroy", "cs3d_forces_static",
 ]
 
@@ -120,6 +124,7 @@ def lib():
     L.cs3d_rng_random_vector.argtypes = [C.POINTER(Rng), fp]
     L.cs3d_seed_map.argtypes = [C.c_int, ip, ip]
     L.cs3d_init_positions.argtypes = [C.POINTER(Config), C.POINTER(Mesh), C.c_int, C.POINTER(Rng), fp, fp, fp]
+    L.cs3d_initial_stiffness.argtypes = [C.POINTER(Config), C.c_int, fp, fp, fp, C.POINTER(Rng), fp]
     L.cs3d_traj_open.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(P)]
     L.cs3d_traj_write_frame.argtypes = [P, C.c_int, C.c_int, C.c_int, fp, fp, fp, ip]
     L.cs3d_traj_close.argtypes = [P, C.c_int]
@@ -138,6 +143,7 @@ def lib():
     L.cs3d_set_option.argtypes = [P, C.c_int, C.c_longlong]
     L.cs3d_get_pairs.argtypes = [P, C.c_int, C.c_int, ip, C.c_longlong, C.POINTER(C.c_longlong)]
     L.cs3d_get_events.argtypes = [P, C.c_int, ip, C.c_int, ip]
+    L.cs3d_get_far_counts.argtypes = [P, C.c_int, ip, C.c_int, ip]
     L.cs3d_last_error.argtypes = [P, C.c_int, C.POINTER(C.c_uint32)]
     L.cs3d_get_stats.argtypes = [P, C.POINTER(C.c_longlong), C.c_int]
     L.cs3d_profile_step.argtypes = [P, C.c_int, fp, C.c_char_p, C.c_int, C.c_int, ip]

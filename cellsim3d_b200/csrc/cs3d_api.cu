@@ -31,6 +31,8 @@ struct cs3d_ctx {
     int max_div_steps = 0;
     bool any_growth = false;
     bool any_com = false;          // some instance corrects its centre-of-mass motion
+    bool any_far = false;          // some instance counts internal cells only (mitotic index)
+    std::vector<long long> soften_steps;  // steps whose end softens cells (stiffness schedule)
     float skin = 0.1f;
     int grid_cells = 0;            // blocks of the per-cell kernels
     int grid_flat = 0;             // blocks of the per-thread kernels
@@ -199,6 +201,15 @@ InstParams make_inst(const cs3d_params &p, int base, int cap, float skin)
     q.rdt = sqrtf(p.time_interval);
     q.rseed = (unsigned)p.rand_seed;
     q.correct_com = p.correct_com ? 1 : 0;
+    q.diffE = p.use_different_stiffnesses ? 1 : 0;
+    q.E2 = p.stiffness2;
+    q.phase = p.phase_count;
+    q.soften = p.use_different_stiffnesses && p.soften_after_growth ? 1 : 0;
+    q.soft_n = p.number_of_softer_cells;
+    q.soft_frac = p.fraction_of_softer_cells;
+    q.soft_rand = p.choose_random_cell_indices ? 1 : 0;
+    q.closeness = p.closeness_to_center;
+    q.far_r = p.count_internal_radius > 0.0f ? p.count_internal_radius : 0.0f;
     return q;
 }
 
@@ -315,8 +326,10 @@ int run_init(cs3d_ctx *c)
 // One timestep, src/GPUbounce.cu:1055-1338, as a fixed launch sequence.
 // k1: the step starts with k_integrate (else the previous step's fused S2
 // did it); fuse: S2 also integrates the next step (no division this step,
-// and the next step follows in the same call).
-int launch_step(cs3d_ctx *c, int par, bool div, bool k1 = true, bool fuse = false, const Prof &pf = Prof())
+// and the next step follows in the same call); soften: the number of this
+// step when its end softens cells (launched outside the graphs), else 0.
+int launch_step(cs3d_ctx *c, int par, bool div, bool k1 = true, bool fuse = false, const Prof &pf = Prof(),
+                long long soften = 0)
 {
     const Dev &d = c->d;
     cudaStream_t s = c->stream;
@@ -335,11 +348,18 @@ int launch_step(cs3d_ctx *c, int par, bool div, bool k1 = true, bool fuse = fals
         k_div_select<<<c->n_inst, 256, 0, s>>>(d, par); ++n; pf.mark(s, "div_select");
         k_div_apply<<<c->grid_cells, SLOTS, 0, s>>>(d, par); ++n; pf.mark(s, "div_apply");
         k_grid_fix<<<c->grid_flat, 256, 0, s>>>(d, par); ++n; pf.mark(s, "grid_fix");
+        if (c->any_far) { k_far_count<<<c->n_inst, 32, 0, s>>>(d); ++n; pf.mark(s, "far_count"); }
     }
+    if (soften) { k_soften<<<c->n_inst, 32, 0, s>>>(d, (int)soften); ++n; pf.mark(s, "soften"); }
     if (c->any_com) { k_com_shift<<<c->n_inst, 256, 0, s>>>(d); ++n; pf.mark(s, "com_shift"); }
     CK(cudaGetLastError());
     c->launches_per_step = n;
     return CS3D_OK;
+}
+
+bool is_soften_step(const cs3d_ctx *c, long long s)
+{
+    return std::find(c->soften_steps.begin(), c->soften_steps.end(), s) != c->soften_steps.end();
 }
 
 int get_graph(cs3d_ctx *c, int par, bool div, bool k1, bool fuse, cudaGraphExec_t *out)
@@ -446,6 +466,12 @@ int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topol
         base += capacity[k];
         if (params[k].growth_rate > 0) c->any_growth = true;
         if (params[k].correct_com) c->any_com = true;
+        if (params[k].count_internal_radius > 0) c->any_far = true;
+        if (params[k].use_different_stiffnesses && params[k].soften_after_growth) {
+            const long long s = (long long)params[k].div_time_steps + 2;
+            if (std::find(c->soften_steps.begin(), c->soften_steps.end(), s) == c->soften_steps.end())
+                c->soften_steps.push_back(s);
+        }
         c->max_div_steps = std::max(c->max_div_steps, params[k].div_time_steps);
     }
     Dev &d = c->d;
@@ -475,6 +501,9 @@ int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topol
     AL(d.divtab, c->cap_total); AL(d.div_total, 1);
     d.ev_cap = std::max(1 << 16, 2 * c->cap_total);
     AL(d.events, d.ev_cap); AL(d.n_events, 1);
+    d.far_cap = d.ev_cap;
+    AL(d.farlog, d.far_cap); AL(d.n_far, 1);
+    AL(d.pick, (size_t)c->cap_total + n_inst);
     AL(d.flags, 4);
     d.pair_cap = 1;
     AL(d.pairs, 1); AL(d.n_pairs, 1);
@@ -491,6 +520,7 @@ int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topol
             free_all(c); delete c; return CS3D_E_CONFIG;
         }
         memcpy(st[k].u, r.u, sizeof r.u);
+        st[k].syscm[0] = st[k].syscm[1] = st[k].syscm[2] = 1.0f;   // src/GPUbounce.cu:240
         st[k].rc = r.c; st[k].rcd = r.cd; st[k].rcm = r.cm; st[k].i97 = r.i97; st[k].j97 = r.j97;
         for (int q = 0; q < capacity[k]; ++q) owner[c->hprm[k].base + q] = k;
     }
@@ -620,6 +650,8 @@ int cs3d_load_state(cs3d_ctx *c, int inst, int n, const float *X, const float *Y
     int zero = 0;
     CK(cudaMemcpyAsync(&d.st[inst].step, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(&d.st[inst].err, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    static const float one3[3] = {1.0f, 1.0f, 1.0f};   // the reference's initial system centre
+    CK(cudaMemcpyAsync(d.st[inst].syscm, one3, sizeof one3, cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     c->hn[inst] = n;
     c->need_init = true;
@@ -666,10 +698,16 @@ int cs3d_step(cs3d_ctx *c, int n_steps)
         long long s = c->host_step + 1;
         int par = (int)((s - 1) & 1);
         bool div = c->any_growth && s <= c->max_div_steps;
-        bool fuse = !div && !c->any_com && k + 1 < n_steps;
-        cudaGraphExec_t g;
-        if ((rc = get_graph(c, par, div, k1, fuse, &g))) return rc;
-        CK(cudaGraphLaunch(g, c->stream));
+        const bool soften = is_soften_step(c, s);
+        bool fuse = !div && !c->any_com && !soften && k + 1 < n_steps;
+        if (soften) {
+            // the one step that softens cells runs outside the graphs
+            if ((rc = launch_step(c, par, div, k1, false, Prof(), s))) return rc;
+        } else {
+            cudaGraphExec_t g;
+            if ((rc = get_graph(c, par, div, k1, fuse, &g))) return rc;
+            CK(cudaGraphLaunch(g, c->stream));
+        }
         c->host_step = s;
         k1 = !fuse;
     }
@@ -704,7 +742,7 @@ int cs3d_profile_step(cs3d_ctx *c, int n_steps, float *kernel_ms, char *names, i
         cudaEvent_t e0;
         CK(cudaEventCreate(&e0));
         CK(cudaEventRecord(e0, c->stream));
-        if ((rc = launch_step(c, par, div, true, false, pf))) return rc;
+        if ((rc = launch_step(c, par, div, true, false, pf, is_soften_step(c, st) ? st : 0))) return rc;
         c->host_step = st;
         CK(cudaEventSynchronize(ev.empty() ? e0 : ev.back()));
         if (acc.size() < ev.size()) { acc.resize(ev.size(), 0.0); first_names = nm; }
@@ -891,6 +929,29 @@ int cs3d_get_events(cs3d_ctx *c, int inst, int32_t *out, int max_events, int *co
         ++k;
     }
     *count = k;
+    return CS3D_OK;
+}
+
+int cs3d_get_far_counts(cs3d_ctx *c, int inst, int32_t *out, int max_entries, int *n_entries)
+{
+    if (!c || inst < 0 || inst >= c->n_inst || !n_entries) return CS3D_E_ARG;
+    cudaSetDevice(c->device);
+    int nf = 0;
+    CK(cudaMemcpyAsync(&nf, c->d.n_far, sizeof nf, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    nf = std::min(nf, c->d.far_cap);
+    std::vector<int4> buf(nf);
+    if (nf) CK(cudaMemcpyAsync(buf.data(), c->d.farlog, sizeof(int4) * nf, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::vector<int4> mine;
+    for (auto &e : buf) if (e.x == inst) mine.push_back(e);
+    std::sort(mine.begin(), mine.end(), [](const int4 &a, const int4 &b) { return a.y < b.y; });
+    int k = 0;
+    for (auto &e : mine) {
+        if (out && k < max_entries) { out[2 * k] = e.y; out[2 * k + 1] = e.z; }
+        ++k;
+    }
+    *n_entries = k;
     return CS3D_OK;
 }
 

@@ -33,6 +33,15 @@ struct InstParams {
     float rdt;      // sqrtf(dt), the random force's weight in the kicks
     unsigned rseed; // Philox key
     int correct_com;
+    int diffE;      // variable stiffness: soft cells lose their pressure from step `phase` on
+    float E2;       // stiffness2
+    int phase;      // phase_count
+    int soften;     // more cells softened at the end of step div_steps + 2
+    int soft_n;     // numberOfSofterCells
+    float soft_frac;// fractionOfSofterCells (> 0: replaces soft_n)
+    int soft_rand;  // RANMAR picks instead of the central cells
+    float closeness;// closenessToCenter
+    float far_r;    // radius_cutoff of the internal-cells mitotic count (0: off)
 };
 
 // Per-instance mutable state (device resident).
@@ -52,6 +61,8 @@ struct InstState {
     int hbits;             // log2 of the slice size (0: not rebuilding)
     int built;             // cells whose lists were built (cumulative)
     int rebuilds;
+    float syscm[3];        // the reference's system centre of mass as of its last
+                           // calc_sys_CM call, (1, 1, 1) before the first one
     // RANMAR, src/marsaglia.h:50-52
     float u[98];
     float rc, rcd, rcm;
@@ -119,6 +130,10 @@ struct Dev {
     DivEntry *divtab;
     int *div_total;
     int4 *events;       // (inst, step, parent, daughter)
+    int4 *farlog;       // (inst, step, far cells, 0) of the internal-cells mitotic count
+    int *n_far;
+    int far_cap;
+    uint8_t *pick;      // [cap_total + n_inst] flags of the random soft-cell picks
     int *n_events;
     int ev_cap;
     int *flags;         // [0] any rebuild, [1] any division

@@ -5,6 +5,7 @@
 // with -ffp-contract=off so no FMA contraction changes a rounding.
 #include "../../include/cs3d.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -409,10 +410,23 @@ int cs3d_config_to_params(const cs3d_config *c, cs3d_params *p)
     p->rand_scale_factor = c->rand_scale_factor;
     p->rand_seed = c->rand_seed;   // <= 0: the caller picks one (the reference seeds from time())
     p->correct_com = c->correct_com ? 1 : 0;
+    p->use_different_stiffnesses = c->use_different_stiffnesses ? 1 : 0;
+    p->stiffness2 = c->soft_stiff_factor * c->youngs_mod;
+    p->phase_count = c->phase_count;
+    p->soften_after_growth = c->use_different_stiffnesses && !c->during_growth ? 1 : 0;
+    p->number_of_softer_cells = c->number_of_softer_cells;
+    p->fraction_of_softer_cells = c->fraction_of_softer_cells;
+    p->choose_random_cell_indices = c->choose_random_cell_indices ? 1 : 0;
+    p->closeness_to_center = c->closeness_to_center;
+    p->count_internal_radius = c->count_only_internal ? c->radius_cutoff : 0.0f;
     // Features of the reference this build leaves out (all off in the
     // reference's shipped inp.json and in every benchmark configuration).
-    if (c->use_different_stiffnesses || c->do_pop_model ||
-        c->use_div_plane_basis || c->use_walls || c->use_pbcs || c->do_adaptive_dt)
+    // recalc_r0: the reference's CalculateR0 (src/BondKernels.cu:3-37) stores
+    // per-cell mean bond lengths into the 3x192 per-bond table d_R0
+    // (src/GPUbounce.cu:400), past its end from cell 576 on, so the behaviour
+    // it asks for is not defined.
+    if (c->do_pop_model || c->use_div_plane_basis || c->use_walls || c->use_pbcs || c->do_adaptive_dt ||
+        (c->use_different_stiffnesses && c->recalc_r0))
         return CS3D_E_UNSUPPORTED;
     return CS3D_OK;
 }
@@ -564,6 +578,85 @@ int cs3d_rng_random_vector(cs3d_rng *r, float n[3])
     n[0] = 2 * x1 * sqrtf(1 - x1 * x1 - x2 * x2);
     n[1] = 2 * x2 * sqrtf(1 - x1 * x1 - x2 * x2);
     n[2] = 1 - 2 * (x1 * x1 + x2 * x2);
+    return CS3D_OK;
+}
+
+// Centre of mass of one cell as the device computes it: six groups of 32
+// slots (180..191 zero), each reduced pairwise in double, the group sums
+// added in order, divided by 180 and rounded to float.
+static float cell_mean(const float *v)
+{
+    double tot = 0.0;
+    for (int g = 0; g < 6; ++g) {
+        double w[32];
+        for (int l = 0; l < 32; ++l) w[l] = 32 * g + l < 180 ? (double)v[32 * g + l] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            double t[32];
+            for (int l = 0; l < 32; ++l) t[l] = w[l] + w[l ^ o];
+            memcpy(w, t, sizeof w);
+        }
+        tot += w[0];
+    }
+    return (float)(tot / 180.0);
+}
+
+// src/GPUbounce.cu:616-692.  The reference takes the centres of mass from
+// its CenterOfMass kernel (float tree sum); they come from cell_mean here,
+// the centre of mass of every other use in this library.
+int cs3d_initial_stiffness(const cs3d_config *cfg, int n, const float *X, const float *Y, const float *Z,
+                           cs3d_rng *rng, float *youngs)
+{
+    if (!cfg || n < 0 || (n && !youngs)) return CS3D_E_ARG;
+    const float stiffness1 = cfg->stiff_factor1 * cfg->youngs_mod;
+    const float stiffness2 = cfg->soft_stiff_factor * cfg->youngs_mod;
+    for (int i = 0; i < n; ++i) youngs[i] = stiffness1;
+    if (!cfg->use_different_stiffnesses || n == 0) return CS3D_OK;
+    const float close = cfg->closeness_to_center;
+    if (close > 0.f && close < 1.f) {
+        if (!X || !Y || !Z) return CS3D_E_ARG;
+        std::vector<float> cx(n), cy(n), cz(n);
+        float sx = 0.f, sy = 0.f, sz = 0.f;
+        for (int i = 0; i < n; ++i) {
+            cx[i] = cell_mean(X + (size_t)i * 192);
+            cy[i] = cell_mean(Y + (size_t)i * 192);
+            cz[i] = cell_mean(Z + (size_t)i * 192);
+            sx = sx + cx[i];
+            sy = sy + cy[i];
+            sz = sz + cz[i];
+        }
+        // float3 / float is (1/a) * b, inc/VectorFunctions.hpp:84-92
+        const float inv = 1.0f / (float)n;
+        sx = inv * sx;
+        sy = inv * sy;
+        sz = inv * sz;
+        std::vector<float> mags(n);
+        float rmax = 0.f;
+        for (int i = 0; i < n; ++i) {
+            const float dx = cx[i] - sx, dy = cy[i] - sy, dz = cz[i] - sz;
+            mags[i] = sqrtf(dx * dx + dy * dy + dz * dz);
+            rmax = std::max(rmax, mags[i]);
+        }
+        for (int i = 0; i < n; ++i)
+            if (mags[i] / rmax <= close) youngs[i] = stiffness2;
+        return CS3D_OK;
+    }
+    int count = cfg->number_of_softer_cells;
+    const float frac = cfg->fraction_of_softer_cells;
+    if (frac > 0.f && frac < 1.f) count = (int)roundf(frac * (float)n);
+    if (count > n) return CS3D_E_CONFIG;
+    if (cfg->use_rigid_box) {
+        for (int i = 0; i < count; ++i) youngs[i] = stiffness2;
+        return CS3D_OK;
+    }
+    if (!rng || !rng->ok) return CS3D_E_ARG;
+    for (int i = 0; i < count; ++i) {
+        float u;
+        cs3d_rng_draw(rng, &u, 1);
+        const int ind = (int)roundf(u * (float)n);
+        // ind == n names the next free slot, which a division overwrites before
+        // any use (src/GPUbounce.cu:1257-1261)
+        if (ind < n) youngs[ind] = stiffness2;
+    }
     return CS3D_OK;
 }
 

@@ -403,9 +403,22 @@ __device__ __forceinline__ float3 dis_force(const InstParams &P, const float4 *v
                        (float)(-gi * dz - ge * vt.z - go * v.z));
 }
 
+// PressureUpdate, src/PressureKernels.cu:4-40, for the step `step` being
+// taken: with variable stiffness, from step phase_count on a cell whose
+// stiffness is not stiffness1 has pressure 0; every other cell grows by the
+// growth rate up to maxPressure.
+__device__ __forceinline__ void pressure_update(const Dev &d, const InstParams &P, int a, int step)
+{
+    if (P.diffE && step >= P.phase && d.E[a] != P.stiff1) {
+        if (d.press[a] != 0.0f) d.press[a] = 0.0f;
+    } else if (d.press[a] < P.maxp) {
+        d.press[a] = d.press[a] + P.growth;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // K1: first half kick + drift of a step (Integrate + ForwardTime,
-// src/propagate.cu:681-763) and PressureUpdate (src/PressureKernels.cu:35-39).
+// src/propagate.cu:681-763) and PressureUpdate (src/PressureKernels.cu:4-40).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(SLOTS) k_integrate(Dev d)
 {
@@ -449,7 +462,7 @@ __global__ void __launch_bounds__(SLOTS) k_integrate(Dev d)
             float m = smax[0];
             for (int q = 1; q < SLOTS / 32; ++q) m = fmaxf(m, smax[q]);
             atomicMax(&d.st[inst].disp_step, __float_as_uint(m));
-            if (d.press[a] < P.maxp) d.press[a] = d.press[a] + P.growth;
+            pressure_update(d, P, a, d.st[inst].step + 1);
         }
         __syncthreads();
     }
@@ -932,7 +945,7 @@ __global__ void __launch_bounds__(SLOTS, 5) k_s2(Dev d, int par)
                 float mx = smax[0];  // visible: cell_geom synchronises the block
                 for (int q = 1; q < SLOTS / 32; ++q) mx = fmaxf(mx, smax[q]);
                 atomicMax(&st->disp_step, __float_as_uint(mx));
-                if (d.press[a] < P.maxp) d.press[a] = d.press[a] + P.growth;  // PressureUpdate
+                pressure_update(d, P, a, st->step + 1);  // the next step's PressureUpdate
             }
             d.CM[a] = make_float4(cm.x, cm.y, cm.z, 0.f);
             d.aabb[pn][2 * a] = lo;
@@ -1191,6 +1204,9 @@ __global__ void __launch_bounds__(256) k_com_shift(Dev d)
         sys[0] = __fdiv_rn(sx, (float)n);
         sys[1] = __fdiv_rn(sy, (float)n);
         sys[2] = __fdiv_rn(sz, (float)n);
+        d.st[k].syscm[0] = sys[0];
+        d.st[k].syscm[1] = sys[1];
+        d.st[k].syscm[2] = sys[2];
     }
     __syncthreads();
     const float ox = sys[0], oy = sys[1], oz = sys[2];
@@ -1202,6 +1218,114 @@ __global__ void __launch_bounds__(256) k_com_shift(Dev d)
         d.X[g] = x;
         d.Xb[g] = b;
     }
+}
+
+// calc_sys_CM, src/GPUbounce.cu:2504-2520: the float mean of the first n
+// centres of mass, summed in cell order; recorded as the instance's system
+// centre.
+__device__ float3 sys_centre(const Dev &d, const InstParams &P, InstState *st, int n)
+{
+    float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+    for (int c = 0; c < n; ++c) {
+        const float4 cm = d.CM[P.base + c];
+        sx = __fadd_rn(sx, cm.x);
+        sy = __fadd_rn(sy, cm.y);
+        sz = __fadd_rn(sz, cm.z);
+    }
+    sx = __fdiv_rn(sx, (float)n);
+    sy = __fdiv_rn(sy, (float)n);
+    sz = __fdiv_rn(sz, (float)n);
+    st->syscm[0] = sx;
+    st->syscm[1] = sy;
+    st->syscm[2] = sz;
+    return make_float3(sx, sy, sz);
+}
+
+__device__ __forceinline__ float dist2(float4 cm, float3 o)
+{
+    const float dx = __fsub_rn(cm.x, o.x), dy = __fsub_rn(cm.y, o.y), dz = __fsub_rn(cm.z, o.z);
+    return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+}
+
+// getRmax2, src/GPUbounce.cu:2523-2536: the largest squared distance of the
+// first n centres of mass from the recorded system centre.
+__device__ float rmax2_from(const Dev &d, const InstParams &P, const InstState *st, int n)
+{
+    const float3 o = make_float3(st->syscm[0], st->syscm[1], st->syscm[2]);
+    float r2 = 0.0f;
+    for (int c = 0; c < n; ++c) {
+        const float v = dist2(d.CM[P.base + c], o);
+        r2 = r2 < v ? v : r2;   // std::max
+    }
+    return r2;
+}
+
+// num_cells_far, src/GPUbounce.cu:1288-1290 and :2538-2565, after the
+// divisions of a step (count_only_internal_cells): the newest div_count cells
+// whose centre of mass lies farther than radius_cutoff x the largest distance
+// from the system's centre are not counted as dividing.  The daughters'
+// centres of mass are still 0 here (computed in their first step), as in the
+// reference.  One thread per instance.
+__global__ void k_far_count(Dev d)
+{
+    const int k = blockIdx.x;
+    if (k >= d.n_inst || threadIdx.x != 0) return;
+    const InstParams &P = d.prm[k];
+    InstState *st = &d.st[k];
+    if (!(P.far_r > 0.0f) || !(st->step <= P.div_steps && P.growth > 0.0f)) return;
+    const int n = st->n, nd = st->div_count;
+    if (nd == 0 || n < 50) return;
+    const float3 o = sys_centre(d, P, st, n);
+    const float thr = __fmul_rn(__fmul_rn(P.far_r, P.far_r), rmax2_from(d, P, st, n));
+    int far = 0;
+    for (int c = n - nd; c < n; ++c)
+        if (dist2(d.CM[P.base + c], o) > thr) ++far;
+    if (far) {
+        const int q = atomicAdd(d.n_far, 1);
+        if (q < d.far_cap) d.farlog[q] = make_int4(k, st->step, far, 0);
+    }
+}
+
+// Cells softened when growth ends, src/GPUbounce.cu:1340-1429 (duringGrowth
+// off): at the end of step div_time_steps + 2, after the step's grid and
+// before its CoM correction.  One thread per instance runs the reference's
+// host loops in their order.
+__global__ void k_soften(Dev d, int step)
+{
+    const int k = blockIdx.x;
+    if (k >= d.n_inst || threadIdx.x != 0) return;
+    const InstParams &P = d.prm[k];
+    InstState *st = &d.st[k];
+    if (!P.soften || st->step != step || P.div_steps + 2 != step) return;
+    const int n = st->n;
+    int count = P.soft_n;
+    if (P.soft_frac > 0.0f) count = (int)roundf(__fmul_rn(P.soft_frac, (float)n));
+    float *E = d.E + P.base;
+    if (P.soft_rand) {
+        // distinct picks roundf(u * n) in [0, n]; n itself names no cell
+        if (count > n + 1) { atomicOr(&st->err, CS3D_ERRBIT_SOFT_CELLS); return; }
+        uint8_t *pick = d.pick + P.base + k;
+        for (int c = 0; c <= n; ++c) pick[c] = 0;
+        long long draws = 0;
+        for (int got = 0; got < count;) {
+            if (++draws > 64ll * (n + 1) + (1ll << 20)) { atomicOr(&st->err, CS3D_ERRBIT_SOFT_CELLS); break; }
+            float u;
+            ranmar_dev(st, &u, 1);
+            const int ind = (int)roundf(__fmul_rn(u, (float)n));
+            if (!pick[ind]) { pick[ind] = 1; ++got; }
+        }
+        for (int c = 0; c < n; ++c)
+            if (pick[c]) E[c] = P.E2;
+        return;
+    }
+    // getRmax2 runs before calc_sys_CM here (src/GPUbounce.cu:1399-1402), so
+    // it measures from the previously recorded system centre
+    const float r2max = rmax2_from(d, P, st, n);
+    const float3 o = sys_centre(d, P, st, n);
+    const float f = __fsub_rn(1.0f, P.closeness);
+    const float thr = __fmul_rn(__fmul_rn(f, f), r2max);
+    for (int c = 0, got = 0; got < count && c < n; ++c)
+        if (dist2(d.CM[P.base + c], o) <= thr) { E[c] = P.E2; ++got; }
 }
 
 // G: grid extents of instances that divided this step, from all boxes.

@@ -52,13 +52,25 @@ bool read_init_file(const char *path, int &n, std::vector<float> &a, std::vector
     return ok;
 }
 
-void write_ascii_frame(FILE *f, int step, int interval, int n, const float *X, const float *Y, const float *Z)
+// Stiffness class of every cell for the trajectory: 0 (stiffness1) or 1,
+// src/GPUbounce.cu:2459-2464.
+void cell_types(const cs3d_params &p, int n, const float *E, std::vector<int32_t> &t)
 {
-    // write_traj, src/GPUbounce.cu:2412-2444
+    t.resize(n > 0 ? n : 1);
+    for (int c = 0; c < n; ++c) t[c] = E[c] == p.stiffness1 ? 0 : 1;
+}
+
+void write_ascii_frame(FILE *f, int step, int interval, int n, const float *X, const float *Y, const float *Z,
+                       const cs3d_params &prm, const float *E)
+{
+    // write_traj, src/GPUbounce.cu:2412-2444 (cell labels H / C with variable stiffness)
     fprintf(f, "%d\n", n * 192);
     fprintf(f, "Step: %d frame: %d\n", step, step / interval);
     for (int c = 0; c < n; c++) {
-        fprintf(f, "cell: %d\n", c);
+        if (!prm.use_different_stiffnesses) fprintf(f, "cell: %d\n", c);
+        else if (E[c] == prm.stiffness1) fprintf(f, "cell: %d H\n", c);
+        else if (E[c] == prm.stiffness2) fprintf(f, "cell: %d C\n", c);
+        else fprintf(f, "cell: %d UnknownStiffness\n", c);
         for (int p = 0; p < 192; p++)
             fprintf(f, "%.7f,  %.7f,  %.7f\n", X[c * 192 + p], Y[c * 192 + p], Z[c * 192 + p]);
     }
@@ -120,6 +132,14 @@ int main(int argc, char **argv)
         if ((rc = cs3d_init_positions(&cfg, &mesh, n0, &rng, X.data(), Y.data(), Z.data())))
             return fail("initial placement", rc);
     }
+    if (youngs.empty()) {
+        // softer cells at set-up, src/GPUbounce.cu:616-692
+        youngs.assign(cfg.max_cells, 0.f);
+        if ((rc = cs3d_initial_stiffness(&cfg, n0, X.data(), Y.data(), Z.data(), &rng, youngs.data()))) {
+            if (rc == CS3D_E_CONFIG) printf("ERROR: Too many softer cells requested\n");
+            return fail("initial stiffness", rc);
+        }
+    }
     cs3d_topology topo;
     if ((rc = cs3d_topology_build(&mesh, X.data(), Y.data(), Z.data(), &topo))) return fail("mesh tables", rc);
     cs3d_ctx *ctx = nullptr;
@@ -135,17 +155,21 @@ int main(int argc, char **argv)
     FILE *ascii = nullptr;
     cs3d_traj *traj = nullptr;
     const int max_frames = (total_steps + 1) / interval;
+    const int varstiff = cfg.use_different_stiffnesses ? 1 : 0;
     if (cfg.binary_output) {
-        if ((rc = cs3d_traj_open(cfg.traj_file_name, cfg.max_cells, 0, max_frames, &traj)))
+        if ((rc = cs3d_traj_open(cfg.traj_file_name, cfg.max_cells, varstiff, max_frames, &traj)))
             return fail("trajectory file", rc);
-        if ((rc = cs3d_traj_write_frame(traj, 0, 1, n0, X.data(), Y.data(), Z.data(), nullptr)))
+        std::vector<int32_t> types;
+        cell_types(prm, n0, youngs.data(), types);
+        if ((rc = cs3d_traj_write_frame(traj, 0, 1, n0, X.data(), Y.data(), Z.data(), types.data())))
             return fail("trajectory frame", rc);
     } else {
         ascii = fopen(cfg.traj_file_name, "w");
         if (!ascii) return fail("trajectory file", CS3D_E_IO);
-        fprintf(ascii, "Header Start:\nMaximum number of cells:\n%d\nUsing variable stiffness:\nFalse\n"
-                       "Maximum number of frames:\n%d\nHeader End\n", cfg.max_cells, max_frames);
-        write_ascii_frame(ascii, 0, interval, n0, X.data(), Y.data(), Z.data());
+        fprintf(ascii, "Header Start:\nMaximum number of cells:\n%d\nUsing variable stiffness:\n%s\n"
+                       "Maximum number of frames:\n%d\nHeader End\n", cfg.max_cells, varstiff ? "True" : "False",
+                max_frames);
+        write_ascii_frame(ascii, 0, interval, n0, X.data(), Y.data(), Z.data(), prm, youngs.data());
     }
     int frame = 1;
     int step = 0;
@@ -153,7 +177,7 @@ int main(int argc, char **argv)
     // Frames are written by a second thread from one of two host buffers
     // while the GPU steps on (the reference writes them on the step loop's
     // thread, src/GPUbounce.cu:1430-1470).
-    std::vector<float> WB[2][3];
+    std::vector<float> WB[2][4];   // X, Y, Z, stiffness per cell
     for (auto &b : WB)
         for (auto &v : b) v.assign(cap_nodes, 0.f);
     std::thread writer;
@@ -187,14 +211,21 @@ int main(int argc, char **argv)
             ++frame;
             std::vector<float> *b = WB[buf];
             if ((rc = cs3d_get_state(ctx, 0, &n, b[0].data(), b[1].data(), b[2].data(), nullptr, nullptr, nullptr,
-                                     nullptr, nullptr))) {
+                                     nullptr, b[3].data()))) {
                 join_writer();
                 return fail("reading the state", rc);
             }
             if (join_writer()) return fail("trajectory frame", wrc);
-            writer = std::thread([&wrc, traj, ascii, b, step, frame, interval, nn = n]() {
-                if (traj) wrc = cs3d_traj_write_frame(traj, step, frame, nn, b[0].data(), b[1].data(), b[2].data(), nullptr);
-                else write_ascii_frame(ascii, step, interval, nn, b[0].data(), b[1].data(), b[2].data());
+            writer = std::thread([&wrc, &prm, traj, ascii, b, step, frame, interval, nn = n]() {
+                if (traj) {
+                    std::vector<int32_t> types;
+                    cell_types(prm, nn, b[3].data(), types);
+                    wrc = cs3d_traj_write_frame(traj, step, frame, nn, b[0].data(), b[1].data(), b[2].data(),
+                                                types.data());
+                } else {
+                    write_ascii_frame(ascii, step, interval, nn, b[0].data(), b[1].data(), b[2].data(), prm,
+                                      b[3].data());
+                }
             });
             buf ^= 1;
         }
@@ -208,20 +239,29 @@ int main(int argc, char **argv)
     cs3d_get_grid(ctx, 0, mm, divs);
     printf("Xdiv = %d, Ydiv = %d, Zdiv = %d\n", divs[0], divs[1], divs[2]);
 
-    // mitotic index file, src/GPUbounce.cu:1288-1302 and :1515-1547
+    // mitotic index file, src/GPUbounce.cu:1288-1302 and :1515-1547; with
+    // count_only_internal_cells the far daughters of a step are not counted
+    // (num_cells_far, :2538-2565)
     int nev = 0;
     cs3d_get_events(ctx, 0, nullptr, 0, &nev);
     std::vector<int32_t> ev(3 * (size_t)(nev > 0 ? nev : 1));
     cs3d_get_events(ctx, 0, ev.data(), nev, &nev);
+    int nfar = 0;
+    cs3d_get_far_counts(ctx, 0, nullptr, 0, &nfar);
+    std::vector<int32_t> far(2 * (size_t)(nfar > 0 ? nfar : 1));
+    cs3d_get_far_counts(ctx, 0, far.data(), nfar, &nfar);
     const int cci = cfg.cell_count_int;
     const int nbuckets = cfg.div_time_steps / cci + 1;
-    std::vector<int> per_step(cfg.div_time_steps + 2, 0);
+    std::vector<int> born(cfg.div_time_steps + 2, 0), per_step(cfg.div_time_steps + 2, 0);
     for (int k = 0; k < nev; ++k)
-        if (ev[3 * k] >= 1 && ev[3 * k] <= cfg.div_time_steps) per_step[ev[3 * k]] += 1;
+        if (ev[3 * k] >= 1 && ev[3 * k] <= cfg.div_time_steps) born[ev[3 * k]] += 1;
+    per_step = born;
+    for (int k = 0; k < nfar; ++k)
+        if (far[2 * k] >= 1 && far[2 * k] <= cfg.div_time_steps) per_step[far[2 * k]] -= far[2 * k + 1];
     std::vector<int> dividing(nbuckets, 0), totals(nbuckets, 0);
     int cells = n0;
     for (int s = 1; s <= cfg.div_time_steps; ++s) {
-        cells += per_step[s];
+        cells += born[s];
         if (s % cci == 0) {
             int nc = 0;
             for (int q = 0; q < cci; ++q) nc += per_step[s - cci + 1 + q];

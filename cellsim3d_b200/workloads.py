@@ -194,6 +194,15 @@ def random_centres(n, box, rng, min_dist=1.9, margin=1.05):
     return np.array(out, dtype=np.float32)
 
 
+def soft_params(p, soft_factor=0.8, **over):
+    """`p` with variable stiffness on: stiffness2 = fl(softStiffFactor x
+    Youngs_mod), as the reference computes it (src/GPUbounce.cu:2048)."""
+    q = dict(p, use_different_stiffnesses=1, soft_stiff_factor=soft_factor,
+             stiffness2=float(np.float32(soft_factor) * np.float32(p["youngs_mod"])))
+    q.update(over)
+    return q
+
+
 def config4(n_inst=256, master_seed=2024):
     """256 instances: N0 = round(exp(U[0, ln 512])) >= 1 cells, growth rate
     U[0.001, 0.004], division volume U[2.6, 3.2], box 30, seed i."""
@@ -265,7 +274,7 @@ def config5(n_inst=64, master_seed=2025):
     return inst
 
 
-def inp_json(p, max_cells, steps, traj_write_int, traj_file="traj.bin", seed=42, binary=True):
+def inp_json(p, max_cells, steps, traj_write_int, traj_file="traj.bin", seed=42, binary=True, non_div_steps=0):
     """The reference's inp.json (src/GPUbounce.cu:1938-2096 keys) for the
     hot-path parameters `p` (base_params layout); features off the path are
     switched off.  youngs_mod is the contact modulus, stiffness1 the bond
@@ -278,15 +287,17 @@ def inp_json(p, max_cells, steps, traj_write_int, traj_file="traj.bin", seed=42,
                  "viscotic_damping": p["viscotic_damping"], "internal_damping": p["internal_damping"],
                  "gamma_visc": p["gamma_visc"], "division_Vol": p["division_vol"], "random_z_offset?": 0,
                  "z_offset": 0.0, "div_time_steps": int(steps), "time_interval": p["time_interval"],
-                 "Restart": 0, "trajWriteInt": int(traj_write_int), "non_div_time_steps": 0,
+                 "Restart": 0, "trajWriteInt": int(traj_write_int), "non_div_time_steps": int(non_div_steps),
                  "trajFileName": traj_file, "binaryOutput": 1 if binary else 0,
                  "maxPressure": p["max_pressure"], "minPressure": p["min_pressure"],
                  "growth_rate": p["growth_rate"], "checkSphericity": bool(p["check_sphericity"]),
                  "constrainAngles": bool(p["constrain_angles"]), "doAdaptive_dt": False, "dt_max": 1e-4,
-                 "dt_tol": 1e-8, "phase_count": 2000000000, "write_cont_force": False,
+                 "dt_tol": 1e-8, "phase_count": int(p.get("phase_count", 2000000000)), "write_cont_force": False,
                  "forces_file": "forces.csv", "correct_com": False},
-        "counting": {"mit-index_file_name": "mit-index.dat", "count_only_internal_cells?": False,
-                     "radius_cutoff": 0.6, "overwrite_mit_ind_file?": True,
+        "counting": {"mit-index_file_name": "mit-index.dat",
+                     "count_only_internal_cells?": bool(p.get("count_internal_radius", 0.0) > 0),
+                     "radius_cutoff": float(p.get("count_internal_radius", 0.0)) or 0.6,
+                     "overwrite_mit_ind_file?": True,
                      "cell_count_int": max(1, min(1000, int(steps)))},
         "population": {"doPopModel": 0, "totalFood": 5000.0, "regular_consumption": 2.0,
                        "division_consumption": 10.0, "death_release_food": 10.0, "cellLifeTime": 20000,
@@ -294,9 +305,13 @@ def inp_json(p, max_cells, steps, traj_write_int, traj_file="traj.bin", seed=42,
         "walls": {"useWalls": 0, "perpAxis": "Z", "dAxis": 1.0, "wallLen": 10.0, "wallWidth": 10.0,
                   "threshDist": p["thresh_dist"]},
         "divParams": {"useDivPlaneBasis": 0, "divPlaneBasisX": 0.0, "divPlaneBasisY": 1.0, "divPlaneBasisZ": 0.0},
-        "stiffnessParams": {"useDifferentStiffnesses": False, "softStiffFactor": 1.0, "numberOfSofterCells": 0,
-                            "duringGrowth": False, "closenessToCenter": 0.0, "startAtPop": 0,
-                            "fractionOfSofterCells": 0.0, "chooseRandomCellIndices": False,
+        "stiffnessParams": {"useDifferentStiffnesses": bool(p.get("use_different_stiffnesses", 0)),
+                            "softStiffFactor": float(p.get("soft_stiff_factor", 1.0)),
+                            "numberOfSofterCells": int(p.get("number_of_softer_cells", 0)),
+                            "duringGrowth": not p.get("soften_after_growth", 0),
+                            "closenessToCenter": float(p.get("closeness_to_center", 0.0)), "startAtPop": 0,
+                            "fractionOfSofterCells": float(p.get("fraction_of_softer_cells", 0.0)),
+                            "chooseRandomCellIndices": bool(p.get("choose_random_cell_indices", 0)),
                             "daughtSameStiffness": bool(p["daught_same_stiffness"]), "recalc_r0": False},
         "boxParams": {"useRigidSimulationBox": bool(p["use_rigid_box"]), "usePBCs": False,
                       "boxLength": float(p["box_len"][0]), "box_len_x": float(p["box_len"][0]),

@@ -48,6 +48,8 @@ extern "C" {
 #define CS3D_ERRBIT_GRID_OVERFLOW  0x040u  /* reserved, never raised (the node hash cannot overflow) */
 #define CS3D_ERRBIT_PAIR_OVERFLOW  0x080u  /* pair-recording buffer full */
 #define CS3D_ERRBIT_HALO_OVERFLOW  0x100u  /* reserved, never raised */
+#define CS3D_ERRBIT_SOFT_CELLS     0x200u  /* more distinct softer cells requested than cell indices
+                                              exist (the reference loops forever, src/GPUbounce.cu:1364-1384) */
 
 #define CS3D_MAX_CAND     128   /* contact-candidate cells per cell */
 #define CS3D_MAX_ENTRIES   64   /* contact-candidate nodes per node */
@@ -90,6 +92,27 @@ typedef struct cs3d_params {
     int32_t rand_seed;          /* rand_params.rand_seed */
     int32_t correct_com;        /* core.correct_com: shift all nodes by minus the mean of the
                                    cells' centres of mass after every step, src/GPUbounce.cu:1430-1440 */
+    /* Variable stiffness (stiffnessParams.useDifferentStiffnesses): the initial softer cells
+     * come from cs3d_initial_stiffness (src/GPUbounce.cu:616-692); from step phase_count on a
+     * cell whose bond stiffness is not stiffness1 has pressure 0 and does not grow
+     * (src/PressureKernels.cu:4-40); with soften_after_growth, more cells get stiffness2 at the
+     * end of step div_time_steps + 2 (src/GPUbounce.cu:1340-1429): number_of_softer_cells of
+     * them (roundf(fraction * cells) when fraction > 0), either distinct RANMAR picks
+     * round(u * cells) from the division stream (choose_random_cell_indices) or the cells in
+     * index order whose centre lies within (1 - closeness_to_center) of the largest distance
+     * from the system's centre. */
+    int32_t use_different_stiffnesses;
+    float stiffness2;               /* stiffnessParams.softStiffFactor * Youngs_mod, src/GPUbounce.cu:2048 */
+    int32_t phase_count;            /* core.phase_count */
+    int32_t soften_after_growth;    /* !stiffnessParams.duringGrowth */
+    int32_t number_of_softer_cells; /* stiffnessParams.numberOfSofterCells */
+    float fraction_of_softer_cells; /* stiffnessParams.fractionOfSofterCells */
+    int32_t choose_random_cell_indices; /* stiffnessParams.chooseRandomCellIndices */
+    float closeness_to_center;      /* stiffnessParams.closenessToCenter */
+    /* Mitotic index of internal cells (counting.count_only_internal_cells?): > 0 enables the
+     * reference's num_cells_far test with this radius_cutoff, src/GPUbounce.cu:1288-1290,
+     * :2538-2565; its results are read with cs3d_get_far_counts. */
+    float count_internal_radius;
 } cs3d_params;
 
 /* ---- static mesh data ------------------------------------------------- */
@@ -193,6 +216,16 @@ int cs3d_rng_random_vector(cs3d_rng *rng, float n[3]);
  * (seed mod 31329, 100*seed mod 30082). */
 int cs3d_seed_map(int seed, int *ij, int *kl);
 
+/* Bond stiffness (Young's modulus) of the n_cells initial cells, src/GPUbounce.cu:616-692:
+ * stiffness1 for every cell; with useDifferentStiffnesses stiffness2 for the cells whose centre
+ * of mass lies within closenessToCenter of the largest distance from the system's centre (when
+ * 0 < closenessToCenter < 1), else for numberOfSofterCells cells (roundf(fraction * n) when
+ * 0 < fraction < 1): the first ones in a rigid box, RANMAR picks round(u * n) from rng
+ * otherwise.  X/Y/Z are 192-stride.  Returns CS3D_E_CONFIG when more softer cells than cells
+ * are requested (the reference exits with 12516). */
+int cs3d_initial_stiffness(const cs3d_config *cfg, int n_cells, const float *X, const float *Y,
+                           const float *Z, cs3d_rng *rng, float *youngs);
+
 /* Initial cell placement, src/GPUbounce.cu:1598-1774 (lattice or random
  * insertion with RANMAR draws).  X/Y/Z have capacity n_cells*192. */
 int cs3d_init_positions(const cs3d_config *cfg, const cs3d_mesh *mesh, int n_cells,
@@ -250,6 +283,11 @@ int cs3d_get_state(cs3d_ctx *ctx, int inst, int *n_cells, float *X, float *Y, fl
  * evaluation, 192-stride SoA. */
 int cs3d_get_forces(cs3d_ctx *ctx, int inst, float *FCX, float *FCY, float *FCZ,
                     float *FDX, float *FDY, float *FDZ);
+
+/* Division steps at which cells were discounted from the mitotic index as far from the
+ * system's centre (count_internal_radius > 0; src/GPUbounce.cu:1288-1290, :2538-2565):
+ * pairs (step, count) into out[2 * max_entries]; *n_entries = the number recorded. */
+int cs3d_get_far_counts(cs3d_ctx *ctx, int inst, int32_t *out, int max_entries, int *n_entries);
 
 /* Langevin random force of the last step (zeros when add_rands is off or
  * before the first step), 192-stride SoA.  No counterpart in the reference

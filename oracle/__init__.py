@@ -23,7 +23,10 @@ class OrcParams(C.Structure):
         "growth_rate", "thresh_dist")] + [("box", C.c_float * 3)] + [(n, C.c_int) for n in (
         "check_sphericity", "constrain_angles", "use_rigid_box", "daught_same_stiffness",
         "div_time_steps", "pad_", "add_rands")] + [("rand_scale", C.c_float), ("rand_seed", C.c_uint),
-                                                   ("correct_com", C.c_int)]
+                                                   ("correct_com", C.c_int)] + [
+        ("diff_stiff", C.c_int), ("stiffness2", C.c_float), ("phase_count", C.c_int),
+        ("soften_after_growth", C.c_int), ("soft_n", C.c_int), ("soft_frac", C.c_float), ("soft_rand", C.c_int),
+        ("closeness", C.c_float), ("far_r", C.c_float)]
 
 
 class OrcTopo(C.Structure):
@@ -78,6 +81,9 @@ def lib():
         L.orc_random_vector.argtypes = [C.POINTER(OrcRanmar), C.POINTER(C.c_float)]
         L.orc_seed_map.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.orc_random_force.argtypes = [C.POINTER(OrcParams), C.c_int, C.c_int, C.POINTER(C.c_float)]
+        L.orc_initial_stiffness.restype = C.c_int
+        L.orc_initial_stiffness.argtypes = [C.POINTER(OrcParams), C.c_int, C.c_int] + [C.POINTER(C.c_float)] * 3 + [
+            C.POINTER(OrcRanmar), C.POINTER(C.c_float)]
         L.orc_r0_theta0.argtypes = [C.POINTER(C.c_float)] * 3 + [C.POINTER(C.c_int),
                                                                  C.POINTER(C.c_float), C.POINTER(C.c_float)]
         L.orc_divide_cell.restype = C.c_int
@@ -164,7 +170,29 @@ def make_params(p):
     o.rand_scale = float(p.get("rand_scale_factor", 0.0))
     o.rand_seed = int(p.get("rand_seed", 0)) & 0xffffffff
     o.correct_com = int(p.get("correct_com", 0))
+    o.diff_stiff = int(p.get("use_different_stiffnesses", 0))
+    o.stiffness2 = float(p.get("stiffness2", 0.0))
+    o.phase_count = int(p.get("phase_count", 0))
+    o.soften_after_growth = int(p.get("soften_after_growth", 0))
+    o.soft_n = int(p.get("number_of_softer_cells", 0))
+    o.soft_frac = float(p.get("fraction_of_softer_cells", 0.0))
+    o.soft_rand = int(p.get("choose_random_cell_indices", 0))
+    o.closeness = float(p.get("closeness_to_center", 0.0))
+    o.far_r = float(p.get("count_internal_radius", 0.0))
     return o
+
+
+def initial_stiffness(params, rigid, X, Y, Z, n, rng=None):
+    """The oracle's initial bond stiffness of n cells (None when more softer
+    cells than cells are asked for)."""
+    P = make_params(params) if isinstance(params, dict) else params
+    E = np.zeros(max(n, 1), dtype=np.float32)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    Y = np.ascontiguousarray(Y, dtype=np.float32)
+    Z = np.ascontiguousarray(Z, dtype=np.float32)
+    r = rng if rng is not None else OrcRanmar()
+    rc = lib().orc_initial_stiffness(C.byref(P), int(rigid), int(n), _fp(X), _fp(Y), _fp(Z), C.byref(r), _fp(E))
+    return None if rc else E[:n]
 
 
 def random_force(params, node, step):
@@ -216,6 +244,9 @@ class System:
         self._div = np.ctypeslib.as_array(L.orc_ptr_i(self.h, 2), shape=(3,))
         self._nev = np.ctypeslib.as_array(L.orc_ptr_i(self.h, 3), shape=(1,))
         self._ev = L.orc_ptr_i(self.h, 4)
+        self._nfar = np.ctypeslib.as_array(L.orc_ptr_i(self.h, 9), shape=(1,))
+        self._far = L.orc_ptr_i(self.h, 10)
+        self.syscm = fv(14, 3)
 
     def close(self):
         if self.h:
@@ -292,6 +323,11 @@ class System:
     def events(self):
         ne = int(self._nev[0])
         return np.ctypeslib.as_array(self._ev, shape=(3 * max(ne, 1),))[:3 * ne].reshape(ne, 3).copy()
+
+    def far_counts(self):
+        """(step, cells) of num_cells_far at the division steps where it left cells out."""
+        nf = int(self._nfar[0])
+        return np.ctypeslib.as_array(self._far, shape=(2 * max(nf, 1),))[:2 * nf].reshape(nf, 2).copy()
 
     def pairs(self, kind):
         cnt = lib().orc_pairs(self.h, kind, None, 0)

@@ -40,6 +40,7 @@
 #define ORC_ERR_LOCALNN        0x8u   /* a node would accept > 10 cells */
 #define ORC_ERR_MEMSET_BUG     0x10u  /* > 262144 bins: reference leaves stale counts */
 #define ORC_ERR_NONFINITE_VOL  0x20u
+#define ORC_ERR_SOFT_CELLS     0x40u  /* more softer cells than indices: the reference loops forever */
 
 typedef struct {
     float mass;               /* core.particle_mass */
@@ -68,6 +69,15 @@ typedef struct {
     float rand_scale;         /* rand_params.rand_scale_factor */
     unsigned rand_seed;       /* Philox key (see orc_random_force) */
     int correct_com;          /* core.correct_com */
+    int diff_stiff;           /* stiffnessParams.useDifferentStiffnesses */
+    float stiffness2;         /* softStiffFactor * Youngs_mod */
+    int phase_count;          /* core.phase_count */
+    int soften_after_growth;  /* !stiffnessParams.duringGrowth */
+    int soft_n;               /* numberOfSofterCells */
+    float soft_frac;          /* fractionOfSofterCells */
+    int soft_rand;            /* chooseRandomCellIndices */
+    float closeness;          /* closenessToCenter */
+    float far_r;              /* radius_cutoff when count_only_internal_cells (else 0) */
 } orc_params;
 
 typedef struct {
@@ -106,6 +116,9 @@ typedef struct orc_sys {
     int step;
     int nev;
     int *ev;                   /* (step, parent, daughter) */
+    float syscm[3];            /* the reference's sysCM globals, src/GPUbounce.cu:240 */
+    int nfar;
+    int *far;                  /* (step, cells not counted) of num_cells_far */
     unsigned err;
     /* pairs used by the last force evaluation (recording mode) */
     int record;
@@ -239,6 +252,8 @@ orc_sys *orc_create(int cap, const orc_params *P, const orc_topo *T)
     s->div_flag = calloc(cap, 1);
     s->aabb = calloc(6 * (size_t)cap, 4);
     s->ev = calloc(3 * ORC_MAX_EVENTS, 4);
+    s->far = calloc(2 * ORC_MAX_EVENTS, 4);
+    s->syscm[0] = s->syscm[1] = s->syscm[2] = 1.0f;
     return s;
 }
 
@@ -248,7 +263,7 @@ void orc_destroy(orc_sys *s)
     free(s->X); free(s->Y); free(s->Z); free(s->VX); free(s->VY); free(s->VZ);
     free(s->FC); free(s->FD); free(s->FR); free(s->CM); free(s->press); free(s->E);
     free(s->vol); free(s->area); free(s->div_flag); free(s->aabb);
-    free(s->bin_start); free(s->bin_cells); free(s->ev);
+    free(s->bin_start); free(s->bin_cells); free(s->ev); free(s->far);
     free(s->rec[0]); free(s->rec[1]);
     free(s);
 }
@@ -261,7 +276,7 @@ float *orc_ptr_f(orc_sys *s, int which)
     case 3: return s->VX; case 4: return s->VY; case 5: return s->VZ;
     case 6: return s->CM; case 7: return s->press; case 8: return s->E;
     case 9: return s->vol; case 10: return s->area; case 11: return s->aabb;
-    case 12: return s->minmax; case 13: return s->FR;
+    case 12: return s->minmax; case 13: return s->FR; case 14: return s->syscm;
     default: return NULL;
     }
 }
@@ -273,6 +288,7 @@ int *orc_ptr_i(orc_sys *s, int which)
     case 3: return &s->nev; case 4: return s->ev;
     case 5: return &s->max_bin_count; case 6: return &s->max_local_nn;
     case 7: return &s->ydiv; case 8: return &s->zdiv;
+    case 9: return &s->nfar; case 10: return s->far;
     default: return NULL;
     }
 }
@@ -878,11 +894,131 @@ static void correct_com(orc_sys *s)
     sx = sx / (float)n;
     sy = sy / (float)n;
     sz = sz / (float)n;
+    s->syscm[0] = sx; s->syscm[1] = sy; s->syscm[2] = sz;
     for (int g = 0; g < n * 192; ++g) {
         s->X[g] -= sx;
         s->Y[g] -= sy;
         s->Z[g] -= sz;
     }
+}
+
+/* calc_sys_CM, src/GPUbounce.cu:2504-2520, over the first n cells. */
+static void calc_sys_cm(orc_sys *s, int n)
+{
+    float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+    for (int c = 0; c < n; ++c) {
+        sx += s->CM[c];
+        sy += s->CM[s->cap + c];
+        sz += s->CM[2 * s->cap + c];
+    }
+    s->syscm[0] = sx / (float)n;
+    s->syscm[1] = sy / (float)n;
+    s->syscm[2] = sz / (float)n;
+}
+
+static float cm_dist2(const orc_sys *s, int c)
+{
+    float dx = s->CM[c] - s->syscm[0], dy = s->CM[s->cap + c] - s->syscm[1], dz = s->CM[2 * s->cap + c] - s->syscm[2];
+    return dx * dx + dy * dy + dz * dz;
+}
+
+/* getRmax2, src/GPUbounce.cu:2523-2536. */
+static float get_rmax2(const orc_sys *s, int n)
+{
+    float r2 = 0.0f;
+    for (int c = 0; c < n; ++c) {
+        float v = cm_dist2(s, c);
+        r2 = r2 < v ? v : r2;
+    }
+    return r2;
+}
+
+/* num_cells_far, src/GPUbounce.cu:2538-2565 (called at :1288-1290 after the
+ * divisions of a step). */
+static int num_cells_far(orc_sys *s, int ndiv)
+{
+    const int n = s->n;
+    if (ndiv == 0 || n < 50) return 0;
+    calc_sys_cm(s, n);
+    float thr = s->P.far_r * s->P.far_r * get_rmax2(s, n);
+    int far = 0;
+    for (int c = n - ndiv; c < n; ++c)
+        if (cm_dist2(s, c) > thr) ++far;
+    return far;
+}
+
+/* Cells softened when growth ends, src/GPUbounce.cu:1340-1429. */
+static void soften_cells(orc_sys *s)
+{
+    const orc_params *P = &s->P;
+    const int n = s->n;
+    int count = P->soft_n;
+    if (P->soft_frac > 0) count = (int)roundf(P->soft_frac * (float)n);
+    if (P->soft_rand) {
+        if (count > n + 1) { s->err |= ORC_ERR_SOFT_CELLS; return; }
+        int *chosen = (int *)malloc(sizeof(int) * (count > 0 ? count : 1));
+        int got = 0;
+        while (got < count) {
+            float r;
+            orc_ranmar_draw(&s->rng, &r, 1);
+            int ind = (int)roundf(r * (float)n);
+            int seen = 0;
+            for (int q = 0; q < got; ++q)
+                if (chosen[q] == ind) { seen = 1; break; }
+            if (!seen) chosen[got++] = ind;
+        }
+        for (int q = 0; q < got; ++q)
+            if (chosen[q] < n) s->E[chosen[q]] = P->stiffness2;
+        free(chosen);
+        return;
+    }
+    float rmax2 = get_rmax2(s, n);   /* before calc_sys_CM: the previous centre */
+    calc_sys_cm(s, n);
+    float f = 1.0f - P->closeness;
+    for (int c = 0, got = 0; got < count && c < n; ++c)
+        if (cm_dist2(s, c) <= f * f * rmax2) { s->E[c] = P->stiffness2; ++got; }
+}
+
+/* Initial bond stiffness of the cells, src/GPUbounce.cu:616-692 (centres of
+ * mass as everywhere in this oracle, FP64 sums rounded to float). */
+int orc_initial_stiffness(const orc_params *P, int rigid, int n, const float *X, const float *Y, const float *Z,
+                          orc_ranmar *rng, float *E)
+{
+    for (int c = 0; c < n; ++c) E[c] = P->stiffness1;
+    if (!P->diff_stiff || n == 0) return 0;
+    if (P->closeness > 0.f && P->closeness < 1.f) {
+        float *m = (float *)malloc(sizeof(float) * 4 * n);
+        float sc[3] = {0.f, 0.f, 0.f};
+        for (int c = 0; c < n; ++c) {
+            m[4 * c] = (float)(sum192(X + c * 192) / 180.0);
+            m[4 * c + 1] = (float)(sum192(Y + c * 192) / 180.0);
+            m[4 * c + 2] = (float)(sum192(Z + c * 192) / 180.0);
+            for (int q = 0; q < 3; ++q) sc[q] += m[4 * c + q];
+        }
+        float inv = 1.0f / (float)n;   /* float3 / float = (1/a) * b */
+        for (int q = 0; q < 3; ++q) sc[q] = inv * sc[q];
+        float rmax = 0.f;
+        for (int c = 0; c < n; ++c) {
+            float dx = m[4 * c] - sc[0], dy = m[4 * c + 1] - sc[1], dz = m[4 * c + 2] - sc[2];
+            m[4 * c + 3] = sqrtf(dx * dx + dy * dy + dz * dz);
+            if (m[4 * c + 3] > rmax) rmax = m[4 * c + 3];
+        }
+        for (int c = 0; c < n; ++c)
+            if (m[4 * c + 3] / rmax <= P->closeness) E[c] = P->stiffness2;
+        free(m);
+        return 0;
+    }
+    int count = P->soft_n;
+    if (P->soft_frac > 0.f && P->soft_frac < 1.f) count = (int)roundf(P->soft_frac * (float)n);
+    if (count > n) return -1;
+    for (int q = 0; q < count; ++q) {
+        if (rigid) { E[q] = P->stiffness2; continue; }
+        float r;
+        orc_ranmar_draw(rng, &r, 1);
+        int ind = (int)roundf(r * (float)n);
+        if (ind < n) E[ind] = P->stiffness2;
+    }
+    return 0;
 }
 
 void orc_init(orc_sys *s)
@@ -929,8 +1065,7 @@ void orc_random_force(const orc_params *P, int node, int step, float out[3])
     out[2] = P->rand_scale * (rb * cosf(tb));
 }
 
-/* One timestep, src/GPUbounce.cu:1055-1338 (population model, variable
- * stiffness and CoM correction disabled).                                    */
+/* One timestep, src/GPUbounce.cu:1055-1440 (population model disabled).    */
 void orc_step(orc_sys *s)
 {
     const orc_params *P = &s->P;
@@ -959,9 +1094,14 @@ void orc_step(orc_sys *s)
                 X[q][g] = fmaf(V[q][g], dtf, X[q][g]);
             }
         }
-    /* PressureUpdate, src/PressureKernels.cu:35-39 */
-    for (int c = 0; c < N; ++c)
-        if (s->press[c] < P->max_p) s->press[c] += P->growth_rate;
+    /* PressureUpdate, src/PressureKernels.cu:4-40 */
+    for (int c = 0; c < N; ++c) {
+        if (P->diff_stiff && step >= P->phase_count && s->E[c] != P->stiffness1) {
+            if (s->press[c] != 0.f) s->press[c] = 0.f;
+        } else if (s->press[c] < P->max_p) {
+            s->press[c] += P->growth_rate;
+        }
+    }
     record_pairs(s);
     orc_con_force(s);
     orc_dis_force(s);
@@ -993,15 +1133,26 @@ void orc_step(orc_sys *s)
     orc_center_of_mass(s);
     if (step <= P->div_time_steps && P->growth_rate > 0) {
         orc_volumes(s);
+        int ndiv = 0;
         for (int c = 0; c < N; ++c) {
             if (!s->div_flag[c]) continue;
             s->div_flag[c] = 0;
             float nrm[3];
             orc_random_vector(&s->rng, nrm);
             if (orc_divide_cell(s, c, nrm) < 0) break;
+            ++ndiv;
+        }
+        if (P->far_r > 0) {
+            int far = num_cells_far(s, ndiv);
+            if (far && s->nfar < ORC_MAX_EVENTS) {
+                s->far[2 * s->nfar] = step;
+                s->far[2 * s->nfar + 1] = far;
+                s->nfar++;
+            }
         }
     }
     orc_build_grid(s);
+    if (P->diff_stiff && P->soften_after_growth && step == P->div_time_steps + 2) soften_cells(s);
     if (P->correct_com) correct_com(s);
 }
 

@@ -31,10 +31,10 @@ def make_pair(p, st, mesh, capacity, record_pairs=True, pair_capacity=1 << 22):
         sim.set_option(cs.OPT_PAIR_CAPACITY, pair_capacity)
         sim.set_option(cs.OPT_RECORD_PAIRS, 1)
     sim.load_state(st["X"], st["Y"], st["Z"], st.get("VX"), st.get("VY"), st.get("VZ"),
-                   st.get("pressure"), None, n_cells=st["n"])
+                   st.get("pressure"), st.get("youngs"), n_cells=st["n"])
     orc = oracle.System(capacity, p, otopo)
     orc.load(st["X"], st["Y"], st["Z"], st.get("VX"), st.get("VY"), st.get("VZ"),
-             pressure=st.get("pressure"), n=st["n"])
+             pressure=st.get("pressure"), youngs=st.get("youngs"), n=st["n"])
     orc.seed(p["rng_ij"], p["rng_kl"])
     orc.set_record(record_pairs)
     orc.init()
@@ -145,6 +145,9 @@ def single_step_check(sim, tag="", tol=TOL, check_pairs=True):
     k = n * 192
     for a, b in (("X", O.X), ("Y", O.Y), ("Z", O.Z)):
         assert np.array_equal(after[a][:k].view(np.uint32), b[:k].view(np.uint32)), (tag, "positions", a)
+    # per-cell pressure and bond stiffness: exact
+    assert np.array_equal(after["pressure"][:n].view(np.uint32), O.press[:n].view(np.uint32)), (tag, "pressure")
+    assert np.array_equal(after["youngs"][:n].view(np.uint32), O.E[:n].view(np.uint32)), (tag, "stiffness")
     cm_o = O.CM[:, :n].T
     ex = [c for c in range(n)]
     # conservative force (identical inputs)

@@ -62,3 +62,74 @@ def test_cli_trajectory_matches_library(tmp_path, mesh):
             assert np.array_equal(f[key].reshape(-1).view(np.uint32), s[key][: m * 192].view(np.uint32)), (f["step"], key)
     print("cs3d driver: %d frames, %d cells at step %d" % (len(frames), frames[-1]["X"].shape[0], steps))
     sim.close()
+
+
+@pytest.mark.gpu
+def test_cli_variable_stiffness_and_internal_count(tmp_path, mesh):
+    """The driver with variable stiffness and the internal-cells mitotic
+    count: 56 clustered cells divide at step 1 (their daughters all lie far
+    from the system centre), the central cells start soft, RANMAR picks are
+    softened at the end of step 202; the binary frames carry the stiffness class of
+    every cell, and the mitotic-index file leaves the far daughters out."""
+    box = 60.0
+    c = W.rsa_centres(56, 14.0, np.random.default_rng(11)) + np.float32(23.0)
+    p = W.soft_params(W.base_params(box_len=(box, box, box), count_internal_radius=0.6), phase_count=100,
+                      soften_after_growth=1, number_of_softer_cells=10, closeness_to_center=0.5,
+                      choose_random_cell_indices=1)
+    steps, non_div, every = 200, 100, 100
+    st = W.state(c)
+    n = st["n"]
+    write_mesh_files(str(tmp_path), mesh)
+    with open(tmp_path / "inp.json", "w") as f:
+        json.dump(W.inp_json(p, 256, steps, every, "traj.bin", seed=42, non_div_steps=non_div), f, indent=1)
+    cfg = cs.read_json_params(str(tmp_path / "inp.json"))
+    prm = cs.config_to_params(cfg)
+    E0 = cs.initial_stiffness(cfg, st["X"], st["Y"], st["Z"], n)
+    assert 0 < int((E0 != np.float32(prm.stiffness1)).sum()) < n
+    init = dict(st, pressure=np.full(n, p["min_pressure"], np.float32), youngs=E0)
+    W.write_init_file(str(tmp_path / "init.bin"), init)
+    env = dict(os.environ, CS3D_INIT_FILE=str(tmp_path / "init.bin"))
+    r = subprocess.run([CLI, str(n), "inp.json", "0"], cwd=tmp_path, env=env, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    hdr, frames = traj.read_traj(str(tmp_path / "traj.bin"))
+    assert hdr["variable_stiffness"] == 1
+    assert [f["step"] for f in frames] == [0, 100, 200, 300]
+
+    topo = cs.build_topology(cs.read_fullerene_nn(str(tmp_path)), st["X"][:192], st["Y"][:192], st["Z"][:192])
+    sim = cs.Simulation(prm, topo, 256)
+    sim.load_state(st["X"], st["Y"], st["Z"], youngs=E0, n_cells=n)
+    soft_counts = []
+    for f in frames:
+        if f["step"]:
+            sim.step(every)
+        s = sim.state()
+        m = s["n"]
+        assert f["X"].shape[0] == m
+        assert np.array_equal(f["X"].reshape(-1).view(np.uint32), s["X"][: m * 192].view(np.uint32)), f["step"]
+        types = (s["youngs"][:m] != np.float32(prm.stiffness1)).astype(np.int32)
+        assert np.array_equal(f["types"], types), f["step"]
+        soft_counts.append(int(types.sum()))
+    assert soft_counts[-1] > soft_counts[-2]          # softened at the end of step 202
+
+    # mitotic index of internal cells (src/GPUbounce.cu:1288-1302, :1515-1547)
+    ev, far = sim.events(), sim.far_counts()
+    assert len(far) and far[0].tolist() == [1, 56]
+    born = np.zeros(steps + 1, int)
+    for e in ev:
+        born[e[0]] += 1
+    counted = born.copy()
+    for s_, k in far:
+        counted[s_] -= k
+    cci = max(1, min(1000, steps))
+    buckets = [0.0] * (steps // cci + 1)
+    cells = n
+    for s_ in range(1, steps + 1):
+        cells += born[s_]
+        if s_ % cci == 0:
+            nc = counted[s_ - cci + 1: s_ + 1].sum()
+            tot = cells - nc
+            buckets[(s_ - 1) // cci] = float(np.float32(nc) / np.float32(tot)) if nc and tot else 0.0
+    got = [float(v) for v in open(tmp_path / "mit-index.dat").read().split()]
+    assert got == pytest.approx(buckets, abs=1e-6)
+    sim.close()
