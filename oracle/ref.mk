@@ -27,6 +27,6 @@ $(OUT)/ref_harness.o: $(HERE)ref_harness.cu $(HERE)../include/cs3d.h | $(OUT)
 	$(NVCC) $(FLAGS) -c $< -o $@
 
 $(OUT)/cs3d_ref: $(OBJS) $(OUT)/ref_harness.o
-	$(NVCC) $(ARCH) -rdc=true -o $@ $^
+	$(NVCC) $(ARCH) -rdc=true -o $@ $^ -lcurand
 
 .PHONY: all

@@ -15,8 +15,10 @@ File formats (little-endian):
   output  "CS3DREFO", int32 status, steps_done, n, n_events, max_bin, max_nn,
           float32 total_ms, guard_ms (timed region), int32 events [n_events*3] (step, parent,
           daughter), float32 X, Y, Z, VX, VY, VZ, FCX..FCZ, FDX..FDZ [n*192],
-          pressure [n], CM x, y, z [n], int32 n_init, n_first, float32 initial
-          FCX..FCZ, FDX..FDZ [n_init*192] when requested.
+          pressure [n], stiffness [n], CM x, y, z [n], int32 n_init, n_first, float32 initial
+          FCX..FCZ, FDX..FDZ [n_init*192] when requested, float32 FRX..FRZ [n*192]
+          (random force of the last step), int32 n_far, (step, cells) [n_far] of
+          the internal-cells count.
 """
 import os
 import struct
@@ -33,7 +35,8 @@ _DEPS = [os.path.join(HERE, "ref_harness.cu"), os.path.join(HERE, "..", "include
 
 STATUS = {0: "ok", 1: "a grid bin held more than 32 cells (clamped)",
           2: "more than 10 cells passed the box filter for a node (bin cut)",
-          3: "NaN position", 4: "division past capacity", 5: "grid larger than the reference's buffers"}
+          3: "NaN position", 4: "division past capacity", 5: "grid larger than the reference's buffers",
+          6: "more distinct softer cells requested than exist"}
 
 
 def available():
@@ -110,6 +113,8 @@ def run(params, topo, state, capacity, steps, dump_init=False, warmup=0, timeout
         off += 4 * kf
     out["pressure"] = np.frombuffer(buf, np.float32, nf, off).copy()
     off += 4 * nf
+    out["youngs"] = np.frombuffer(buf, np.float32, nf, off).copy()
+    off += 4 * nf
     out["cm"] = np.frombuffer(buf, np.float32, 3 * nf, off).reshape(3, nf).T.copy()
     off += 12 * nf
     n_init, n_first = struct.unpack_from("<2i", buf, off)
@@ -117,4 +122,11 @@ def run(params, topo, state, capacity, steps, dump_init=False, warmup=0, timeout
     if n_first:
         first = np.frombuffer(buf, np.float32, n_first, off).reshape(6, n_init * 192)
         out["init"] = {key: first[q].copy() for q, key in enumerate(("FCX", "FCY", "FCZ", "FDX", "FDY", "FDZ"))}
+        off += 4 * n_first
+    for key in ("FRX", "FRY", "FRZ"):
+        out[key] = np.frombuffer(buf, np.float32, kf, off).copy()
+        off += 4 * kf
+    (nfar,) = struct.unpack_from("<i", buf, off)
+    off += 4
+    out["far"] = np.frombuffer(buf, np.int32, 2 * nfar, off).reshape(nfar, 2).copy()
     return out

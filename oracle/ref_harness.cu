@@ -27,7 +27,17 @@
 //     is against MAX_NN = 1024) pass the bounding-box filter for a node, the
 //     bin's count is cut so that no node sees more than 10.
 // Clamped or cut counts change the reference's contacts, so such a run is
-// flagged (status 1 or 2) and is valid for timing only.  The guard kernels
+// flagged (status 1 or 2) and is valid for timing only.
+//
+// Also driven, as the reference's main does: the CoM correction
+// (src/GPUbounce.cu:783-805 at set-up, :1430-1440 every step, with the host's
+// calc_sys_CM), the variable-stiffness schedule (PressureUpdate and volumes
+// with their stiffness arguments, the growth-end softening of :1340-1429 on
+// the host with the reference's ranmar), the internal-cells count of the
+// mitotic index (num_cells_far, :2538-2565) and the Langevin force (curand
+// MT19937 seeds, DeviceRandInit and CalculateRanForce, :697-730, :1133-1137).
+// A growth-end random softening that asks for more distinct cells than
+// exist, where the reference loops forever, stops the run (status 6).  The guard kernels
 // are asynchronous (no host round trip is added to the step) and their
 // device time, measured with events, is excluded from the timing.
 //
@@ -35,8 +45,12 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <cmath>
+#include <ctime>
 #include <vector>
+
+#include <curand.h>
 
 #include "postscript.h"
 #include "marsaglia.h"
@@ -61,6 +75,7 @@ enum {
     ST_NAN = 3,            // NaN position seen
     ST_CAPACITY = 4,       // division past capacity (stopped)
     ST_GRID = 5,           // grid larger than the reference's buffers (stopped)
+    ST_SOFT = 6,           // more distinct softer cells requested than exist (stopped)
 };
 
 // ---------------------------------------------------------------------------
@@ -187,7 +202,10 @@ static bool read_input(const char *path, Input &in)
           std::isfinite(p.stiffness1) && std::isfinite(p.max_pressure) && std::isfinite(p.min_pressure) &&
           std::isfinite(p.growth_rate) && std::isfinite(p.division_vol)))
         return fail_input("parameters out of range");
-    if (p.add_rands || p.correct_com) return fail_input("random forces / CoM correction are not driven by this harness");
+    if (!(std::isfinite(p.rand_scale_factor) && std::isfinite(p.stiffness2) && p.number_of_softer_cells >= 0 &&
+          std::isfinite(p.fraction_of_softer_cells) && std::isfinite(p.closeness_to_center) &&
+          std::isfinite(p.count_internal_radius)))
+        return fail_input("schedule parameters out of range");
     for (int q = 0; q < 3; ++q)
         for (int i = 0; i < 180; ++i) {
             const int nb = in.t.nn[q * 192 + i];
@@ -252,6 +270,53 @@ int main(int argc, char **argv)
     float *d_time = dev<float>(1), *d_boxMin = dev<float>(3), *d_ran2 = dev<float>(3);
     int *d_reset = dev<int>(2 * (size_t)cap + 2);
     int *d_gmax = dev<int>(4);
+    curandState *d_rng = nullptr;
+    if (p.add_rands) {
+        // src/GPUbounce.cu:697-730
+        d_rng = dev<curandState>(NS);
+        // MT19937 output lengths are whole multiples of 2048 values; the
+        // first NS seed the node states
+        const size_t NSR = (NS + 2047) / 2048 * 2048;
+        unsigned *d_seeds = dev<unsigned>(NSR);
+        curandGenerator_t gen;
+        if (curandCreateGenerator(&gen, CURAND_RNG_PSEUDO_MT19937) != CURAND_STATUS_SUCCESS ||
+            curandSetPseudoRandomGeneratorSeed(gen, p.rand_seed > 0 ? (unsigned long long)p.rand_seed
+                                                                    : (unsigned long long)time(nullptr)) !=
+                CURAND_STATUS_SUCCESS ||
+            curandGenerate(gen, d_seeds, NSR) != CURAND_STATUS_SUCCESS) {
+            fprintf(stderr, "cs3d_ref: curand set-up failed\n");
+            return 2;
+        }
+        DeviceRandInit<<<(unsigned)(NS / 256 + 1), 256>>>(d_rng, d_seeds, NS);
+        CK(cudaGetLastError());
+        CK(cudaDeviceSynchronize());
+        curandDestroyGenerator(gen);
+        CK(cudaFree(d_seeds));
+    }
+    // the reference's host system centre (globals, src/GPUbounce.cu:240) and
+    // its calc_sys_CM / getRmax2 (:2504-2536) on a host copy of the centres
+    float sysCM[3] = {1.0f, 1.0f, 1.0f};
+    std::vector<float> hcx(cap), hcy(cap), hcz(cap);
+    auto fetch_cm = [&](int n) {
+        CK(cudaMemcpy(hcx.data(), d_CMx, n * sizeof(float), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(hcy.data(), d_CMy, n * sizeof(float), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(hcz.data(), d_CMz, n * sizeof(float), cudaMemcpyDeviceToHost));
+    };
+    auto calc_sys_cm = [&](int n) {
+        float sx = 0, sy = 0, sz = 0;
+        for (int c = 0; c < n; ++c) { sx += hcx[c]; sy += hcy[c]; sz += hcz[c]; }
+        sysCM[0] = sx / n; sysCM[1] = sy / n; sysCM[2] = sz / n;
+    };
+    auto dist2 = [&](int c) {
+        float dx = hcx[c] - sysCM[0], dy = hcy[c] - sysCM[1], dz = hcz[c] - sysCM[2];
+        return dx * dx + dy * dy + dz * dz;
+    };
+    auto get_rmax2 = [&](int n) {
+        float r2 = 0;
+        for (int c = 0; c < n; ++c) r2 = std::max(r2, dist2(c));
+        return r2;
+    };
+    std::vector<int> far_log;
 
     // initial state and tables
     const size_t k0 = (size_t)192 * in.n;
@@ -349,6 +414,17 @@ int main(int argc, char **argv)
     // initialisation, src/GPUbounce.cu:739-763 and :978-1004
     CenterOfMass<<<N, 256>>>(N, d_X, d_Y, d_Z, d_CMx, d_CMy, d_CMz);
     status = grid();
+    if (p.correct_com) {
+        // src/GPUbounce.cu:783-805
+        CenterOfMass<<<N, 256>>>(N, d_X, d_Y, d_Z, d_CMx, d_CMy, d_CMz);
+        fetch_cm(N);
+        calc_sys_cm(N);
+        const long np = (long)N * 192;
+        CorrectCoMMotion<<<(unsigned)(np / 1024 + 1), 1024>>>(d_X, d_Y, d_Z, sysCM[0], sysCM[1], sysCM[2], np);
+        CorrectCoMMotion<<<(unsigned)(np / 1024 + 1), 1024>>>(d_XP, d_YP, d_ZP, sysCM[0], sysCM[1], sysCM[2], np);
+        CorrectCoMMotion<<<(unsigned)(np / 1024 + 1), 1024>>>(d_XM, d_YM, d_ZM, sysCM[0], sysCM[1], sysCM[2], np);
+        CK(cudaGetLastError());
+    }
     const int n_init = N;
     std::vector<float> first_forces;
     if (status == ST_OK) {
@@ -382,20 +458,24 @@ int main(int argc, char **argv)
     for (int step = 1; step <= in.steps && status == ST_OK; ++step) {
         const long numNodes = (long)N * 192;
         Integrate<<<N, threadsperblock>>>(d_XP, d_YP, d_ZP, d_X, d_Y, d_Z, d_XM, d_YM, d_ZM, d_vx, d_vy, d_vz, d_time,
-                                          p.particle_mass, fCon, fDis, fRan, N, false, nullptr, 0.0f);
+                                          p.particle_mass, fCon, fDis, fRan, N, p.add_rands != 0, d_rng,
+                                          p.rand_scale_factor);
         ForwardTime<<<N, threadsperblock>>>(d_XP, d_YP, d_ZP, d_X, d_Y, d_Z, d_XM, d_YM, d_ZM, N);
-        PressureUpdate<<<N / 1024 + 1, 1024>>>(d_press, p.min_pressure, p.max_pressure, rGrowth, N, false,
-                                               p.stiffness1, d_E, step, 0x7fffffff);
+        PressureUpdate<<<N / 1024 + 1, 1024>>>(d_press, p.min_pressure, p.max_pressure, rGrowth, N,
+                                               p.use_different_stiffnesses != 0, p.stiffness1, d_E, step,
+                                               p.phase_count);
         guard_forces();
         con_force();
         dis_force();
+        if (p.add_rands) CalculateRanForce<<<N, threadsperblock>>>(N, d_rng, p.rand_scale_factor, fRan);
         VelocityUpdateA<<<N, threadsperblock>>>(d_vx, d_vy, d_vz, fCon, fRan, delta_t, numNodes, p.particle_mass);
         VelocityUpdateB<<<N, threadsperblock>>>(d_vx, d_vy, d_vz, fDis, delta_t, numNodes, p.particle_mass);
         dis_force();
         CenterOfMass<<<N, 256>>>(N, d_X, d_Y, d_Z, d_CMx, d_CMy, d_CMz);
         if (step <= Time_steps && rGrowth > 0) {
             volumes<<<N, 192>>>(N, d_faces, d_X, d_Y, d_Z, d_CMx, d_CMy, d_CMz, d_vol, d_cell_div, p.division_vol,
-                                p.check_sphericity != 0, d_area, 0x7fffffff, step, p.stiffness1, false, d_E, false);
+                                p.check_sphericity != 0, d_area, p.phase_count, step, p.stiffness1,
+                                p.use_different_stiffnesses != 0, d_E, false);
             // count_and_get_div, src/GPUbounce.cu:2489-2500
             CK(cudaMemcpy(cell_div.data(), d_cell_div, N, cudaMemcpyDeviceToHost));
             std::vector<int> divs;
@@ -422,9 +502,60 @@ int main(int argc, char **argv)
                 PressureReset<<<(2 * nd) / 512 + 1, 512>>>(d_reset, d_press, p.min_pressure, 2 * nd);
                 CK(cudaMemcpy(d_E, youngs.data(), sizeof(float) * N, cudaMemcpyHostToDevice));
             }
+            // num_cells_far, src/GPUbounce.cu:1288-1290, :2538-2565
+            if (p.count_internal_radius > 0 && nd > 0 && N >= 50) {
+                fetch_cm(N);
+                calc_sys_cm(N);
+                const float rf = p.count_internal_radius;
+                const float thr = rf * rf * get_rmax2(N);
+                int far = 0;
+                for (int c = N - nd; c < N; ++c)
+                    if (dist2(c) > thr) ++far;
+                if (far) { far_log.push_back(step); far_log.push_back(far); }
+            }
         }
         status = grid();
         CK(cudaGetLastError());
+        if (status == ST_OK && p.use_different_stiffnesses && p.soften_after_growth && step == Time_steps + 2) {
+            // src/GPUbounce.cu:1340-1429, at the end of the first step after Time_steps + 1
+            int count = p.number_of_softer_cells;
+            if (p.fraction_of_softer_cells > 0) count = roundf(p.fraction_of_softer_cells * N);
+            if (p.choose_random_cell_indices) {
+                if (count > N + 1) {
+                    status = ST_SOFT;
+                } else {
+                    std::vector<int> chosen;
+                    while ((int)chosen.size() < count) {
+                        float rnd[1];
+                        ranmar(rnd, 1);
+                        const int ind = roundf(rnd[0] * N);
+                        bool seen = false;
+                        for (int q : chosen) seen = seen || q == ind;
+                        if (!seen) chosen.push_back(ind);
+                    }
+                    // index N names no cell (a division overwrites it before any use)
+                    for (int q : chosen)
+                        if (q < N) youngs[q] = p.stiffness2;
+                }
+            } else {
+                fetch_cm(N);
+                const float rmax2 = get_rmax2(N);   // before calc_sys_CM, as the reference
+                calc_sys_cm(N);
+                const float f = 1 - p.closeness_to_center;
+                int got = 0;
+                for (int c = 0; got < count && c < N; ++c)
+                    if (dist2(c) <= f * f * rmax2) { youngs[c] = p.stiffness2; ++got; }
+            }
+            CK(cudaMemcpy(d_E, youngs.data(), sizeof(float) * N, cudaMemcpyHostToDevice));
+        }
+        if (status == ST_OK && p.correct_com) {
+            // src/GPUbounce.cu:1430-1440
+            fetch_cm(N);
+            calc_sys_cm(N);
+            const long np = (long)N * 192;
+            CorrectCoMMotion<<<(unsigned)(np / 1024 + 1), 1024>>>(d_X, d_Y, d_Z, sysCM[0], sysCM[1], sysCM[2], np);
+            CK(cudaGetLastError());
+        }
         if (status == ST_OK) steps_done = step;
         if (step == in.warmup) {
             // timed region starts after the warm-up steps: drop their guard events
@@ -474,6 +605,8 @@ int main(int argc, char **argv)
     std::vector<float> hp(N);
     CK(cudaMemcpy(hp.data(), d_press, N * 4, cudaMemcpyDeviceToHost));
     fwrite(hp.data(), 4, N, fo);
+    CK(cudaMemcpy(hp.data(), d_E, N * 4, cudaMemcpyDeviceToHost));
+    fwrite(hp.data(), 4, N, fo);
     std::vector<float> hcm(3 * (size_t)N);
     CK(cudaMemcpy(hcm.data(), d_CMx, N * 4, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(hcm.data() + N, d_CMy, N * 4, cudaMemcpyDeviceToHost));
@@ -483,6 +616,10 @@ int main(int argc, char **argv)
     fwrite(&n_init, sizeof(int), 1, fo);
     fwrite(&nf, sizeof(int), 1, fo);
     if (nf) fwrite(first_forces.data(), 4, first_forces.size(), fo);
+    dump3(fRan.x, fRan.y, fRan.z, N);
+    const int nfar = (int)(far_log.size() / 2);
+    fwrite(&nfar, sizeof(int), 1, fo);
+    if (nfar) fwrite(far_log.data(), sizeof(int), far_log.size(), fo);
     fclose(fo);
     for (cudaEvent_t e : gev) cudaEventDestroy(e);
     return 0;

@@ -98,3 +98,140 @@ def test_first_step_velocities_against_reference_kernels(mesh):
     assert ev[1] < TOL
     assert dx < 1e-5
     sim.close()
+
+
+def _soft_config1(**over):
+    p, st, _ = W.config1()
+    p = W.soft_params(dict(p, div_time_steps=2), phase_count=3, soften_after_growth=1, number_of_softer_cells=5)
+    p.update(over)
+    E0 = np.full(8, np.float32(p["stiffness1"]))
+    E0[[1, 6]] = np.float32(p["stiffness2"])
+    return p, dict(st, youngs=E0)
+
+
+@pytest.mark.parametrize("path", ["random", "central"])
+def test_stiffness_schedule_against_reference_kernels(mesh, path):
+    """Variable stiffness driven by the reference's own PressureUpdate and
+    volumes kernels and its host softening code: 12 steps of 8 dividing cells
+    (2 soft), softening at the end of step 4.  Stiffness, pressure and
+    division events exact; positions within FP32 noise."""
+    over = dict(choose_random_cell_indices=1) if path == "random" else dict(closeness_to_center=0.4,
+                                                                             number_of_softer_cells=3)
+    p, st = _soft_config1(**over)
+    topo, _ = topo_for(st, mesh)
+    r = ref.run(cs.make_params(p), topo, st, 64, 12)
+    assert r["status"] == 0, r["status_text"]
+    sim = cs.Simulation(p, topo, 64)
+    sim.load_state(st["X"], st["Y"], st["Z"], youngs=st["youngs"], n_cells=st["n"])
+    sim.step(12)
+    s = sim.state()
+    n = s["n"]
+    assert n == r["n"]
+    assert np.array_equal(np.asarray(sim.events()).reshape(-1, 3), r["events"])
+    assert np.array_equal(s["youngs"][:n], r["youngs"])
+    assert np.array_equal(s["pressure"][:n].view(np.uint32), r["pressure"].view(np.uint32))
+    assert int((r["youngs"] != np.float32(p["stiffness1"])).sum()) > 4
+    dx = max(float(np.max(np.abs(s[k][: n * 192] - r[k]))) for k in ("X", "Y", "Z"))
+    print("stiffness %s: %d soft of %d, position max |dx| %.2e" % (path, int((r["youngs"] != p["stiffness1"]).sum()),
+                                                                 n, dx))
+    assert dx < 1e-4
+    sim.close()
+
+
+def test_correct_com_against_reference_kernels(mesh):
+    """CoM correction by the reference's CorrectCoMMotion kernel and host
+    calc_sys_CM, at set-up and after every step (8 cells dividing at step 1).
+    No rigid box: the correction centres the system on the origin, outside a
+    box that starts there.  The node positions agree to FP32 noise after one
+    step and after 20, and the CUDA path is no farther from the reference
+    than the FP64 oracle is."""
+    p, st, _ = W.config1()
+    p = dict(p, correct_com=1, use_rigid_box=0)
+    topo, _ = topo_for(st, mesh)
+
+    def dist(a, b, n):
+        # the 180 nodes of every cell: the padding slots carry no state (with the
+        # correction the reference's follow its stale XP copies)
+        return max(float(np.max(np.abs(a[k][: n * 192].reshape(n, 192)[:, :180] -
+                                       b[k][: n * 192].reshape(n, 192)[:, :180]))) for k in ("X", "Y", "Z"))
+
+    for steps in (1, 20):
+        r = ref.run(cs.make_params(p), topo, st, 64, steps)
+        assert r["status"] == 0, r["status_text"]
+        sim, orc = make_pair(p, st, mesh, 64, record_pairs=False)
+        sim.step(steps)
+        orc.step(steps)
+        s = sim.state()
+        n = s["n"]
+        assert n == r["n"] == orc.n
+        assert np.array_equal(np.asarray(sim.events()).reshape(-1, 3), r["events"])
+        o = {"X": orc.X, "Y": orc.Y, "Z": orc.Z}
+        d_ours, d_orc, d_pair = dist(s, r, n), dist(o, r, n), dist(s, o, n)
+        centre = np.array([r[k][: n * 192].reshape(n, 192)[:, :180].mean() for k in ("X", "Y", "Z")])
+        print("correct_com %2d steps: |dx| CUDA-reference %.2e, oracle-reference %.2e, CUDA-oracle %.2e, "
+              "reference centre %s" % (steps, d_ours, d_orc, d_pair, centre))
+        assert np.all(np.abs(centre) < 1e-2)      # the system is centred on the origin
+        assert d_ours < 2e-5
+        assert d_ours <= max(1e-5, 1.5 * d_orc)
+        sim.close()
+        orc.close()
+
+
+def test_far_counts_against_reference_kernels(mesh):
+    """The internal-cells mitotic count (num_cells_far) after the step-1
+    divisions of 56 clustered cells, against the reference's host code."""
+    box = 60.0
+    c = W.rsa_centres(56, 14.0, np.random.default_rng(11)) + np.float32(23.0)
+    p = W.base_params(box_len=(box, box, box), div_time_steps=10 ** 9, count_internal_radius=0.6,
+                      rng_ij=11, rng_kl=1100)
+    st = W.state(c)
+    topo, _ = topo_for(st, mesh)
+    r = ref.run(cs.make_params(p), topo, st, 160, 3)
+    assert r["status"] == 0, r["status_text"]
+    sim = cs.Simulation(p, topo, 160)
+    sim.load_state(st["X"], st["Y"], st["Z"], n_cells=st["n"])
+    sim.step(3)
+    assert sim.n_cells() == r["n"]
+    assert np.array_equal(np.asarray(sim.events()).reshape(-1, 3), r["events"])
+    assert np.array_equal(sim.far_counts(), r["far"])
+    assert len(r["far"]) and r["far"][0].tolist() == [1, 56]
+    sim.close()
+
+
+def test_langevin_statistics_against_reference_kernels(mesh):
+    """The Langevin force is Philox4x32-10 here and curand XORWOW (MT19937
+    seeds) in the reference, so parity is statistical: 27 non-dividing cells,
+    200 steps with rand_scale_factor 1.  The last step's random forces of both
+    are samples of the same normal law (two-sample KS test, mean and standard
+    deviation), and the node velocities they drive have the same spread."""
+    from scipy import stats
+    c = np.array([[3 + 2.3 * i, 3 + 2.3 * j, 3 + 2.3 * k] for i in range(3) for j in range(3) for k in range(3)],
+                 dtype=np.float32)
+    p = W.base_params(box_len=(12.0, 12.0, 12.0), growth_rate=0.0, min_pressure=100.0, max_pressure=100.0,
+                      add_rands=1, rand_scale_factor=1.0, rand_seed=17)
+    st = W.state(c)
+    topo, _ = topo_for(st, mesh)
+    r = ref.run(cs.make_params(p), topo, st, 64, 200)
+    assert r["status"] == 0, r["status_text"]
+    sim = cs.Simulation(p, topo, 64)
+    sim.load_state(st["X"], st["Y"], st["Z"], n_cells=st["n"])
+    sim.step(200)
+    n = st["n"]
+    mask = np.zeros((n, 192), bool)
+    mask[:, :180] = True
+    mask = mask.reshape(-1)
+    fr = sim.random_force()
+    ours = np.concatenate([fr[k][: n * 192][mask] for k in ("FRX", "FRY", "FRZ")])
+    theirs = np.concatenate([r[k][mask] for k in ("FRX", "FRY", "FRZ")])
+    ks = stats.ks_2samp(ours, theirs)
+    s = sim.state()
+    v_ours = np.concatenate([s[k][: n * 192][mask] for k in ("VX", "VY", "VZ")])
+    v_ref = np.concatenate([r[k][mask] for k in ("VX", "VY", "VZ")])
+    print("random force: ours mean %.4f sd %.4f, reference mean %.4f sd %.4f, KS p %.3f; "
+          "velocity sd ours %.4e reference %.4e"
+          % (ours.mean(), ours.std(), theirs.mean(), theirs.std(), ks.pvalue, v_ours.std(), v_ref.std()))
+    assert ks.pvalue > 1e-3
+    for a in (ours, theirs):
+        assert abs(a.mean()) < 0.05 and abs(a.std() - 1.0) < 0.03
+    assert abs(v_ours.std() / v_ref.std() - 1.0) < 0.15
+    sim.close()
