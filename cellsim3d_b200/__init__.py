@@ -169,6 +169,7 @@ class Ensemble:
                                     C.c_void_p(stream) if stream else None, C.byref(self.h))
         _lib.check(st, "cs3d_create_ensemble")
         self.n_inst = n
+        self._n0 = [0] * n
         self.capacities = caps.copy()
 
     # -- lifetime
@@ -199,6 +200,7 @@ class Ensemble:
         st = _lib.lib().cs3d_load_state(self.h, inst, n, _fp(X), _fp(Y), _fp(Z), _fp(VX), _fp(VY), _fp(VZ),
                                         _fp(pressure), _fp(youngs))
         _lib.check(st, "cs3d_load_state")
+        self._n0[inst] = n
 
     def set_rng(self, inst, rng):
         _lib.check(_lib.lib().cs3d_set_rng(self.h, inst, C.byref(rng.state)), "cs3d_set_rng")
@@ -322,6 +324,27 @@ class Ensemble:
         out = np.zeros((max(cnt.value, 1), 2), dtype=np.int32)
         _lib.check(L.cs3d_get_far_counts(self.h, inst, _ip(out), cnt.value, C.byref(cnt)), "cs3d_get_far_counts")
         return out[:cnt.value]
+
+    def volume_histogram(self, inst=0, lo=0.0, hi=6.0, nbins=60, volumes=False):
+        """Counts of the cells' volumes at the current positions, computed on the
+        device: [below lo, nbins equal bins of [lo, hi), at or above hi]; with
+        volumes=True also every cell's volume."""
+        counts = np.zeros(nbins + 2, dtype=np.int64)
+        n = self.n_cells(inst)
+        vols = np.zeros(max(n, 1), dtype=np.float32) if volumes else None
+        _lib.check(_lib.lib().cs3d_volume_histogram(self.h, inst, float(lo), float(hi), int(nbins),
+                                                     counts.ctypes.data_as(C.POINTER(C.c_int64)),
+                                                     _fp(vols) if volumes else None), "cs3d_volume_histogram")
+        return (counts, vols[:n]) if volumes else counts
+
+    def population(self, inst=0, steps=None, n0=None):
+        """Cell count after every step 0..steps, from the division events
+        (the curve scripts/pop.py draws from a trajectory)."""
+        ev = self.events(inst)
+        steps = int(self.stats()["steps"]) if steps is None else int(steps)
+        n0 = self._n0[inst] if n0 is None else int(n0)
+        born = np.bincount(ev[:, 0], minlength=steps + 1)[: steps + 1] if len(ev) else np.zeros(steps + 1, int)
+        return n0 + np.cumsum(born)
 
     def last_error(self, inst=0):
         b = C.c_uint32()

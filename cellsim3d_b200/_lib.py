@@ -83,7 +83,7 @@ EXPORTS = [
     "cs3d_initial_stiffness", "cs3d_init_positions", "cs3d_traj_open", "cs3d_traj_write_frame", "cs3d_traj_close", "cs3d_create",
     "cs3d_create_ensemble", "cs3d_load_state", "cs3d_set_rng", "cs3d_get_rng", "cs3d_step", "cs3d_get_state",
     "cs3d_get_forces", "cs3d_get_random_force", "cs3d_get_cells", "cs3d_get_grid", "cs3d_set_option", "cs3d_get_pairs",
-    "cs3d_get_events", "cs3d_get_far_counts", "cs3d_last_error", "cs3d_get_stats", "cs3d_profile_step", "cs3d_last_step_ms",
+    "cs3d_get_events", "cs3d_get_far_counts", "cs3d_volume_histogram", "cs3d_last_error", "cs3d_get_stats", "cs3d_profile_step", "cs3d_last_step_ms",
     "cs3d_destroy", "cs3d_forces_static",
 ]
 
@@ -144,6 +144,7 @@ def lib():
     L.cs3d_get_pairs.argtypes = [P, C.c_int, C.c_int, ip, C.c_longlong, C.POINTER(C.c_longlong)]
     L.cs3d_get_events.argtypes = [P, C.c_int, ip, C.c_int, ip]
     L.cs3d_get_far_counts.argtypes = [P, C.c_int, ip, C.c_int, ip]
+    L.cs3d_volume_histogram.argtypes = [P, C.c_int, C.c_float, C.c_float, C.c_int, C.POINTER(C.c_int64), fp]
     L.cs3d_last_error.argtypes = [P, C.c_int, C.POINTER(C.c_uint32)]
     L.cs3d_get_stats.argtypes = [P, C.POINTER(C.c_longlong), C.c_int]
     L.cs3d_profile_step.argtypes = [P, C.c_int, fp, C.c_char_p, C.c_int, C.c_int, ip]

@@ -3,6 +3,7 @@
 // per step variant into a CUDA graph) and read-back.  All entry points are
 // extern "C" and return CS3D_* status codes.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -929,6 +930,39 @@ int cs3d_get_events(cs3d_ctx *c, int inst, int32_t *out, int max_events, int *co
         ++k;
     }
     *count = k;
+    return CS3D_OK;
+}
+
+int cs3d_volume_histogram(cs3d_ctx *c, int inst, float lo, float hi, int nbins, int64_t *counts, float *volumes)
+{
+    if (!c || inst < 0 || inst >= c->n_inst || nbins < 1 || nbins > (1 << 20) || !counts || !(lo < hi) ||
+        !std::isfinite(lo) || !std::isfinite(hi))
+        return CS3D_E_ARG;
+    cudaSetDevice(c->device);
+    int rc = ensure_init(c);
+    if (rc) return rc;
+    int n = 0;
+    if ((rc = inst_count(c, inst, &n))) return rc;
+    // scratch for the counts and the volumes, freed before returning
+    unsigned long long *dc = nullptr;
+    float *dv = nullptr;
+    if (cudaMalloc(&dc, sizeof(unsigned long long) * (nbins + 2)) != cudaSuccess) return CS3D_E_NOMEM;
+    if (volumes && n && cudaMalloc(&dv, sizeof(float) * n) != cudaSuccess) { cudaFree(dc); return CS3D_E_NOMEM; }
+    std::vector<unsigned long long> h(nbins + 2);
+    cudaError_t e = cudaMemsetAsync(dc, 0, sizeof(unsigned long long) * (nbins + 2), c->stream);
+    if (e == cudaSuccess && n) {
+        const int blocks = std::min(n, c->nsm * 8);
+        k_vol_hist<<<blocks, SLOTS, 0, c->stream>>>(c->d, inst, lo, hi, nbins, dc, dv);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(h.data(), dc, sizeof(unsigned long long) * (nbins + 2), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess && dv) e = cudaMemcpyAsync(volumes, dv, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(dc);
+    if (dv) cudaFree(dv);
+    if (e != cudaSuccess) return CS3D_E_CUDA;
+    for (int b = 0; b < nbins + 2; ++b) counts[b] = (int64_t)h[b];
     return CS3D_OK;
 }
 

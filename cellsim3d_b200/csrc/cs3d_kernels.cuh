@@ -1328,6 +1328,44 @@ __global__ void k_soften(Dev d, int step)
         if (dist2(d.CM[P.base + c], o) <= thr) { E[c] = P.E2; ++got; }
 }
 
+// Volume histogram of one instance's cells at the current positions (the
+// analysis scripts/pop.py and the statistical checks do offline): one block
+// per cell computes the centre of mass and the volume of src/volume.cu:5-163
+// in FP64 (the division test's arithmetic) and counts it into one of nbins
+// equal bins over [lo, hi), counts[0] below, counts[nbins + 1] at or above.
+__global__ void __launch_bounds__(SLOTS) k_vol_hist(Dev d, int inst, float lo, float hi, int nbins,
+                                                    unsigned long long *counts, float *vols)
+{
+    __shared__ float4 xs[SLOTS];
+    __shared__ GeomScratch gs;
+    const InstParams &P = d.prm[inst];
+    const int n = d.st[inst].n;
+    for (int c = blockIdx.x; c < n; c += gridDim.x) {
+        const int a = P.base + c;
+        const int i = threadIdx.x;
+        xs[i] = i < NODES ? d.X[(size_t)a * SLOTS + i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        __syncthreads();
+        float3 cm;
+        float4 blo, bhi;
+        cell_geom(xs, gs, cm, blo, bhi);
+        double vol, area;
+        cell_volume(d, xs, cm, gs, false, vol, area);
+        if (i == 0) {
+            const float v = (float)vol;
+            if (vols) vols[c] = v;
+            int b;
+            if (!(v >= lo)) b = 0;
+            else if (!(v < hi)) b = nbins + 1;
+            else {
+                b = 1 + (int)((double)(v - lo) / ((double)hi - (double)lo) * nbins);
+                b = b > nbins ? nbins : b;
+            }
+            atomicAdd(&counts[b], 1ull);
+        }
+        __syncthreads();
+    }
+}
+
 // G: grid extents of instances that divided this step, from all boxes.
 __global__ void k_grid_fix(Dev d, int par)
 {

@@ -284,6 +284,14 @@ int cs3d_get_state(cs3d_ctx *ctx, int inst, int *n_cells, float *X, float *Y, fl
 int cs3d_get_forces(cs3d_ctx *ctx, int inst, float *FCX, float *FCY, float *FCZ,
                     float *FDX, float *FDY, float *FDZ);
 
+/* Histogram of the volumes of instance inst's cells at the current positions (centre of mass
+ * and volume of src/volume.cu:5-163 in FP64, computed on the device; the analysis that the
+ * reference's scripts do offline): counts[0] below lo, counts[1..nbins] the equal bins of
+ * [lo, hi), counts[nbins + 1] at or above hi.  volumes (may be NULL) receives every cell's
+ * volume. */
+int cs3d_volume_histogram(cs3d_ctx *ctx, int inst, float lo, float hi, int nbins, int64_t *counts,
+                          float *volumes);
+
 /* Division steps at which cells were discounted from the mitotic index as far from the
  * system's centre (count_internal_radius > 0; src/GPUbounce.cu:1288-1290, :2538-2565):
  * pairs (step, count) into out[2 * max_entries]; *n_entries = the number recorded. */

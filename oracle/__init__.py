@@ -365,6 +365,12 @@ class System:
     def compute_cm(self):
         lib().orc_center_of_mass(self.h)
 
+    def compute_volumes(self):
+        """Centres of mass and volumes (src/volume.cu:5-163) of the current positions."""
+        lib().orc_center_of_mass(self.h)
+        lib().orc_volumes(self.h)
+        return self.vol[: self.n].copy()
+
 
 def _attach_force_methods():
     def con_force(self):
