@@ -326,8 +326,9 @@ int run_init(cs3d_ctx *c)
 
 // One timestep, src/GPUbounce.cu:1055-1338, as a fixed launch sequence.
 // k1: the step starts with k_integrate (else the previous step's fused S2
-// did it); fuse: S2 also integrates the next step (no division this step,
-// and the next step follows in the same call); soften: the number of this
+// did it); fuse: S2 also integrates the next step (the next step follows in
+// the same call; on division steps the two cells of each division are
+// integrated after their placement); soften: the number of this
 // step when its end softens cells (launched outside the graphs), else 0.
 int launch_step(cs3d_ctx *c, int par, bool div, bool k1 = true, bool fuse = false, const Prof &pf = Prof(),
                 long long soften = 0)
@@ -341,7 +342,8 @@ int launch_step(cs3d_ctx *c, int par, bool div, bool k1 = true, bool fuse = fals
     if (rc) return rc;
     n += NL_LAUNCHES;
     k_s1<false><<<c->grid_cells, SLOTS, sizeof(S1Smem), s>>>(d, par); ++n; pf.mark(s, "s1_con_dis");
-    if (div) k_s2<true, false><<<c->grid_s2, SLOTS, 0, s>>>(d, par);
+    if (div && fuse) k_s2<true, true><<<c->grid_s2, SLOTS, 0, s>>>(d, par);
+    else if (div) k_s2<true, false><<<c->grid_s2, SLOTS, 0, s>>>(d, par);
     else if (fuse) k_s2<false, true><<<c->grid_s2, SLOTS, 0, s>>>(d, par);
     else k_s2<false, false><<<c->grid_s2, SLOTS, 0, s>>>(d, par);
     ++n; pf.mark(s, fuse ? "s2_dis_geom_integrate" : "s2_dis_geom");
@@ -350,6 +352,8 @@ int launch_step(cs3d_ctx *c, int par, bool div, bool k1 = true, bool fuse = fals
         k_div_apply<<<c->grid_cells, SLOTS, 0, s>>>(d, par); ++n; pf.mark(s, "div_apply");
         k_grid_fix<<<c->grid_flat, 256, 0, s>>>(d, par); ++n; pf.mark(s, "grid_fix");
         if (c->any_far) { k_far_count<<<c->n_inst, 32, 0, s>>>(d); ++n; pf.mark(s, "far_count"); }
+        // S2 did the next half kick of every cell that does not divide
+        if (fuse) { k_integrate_divided<<<c->grid_cells, SLOTS, 0, s>>>(d); ++n; pf.mark(s, "integrate_divided"); }
     }
     if (soften) { k_soften<<<c->n_inst, 32, 0, s>>>(d, (int)soften); ++n; pf.mark(s, "soften"); }
     if (c->any_com) { k_com_shift<<<c->n_inst, 256, 0, s>>>(d); ++n; pf.mark(s, "com_shift"); }
@@ -700,7 +704,7 @@ int cs3d_step(cs3d_ctx *c, int n_steps)
         int par = (int)((s - 1) & 1);
         bool div = c->any_growth && s <= c->max_div_steps;
         const bool soften = is_soften_step(c, s);
-        bool fuse = !div && !c->any_com && !soften && k + 1 < n_steps;
+        bool fuse = !c->any_com && !soften && k + 1 < n_steps;
         if (soften) {
             // the one step that softens cells runs outside the graphs
             if ((rc = launch_step(c, par, div, k1, false, Prof(), s))) return rc;

@@ -420,12 +420,10 @@ __device__ __forceinline__ void pressure_update(const Dev &d, const InstParams &
 // K1: first half kick + drift of a step (Integrate + ForwardTime,
 // src/propagate.cu:681-763) and PressureUpdate (src/PressureKernels.cu:4-40).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(SLOTS) k_integrate(Dev d)
+// One cell, called by the whole block (it synchronises).
+__device__ __forceinline__ void integrate_cell(const Dev &d, int a, float *smax)
 {
-    const int W = n_work(d);
-    __shared__ float smax[SLOTS / 32];
-    for (int w = blockIdx.x; w < W; w += gridDim.x) {
-        int a = cell_of(d, w);
+    {
         int inst = inst_of(d, a);
         const InstParams &P = d.prm[inst];
         int i = threadIdx.x;
@@ -465,6 +463,26 @@ __global__ void __launch_bounds__(SLOTS) k_integrate(Dev d)
             pressure_update(d, P, a, d.st[inst].step + 1);
         }
         __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(SLOTS) k_integrate(Dev d)
+{
+    const int W = n_work(d);
+    __shared__ float smax[SLOTS / 32];
+    for (int w = blockIdx.x; w < W; w += gridDim.x) integrate_cell(d, cell_of(d, w), smax);
+}
+
+// The next step's half kick and drift of the two cells of each division of
+// this step, after their placement (division steps whose S2 did the others).
+__global__ void __launch_bounds__(SLOTS) k_integrate_divided(Dev d)
+{
+    __shared__ float smax[SLOTS / 32];
+    const int T = *d.div_total;
+    for (int q = blockIdx.x; q < T; q += gridDim.x) {
+        const DivEntry e = d.divtab[q];
+        integrate_cell(d, e.parent, smax);
+        integrate_cell(d, e.daughter, smax);
     }
 }
 
@@ -839,7 +857,39 @@ struct S2Smem {
     float4 vs[SLOTS];
     int cell[MAXC];
     GeomScratch gs;
+    int dflag;   // the cell divides (division steps)
 };
+
+// Integrate + ForwardTime of the next step (src/propagate.cu:681-763) on the
+// node's force and velocity after this step; returns the node's distance from
+// its list anchor.  The same operations as k_integrate.
+__device__ __forceinline__ float next_kick(const Dev &d, const InstParams &P, size_t g, float4 x4, float4 v4,
+                                           float3 fd)
+{
+    const float4 fc = d.FC[g];
+    const float dt = P.dt;
+    const double m = P.mass;
+    float sx = __fadd_rn(__fmul_rn(dt, fc.x), __fmul_rn(dt, fd.x));
+    float sy = __fadd_rn(__fmul_rn(dt, fc.y), __fmul_rn(dt, fd.y));
+    float sz = __fadd_rn(__fmul_rn(dt, fc.z), __fmul_rn(dt, fd.z));
+    if (P.rands) {
+        const float4 fr = d.FR[g];
+        sx = __fadd_rn(sx, __fmul_rn(P.rdt, fr.x));
+        sy = __fadd_rn(sy, __fmul_rn(P.rdt, fr.y));
+        sz = __fadd_rn(sz, __fmul_rn(P.rdt, fr.z));
+    }
+    float4 vn = v4;
+    vn.x = kick(v4.x, sx, m);
+    vn.y = kick(v4.y, sy, m);
+    vn.z = kick(v4.z, sz, m);
+    const float4 xn = make_float4(__fmaf_rn(vn.x, dt, x4.x), __fmaf_rn(vn.y, dt, x4.y),
+                                  __fmaf_rn(vn.z, dt, x4.z), 0.0f);
+    const float4 xb = d.Xb[g];
+    const float ddx = xn.x - xb.x, ddy = xn.y - xb.y, ddz = xn.z - xb.z;
+    d.X[g] = xn;
+    d.V[g] = vn;
+    return sqrtf(ddx * ddx + ddy * ddy + ddz * ddz);
+}
 
 __device__ __forceinline__ void flush_mm(Dev &d, int inst, int pn, const float *acc)
 {
@@ -880,45 +930,22 @@ __global__ void __launch_bounds__(SLOTS, 5) k_s2(Dev d, int par)
         sm.vs[i] = v4;
         __syncthreads();
         float disp = 0.0f;
+        float3 fdk = make_float3(0.f, 0.f, 0.f);
         if (i < NODES) {
             const float3 v = f3(v4);
             const float3 nrm = node_normal(sm.xs, n0, n1, n2, sgn);
             const double3 vt = sweep_s2(d, sm.cell, a, i, v, nrm, nd);
             const float3 fd = dis_force(P, sm.vs, n0, n1, n2, v, vt);
             d.FD[g] = make_float4(fd.x, fd.y, fd.z, 0.f);
-            if (FUSE) {
-                // Integrate + ForwardTime of the next step, src/propagate.cu:681-763
-                const float4 fc = d.FC[g];
-                const float dt = P.dt;
-                const double m = P.mass;
-                float sx = __fadd_rn(__fmul_rn(dt, fc.x), __fmul_rn(dt, fd.x));
-                float sy = __fadd_rn(__fmul_rn(dt, fc.y), __fmul_rn(dt, fd.y));
-                float sz = __fadd_rn(__fmul_rn(dt, fc.z), __fmul_rn(dt, fd.z));
-                if (P.rands) {
-                    const float4 fr = d.FR[g];
-                    sx = __fadd_rn(sx, __fmul_rn(P.rdt, fr.x));
-                    sy = __fadd_rn(sy, __fmul_rn(P.rdt, fr.y));
-                    sz = __fadd_rn(sz, __fmul_rn(P.rdt, fr.z));
-                }
-                float4 vn = v4;
-                vn.x = kick(v4.x, sx, m);
-                vn.y = kick(v4.y, sy, m);
-                vn.z = kick(v4.z, sz, m);
-                const float4 xn = make_float4(__fmaf_rn(vn.x, dt, x4.x), __fmaf_rn(vn.y, dt, x4.y),
-                                              __fmaf_rn(vn.z, dt, x4.z), 0.0f);
-                const float4 xb = d.Xb[g];
-                const float ddx = xn.x - xb.x, ddy = xn.y - xb.y, ddz = xn.z - xb.z;
-                disp = sqrtf(ddx * ddx + ddy * ddy + ddz * ddz);
-                d.X[g] = xn;
-                d.V[g] = vn;
-            } else {
-                d.V[g] = v4;
-            }
+            fdk = fd;
+            if (FUSE && !DIV) disp = next_kick(d, P, g, x4, v4, fd);
+            else d.V[g] = v4;
         }
-        if (FUSE) {
+        if (FUSE && !DIV) {
             for (int o = 16; o > 0; o >>= 1) disp = fmaxf(disp, __shfl_xor_sync(0xffffffffu, disp, o));
             if ((i & 31) == 0) smax[i >> 5] = disp;
         }
+        if (i == 0) sm.dflag = 0;
         float3 cm;
         float4 lo, hi;
         cell_geom(sm.xs, sm.gs, cm, lo, hi);
@@ -937,12 +964,24 @@ __global__ void __launch_bounds__(SLOTS, 5) k_s2(Dev d, int par)
                         if (fabs(1.0 - psi) > 0.05) flag = 0;
                     }
                     d.divflag[a] = (uint8_t)flag;
+                    sm.dflag = flag;
                 }
             }
         }
+        if (FUSE && DIV) {
+            // With the division decision known: a cell that does not divide
+            // takes the next step's half kick and drift here, the two cells of
+            // a division after their placement (k_integrate_divided).
+            __syncthreads();
+            const bool divides = sm.dflag != 0;   // uniform
+            if (!divides && i < NODES) disp = next_kick(d, P, g, x4, v4, fdk);
+            for (int o = 16; o > 0; o >>= 1) disp = fmaxf(disp, __shfl_xor_sync(0xffffffffu, disp, o));
+            if ((i & 31) == 0) smax[i >> 5] = disp;
+            __syncthreads();
+        }
         if (i == 0) {
-            if (FUSE) {
-                float mx = smax[0];  // visible: cell_geom synchronises the block
+            if (FUSE && (!DIV || sm.dflag == 0)) {
+                float mx = smax[0];  // visible: cell_geom (and the division decision) synchronise the block
                 for (int q = 1; q < SLOTS / 32; ++q) mx = fmaxf(mx, smax[q]);
                 atomicMax(&st->disp_step, __float_as_uint(mx));
                 pressure_update(d, P, a, st->step + 1);  // the next step's PressureUpdate

@@ -197,34 +197,57 @@ def test_capacity_overflow_reports(mesh):
     assert sim.n_cells() == 12
 
 
-def test_multi_step_launch_equals_single_steps(mesh):
-    """cs3d_step(n) fuses the first half kick and drift of each step into the
-    previous step's last kernel; n single-step calls do not.  The two must
-    give bit-identical states (same float operations)."""
+def _multi_step_cases():
     c, vel, L = W.packed_fcc(64, phi=0.5, seed=5)
-    p = W.base_params(box_len=(L, L, L), growth_rate=0.0, min_pressure=200.0, max_pressure=200.0,
-                      div_time_steps=5000)
-    st = W.state(c, velocities=vel)
-    topo, _ = topo_for(st, mesh)
-    sims = []
+    packed = W.base_params(box_len=(L, L, L), growth_rate=0.0, min_pressure=200.0, max_pressure=200.0,
+                           div_time_steps=5000)
+    p1, st1, _ = W.config1()
+    colony = [(W.base_params(box_len=(12.0, 12.0, 12.0), growth_rate=gr, division_vol=2.9 - 0.1 * k,
+                             rng_ij=k, rng_kl=100 * k), W.state(W.random_centres(n, 12.0, W.SplitMix(100 + k))))
+              for k, (n, gr) in enumerate([(3, 0.002), (1, 0.004), (8, 0.001)])]
+    return {
+        "packed": ([(packed, W.state(c, velocities=vel))], 64, 25),
+        # every cell divides at step 1, more divisions follow
+        "dividing": ([(p1, st1)], 64, 60),
+        "dividing_langevin": ([(dict(p1, add_rands=1, rand_scale_factor=0.5, rand_seed=9), st1)], 64, 60),
+        "ensemble": (colony, 32, 40),
+    }
+
+
+@pytest.mark.parametrize("case", ["packed", "dividing", "dividing_langevin", "ensemble"])
+def test_multi_step_launch_equals_single_steps(mesh, case):
+    """cs3d_step(n) fuses the first half kick and drift of each step into the
+    previous step's S2 (on division steps: into S2 for the cells that do not
+    divide, and into a kernel after the division for the two cells of each
+    division); n single-step calls do not.  The two must give bit-identical
+    states, forces, division events and list rebuilds (same float operations)."""
+    insts, cap, steps = _multi_step_cases()[case]
+    topo, _ = topo_for(insts[0][1], mesh)
+    runs = []
     for mode in ("fused", "single"):
-        sim = cs.Simulation(p, topo, 64)
-        sim.load_state(st["X"], st["Y"], st["Z"], st["VX"], st["VY"], st["VZ"], n_cells=st["n"])
+        ens = cs.Ensemble([p for p, _ in insts], topo, [cap] * len(insts))
+        for k, (p, st) in enumerate(insts):
+            ens.load_state(k, st["X"], st["Y"], st["Z"], st.get("VX"), st.get("VY"), st.get("VZ"), n_cells=st["n"])
         if mode == "fused":
-            sim.step(25)
+            ens.step(steps)
         else:
-            for _ in range(25):
-                sim.step(1)
-        sims.append(sim)
-    a, b = sims[0].state(), sims[1].state()
-    for k in ("X", "Y", "Z", "VX", "VY", "VZ", "pressure"):
-        assert np.array_equal(a[k].view(np.uint32), b[k].view(np.uint32)), k
-    fa, fb = sims[0].forces(), sims[1].forces()
-    for k in fa:
-        assert np.array_equal(fa[k].view(np.uint32), fb[k].view(np.uint32)), k
-    assert sims[0].stats()["rebuilds"] == sims[1].stats()["rebuilds"]
-    for sim in sims:
-        sim.close()
+            for _ in range(steps):
+                ens.step(1)
+        runs.append(ens)
+    for k in range(len(insts)):
+        a, b = runs[0].state(k), runs[1].state(k)
+        assert a["n"] == b["n"]
+        for key in ("X", "Y", "Z", "VX", "VY", "VZ", "pressure", "youngs"):
+            assert np.array_equal(a[key].view(np.uint32), b[key].view(np.uint32)), (k, key)
+        fa, fb = runs[0].forces(k), runs[1].forces(k)
+        for key in fa:
+            assert np.array_equal(fa[key].view(np.uint32), fb[key].view(np.uint32)), (k, key)
+        assert np.array_equal(runs[0].events(k), runs[1].events(k))
+    assert runs[0].stats()["rebuilds"] == runs[1].stats()["rebuilds"]
+    if case != "packed":
+        assert any(len(runs[0].events(k)) for k in range(len(insts)))
+    for ens in runs:
+        ens.close()
 
 
 def test_correct_com_single_steps(mesh):
