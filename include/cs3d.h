@@ -35,7 +35,9 @@ extern "C" {
 #define CS3D_E_PARSE           -5   /* inp.json malformed or missing section */
 #define CS3D_E_CONFIG          -6   /* parameter validation failed */
 #define CS3D_E_DEVICE_FLAGS    -7   /* a kernel raised an error bit, see cs3d_last_error */
-#define CS3D_E_CAPACITY       -69   /* population exceeded capacity, src/GPUbounce.cu:1265-1270 */
+#define CS3D_E_CAPACITY       -69   /* population exceeded capacity, src/GPUbounce.cu:1265-1270; as in the
+                                       reference (which exits), the run ends there: the cells that could
+                                       not divide did not take the step's last half kick either */
 #define CS3D_E_UNSUPPORTED     -8   /* feature of the reference outside this build */
 
 /* ---- device error bits (cs3d_last_error) ------------------------------ */
