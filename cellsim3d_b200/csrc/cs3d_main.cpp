@@ -13,6 +13,7 @@
 // initial state is read from it instead of being placed (format: the 8 bytes
 // "CS3DINIT", int32 n, then float32 X, Y, Z, VX, VY, VZ [n*192 each],
 // pressure [n], youngs [n]).
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -74,6 +75,44 @@ void write_ascii_frame(FILE *f, int step, int interval, int n, const float *X, c
         for (int p = 0; p < 192; p++)
             fprintf(f, "%.7f,  %.7f,  %.7f\n", X[c * 192 + p], Y[c * 192 + p], Z[c * 192 + p]);
     }
+}
+
+// writeForces, src/GPUbounce.cu:2567-2598: one line per node with the total
+// conservative force, the velocity, the position, and the cell's pressure and
+// volume (the volume of the last division test; 0 before any).
+void write_force_rows(FILE *f, int step, int n, const float *FX, const float *FY, const float *FZ, const float *VX,
+                      const float *VY, const float *VZ, const float *X, const float *Y, const float *Z,
+                      const float *press, const float *vol)
+{
+    auto mag = [](float x, float y, float z) { return sqrtf(x * x + y * y + z * z); };
+    for (int c = 0; c < n; ++c)
+        for (int k = 0; k < 180; ++k) {
+            const size_t g = (size_t)c * 192 + k;
+            fprintf(f, "%d,%d,%d,%d,%d,%.8f,%.8f,%.8f,%.8f,%.8f,%.8f,%.8f,%.8f,%.8f,%.8f,%.8f,%.8f,%.8f\n", step, n, c, k,
+                    (int)g, FX[g], FY[g], FZ[g], mag(FX[g], FY[g], FZ[g]), VX[g], VY[g], VZ[g],
+                    mag(VX[g], VY[g], VZ[g]), X[g], Y[g], Z[g], press[c], vol[c]);
+        }
+}
+
+// The force file of write_cont_force: the state of the device at a frame.
+int write_forces_frame(cs3d_ctx *ctx, FILE *f, int step, size_t cap_nodes, int max_cells, const float *X0,
+                       const float *Y0, const float *Z0)
+{
+    std::vector<float> F[3], V[3], P[3], press(max_cells), vol(max_cells);
+    for (int q = 0; q < 3; ++q) {
+        F[q].assign(cap_nodes, 0.f);
+        V[q].assign(cap_nodes, 0.f);
+        if (!X0) P[q].assign(cap_nodes, 0.f);
+    }
+    int n = 0, rc;
+    if ((rc = cs3d_get_state(ctx, 0, &n, X0 ? nullptr : P[0].data(), X0 ? nullptr : P[1].data(),
+                             X0 ? nullptr : P[2].data(), V[0].data(), V[1].data(), V[2].data(), press.data(), nullptr)))
+        return rc;
+    if ((rc = cs3d_get_forces(ctx, 0, F[0].data(), F[1].data(), F[2].data(), nullptr, nullptr, nullptr))) return rc;
+    if ((rc = cs3d_get_cells(ctx, 0, nullptr, vol.data(), nullptr, nullptr))) return rc;
+    write_force_rows(f, step, n, F[0].data(), F[1].data(), F[2].data(), V[0].data(), V[1].data(), V[2].data(),
+                     X0 ? X0 : P[0].data(), X0 ? Y0 : P[1].data(), X0 ? Z0 : P[2].data(), press.data(), vol.data());
+    return CS3D_OK;
 }
 
 }  // namespace
@@ -171,6 +210,16 @@ int main(int argc, char **argv)
                 max_frames);
         write_ascii_frame(ascii, 0, interval, n0, X.data(), Y.data(), Z.data(), prm, youngs.data());
     }
+    // force file, src/GPUbounce.cu:1030-1047 (header and the initial forces;
+    // the positions are the host's initial ones, as there)
+    FILE *forces = nullptr;
+    if (cfg.write_cont_force) {
+        forces = fopen(cfg.forces_file, "w");
+        if (!forces) return fail("forces file", CS3D_E_IO);
+        fprintf(forces, "step,num_cells,cell_ind,node_ind,glob_node_ind,FX,FY,FZ,F,VX,VY,VZ,V,X,Y,Z,P,Vol\n");
+        if ((rc = write_forces_frame(ctx, forces, 0, cap_nodes, cfg.max_cells, X.data(), Y.data(), Z.data())))
+            return fail("forces file", rc);
+    }
     int frame = 1;
     int step = 0;
     int n = n0;
@@ -228,8 +277,15 @@ int main(int argc, char **argv)
                 }
             });
             buf ^= 1;
+            // forces at the frame, src/GPUbounce.cu:1455-1473
+            if (forces && (rc = write_forces_frame(ctx, forces, step, cap_nodes, cfg.max_cells, nullptr, nullptr,
+                                                   nullptr))) {
+                join_writer();
+                return fail("forces file", rc);
+            }
         }
     }
+    if (forces) fclose(forces);
     if (join_writer()) return fail("trajectory frame", wrc);
     cs3d_get_state(ctx, 0, &n, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
     if (traj) cs3d_traj_close(traj, n);

@@ -292,7 +292,8 @@ def inp_json(p, max_cells, steps, traj_write_int, traj_file="traj.bin", seed=42,
                  "maxPressure": p["max_pressure"], "minPressure": p["min_pressure"],
                  "growth_rate": p["growth_rate"], "checkSphericity": bool(p["check_sphericity"]),
                  "constrainAngles": bool(p["constrain_angles"]), "doAdaptive_dt": False, "dt_max": 1e-4,
-                 "dt_tol": 1e-8, "phase_count": int(p.get("phase_count", 2000000000)), "write_cont_force": False,
+                 "dt_tol": 1e-8, "phase_count": int(p.get("phase_count", 2000000000)),
+                 "write_cont_force": bool(p.get("write_cont_force", False)),
                  "forces_file": "forces.csv", "correct_com": False},
         "counting": {"mit-index_file_name": "mit-index.dat",
                      "count_only_internal_cells?": bool(p.get("count_internal_radius", 0.0) > 0),

@@ -32,6 +32,7 @@ def test_cli_rejects_bad_arguments():
 @pytest.mark.gpu
 def test_cli_trajectory_matches_library(tmp_path, mesh):
     p, st, _ = W.config1()
+    p = dict(p, write_cont_force=1)
     steps, every = 300, 100
     write_mesh_files(str(tmp_path), mesh)
     with open(tmp_path / "inp.json", "w") as f:
@@ -53,6 +54,31 @@ def test_cli_trajectory_matches_library(tmp_path, mesh):
     topo = cs.build_topology(cs.read_fullerene_nn(str(tmp_path)), st["X"][:192], st["Y"][:192], st["Z"][:192])
     sim = cs.Simulation(prm, topo, 256)
     sim.load_state(st["X"], st["Y"], st["Z"], n_cells=n)
+    # the force file (write_cont_force, writeForces src/GPUbounce.cu:2567-2598):
+    # a header, then one row per node at step 0 and at every frame
+    lines = open(tmp_path / "forces.csv").read().splitlines()
+    assert lines[0] == "step,num_cells,cell_ind,node_ind,glob_node_ind,FX,FY,FZ,F,VX,VY,VZ,V,X,Y,Z,P,Vol"
+    rows = {}
+    for ln in lines[1:]:
+        rows.setdefault(int(ln.split(",", 1)[0]), []).append(ln)
+    assert sorted(rows) == [0, 100, 200, 300]
+
+    def expect_rows(step, s, fc, vol, X=None):
+        m = s["n"]
+        X = X if X is not None else (s["X"], s["Y"], s["Z"])
+        out = []
+        for c in range(m):
+            for k in range(180):
+                g = c * 192 + k
+                F = [np.float32(fc[q][g]) for q in ("FCX", "FCY", "FCZ")]
+                V = [np.float32(s[q][g]) for q in ("VX", "VY", "VZ")]
+                mag = lambda a: np.sqrt(np.float32(np.float32(a[0] * a[0] + a[1] * a[1]) + a[2] * a[2]), dtype=np.float32)
+                vals = F + [mag(F)] + V + [mag(V)] + [np.float32(X[q][g]) for q in range(3)] + [s["pressure"][c], vol[c]]
+                out.append("%d,%d,%d,%d,%d," % (step, m, c, k, g) + ",".join("%.8f" % float(v) for v in vals))
+        return out
+
+    s0 = sim.state()
+    assert rows[0] == expect_rows(0, s0, sim.forces(), sim.cells()["volume"], (st["X"], st["Y"], st["Z"]))
     for f in frames[1:]:
         sim.step(every)
         s = sim.state()
@@ -60,6 +86,7 @@ def test_cli_trajectory_matches_library(tmp_path, mesh):
         assert f["X"].shape[0] == m
         for key in ("X", "Y", "Z"):
             assert np.array_equal(f[key].reshape(-1).view(np.uint32), s[key][: m * 192].view(np.uint32)), (f["step"], key)
+        assert rows[f["step"]] == expect_rows(f["step"], s, sim.forces(), sim.cells()["volume"]), f["step"]
     print("cs3d driver: %d frames, %d cells at step %d" % (len(frames), frames[-1]["X"].shape[0], steps))
     sim.close()
 
