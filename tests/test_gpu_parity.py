@@ -270,3 +270,41 @@ def test_correct_com_single_steps(mesh):
     assert abs(float(np.mean(s["X"].reshape(-1, 192)[:, :180]))) < 0.5
     sim.close()
     orc.close()
+
+
+def test_empty_instance_and_empty_system(mesh):
+    """An ensemble instance with no cells steps along with nothing to do and
+    leaves the others unchanged (their cell counts and division events equal
+    the oracle's); a single simulation with no cells steps, too."""
+    insts = []
+    for k, (n, gr) in enumerate([(3, 0.002), (8, 0.001)]):
+        c = W.random_centres(n, 12.0, W.SplitMix(200 + k))
+        p = W.base_params(box_len=(12.0, 12.0, 12.0), growth_rate=gr, rng_ij=k + 5, rng_kl=100 * (k + 5))
+        insts.append((p, W.state(c)))
+    topo, otopo = topo_for(insts[0][1], mesh)
+    empty = np.zeros(0, np.float32)
+    params = [insts[0][0], W.base_params(box_len=(12.0, 12.0, 12.0)), insts[1][0]]
+    ens = cs.Ensemble(params, topo, [32, 32, 32])
+    ens.load_state(0, insts[0][1]["X"], insts[0][1]["Y"], insts[0][1]["Z"], n_cells=insts[0][1]["n"])
+    ens.load_state(1, empty, empty, empty, n_cells=0)
+    ens.load_state(2, insts[1][1]["X"], insts[1][1]["Y"], insts[1][1]["Z"], n_cells=insts[1][1]["n"])
+    ens.step(30)
+    assert ens.n_cells(1) == 0 and len(ens.events(1)) == 0
+    for k in range(3):
+        assert ens.last_error(k) == 0, k
+    assert ens.state(1)["n"] == 0
+    for k, (p, st) in zip((0, 2), insts):
+        o = oracle.System(32, p, otopo)
+        o.load(st["X"], st["Y"], st["Z"], n=st["n"])
+        o.seed(p["rng_ij"], p["rng_kl"])
+        o.init()
+        o.step(30)
+        assert ens.n_cells(k) == o.n
+        assert np.array_equal(ens.events(k), o.events())
+        o.close()
+    ens.close()
+    sim = cs.Simulation(insts[0][0], topo, 8)
+    sim.load_state(empty, empty, empty, n_cells=0)
+    sim.step(5)
+    assert sim.n_cells() == 0 and sim.last_error() == 0
+    sim.close()
