@@ -52,7 +52,6 @@ struct InstState {
     int rebuild;           // list rebuild this step: 0 none, 1 around divisions, 2 whole instance
     float rcur;            // list radius of this step's build
     int mm[2][6];          // grid extents (ordered-int min/max) by step parity
-    float disp_acc;        // displacement bound accumulated since the last rebuild
     unsigned disp_step;    // max node displacement of the current step (float bits)
     int div_count;         // divisions in the current step
     int force_rebuild;

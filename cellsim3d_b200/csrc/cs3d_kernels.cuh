@@ -551,7 +551,6 @@ __global__ void __launch_bounds__(256) k_step_begin(Dev d, int par_next)
         st->rebuild = full ? 2 : part ? 1 : 0;
         st->rcur = full ? P.rlist : P.rlist + 2.0f * ds + 1e-3f;
         st->force_rebuild = 0;
-        st->disp_acc = ds;
         st->div_count = 0;
         if (full || part) {
             if (full) st->rebuilds += 1;
@@ -584,7 +583,6 @@ __global__ void __launch_bounds__(256) k_init_begin(Dev d)
         st->rebuild = 2;
         st->rcur = d.prm[k].rlist;
         st->force_rebuild = 0;
-        st->disp_acc = 0.0f;
         st->disp_step = 0u;
         for (int p = 0; p < 2; ++p)
             for (int q = 0; q < 3; ++q) {

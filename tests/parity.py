@@ -9,7 +9,6 @@ import numpy as np
 
 import cellsim3d_b200 as cs
 import oracle
-from cellsim3d_b200 import workloads as W
 
 TOL = 1e-5   # relative force / velocity tolerance of the parity bar
 

@@ -12,8 +12,8 @@ import cellsim3d_b200 as cs
 import oracle
 from cellsim3d_b200 import workloads as W
 
-from parity import (TOL, force_errors, make_pair, oracle_from, rel_err, single_step_check, snapshot,
-                    sorted_pairs, topo_for)
+from parity import (TOL, force_errors, make_pair, oracle_from, rel_err, single_step_check, sorted_pairs,
+                    topo_for)
 
 pytestmark = pytest.mark.gpu
 

@@ -5,7 +5,6 @@ import os
 import socket
 
 import numpy as np
-import pytest
 
 from cellsim3d_b200 import shard
 from cellsim3d_b200 import workloads as W

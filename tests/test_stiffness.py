@@ -16,7 +16,7 @@ import oracle
 from cellsim3d_b200 import _lib
 from cellsim3d_b200 import workloads as W
 
-from parity import TOL, make_pair, oracle_from, single_step_check, snapshot, topo_for
+from parity import make_pair, single_step_check
 
 
 def _lattice(n_side=3, spacing=2.3, seed=5):
