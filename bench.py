@@ -283,7 +283,8 @@ def run_cs3d(args, world, rank, local):
             "step_roofline": {"achieved": NODE_BYTES * value / 1e9 / world, "frac": NODE_BYTES * value / 1e9 / world / peak},
             "kernels_ms": {k: round(v, 4) for k, v in prof},
             "profiled_step_ms": step_ms,
-            "gpu_launches": int(stats["launches_per_step"]) * args.steps,
+            # every rank launches the same kernel sequence: the whole job's count
+            "gpu_launches": int(stats["launches_per_step"]) * args.steps * world,
             "nl_rebuilds": stats["rebuilds"],
             "max_entries": stats["max_entries"],
             "max_cand": stats["max_cand"],
@@ -302,8 +303,8 @@ def run_cs3d(args, world, rank, local):
                                   "instance_step_ms_p50": ms_max / args.steps,
                                   "instance_step_ms_p99": ms_max / args.steps}
         if e2e:
-            result["e2e"] = {"value": e2e["node_steps"] * world / e2e["seconds"] if world == 1 else
-                             e2e["node_steps"] / e2e["seconds"] * world,
+            # rank 0's end-to-end rate times the ranks (replicas, or equal shares of an ensemble)
+            result["e2e"] = {"value": e2e["node_steps"] / e2e["seconds"] * world,
                              "unit": "node-steps/s", "h2d_bytes_per_step": int(e2e["h2d"]),
                              "d2h_bytes_per_step": int(e2e["d2h"]),
                              "how": "cs3d_load_state of the timed region's starting state from pinned host, "
