@@ -316,6 +316,72 @@ def run_cs3d(args, world, rank, local):
     return result
 
 
+DECADES = ((1, 10), (10, 100), (100, 1000), (1000, 4096))
+
+
+def colony_decades(events, n0, bounds, times_ms):
+    """Node-steps and device time per population decade of a colony run.
+
+    events: (step, parent, daughter) of the run; bounds: the steps at which
+    the population first reached 10, 100, 1000 and 4096 cells (the end of a
+    decade); times_ms: the device time up to each bound.  The cells stepped
+    in step t are those present at its start: n0 plus the divisions of
+    steps < t."""
+    ev_steps = np.asarray([e[0] for e in events], dtype=np.int64)
+    out = {}
+    prev_s, prev_ms = 0, 0.0
+    for (lo, hi), s, ms in zip(DECADES, bounds, times_ms):
+        t = np.arange(prev_s + 1, s + 1)
+        n_start = n0 + np.searchsorted(np.sort(ev_steps), t, side="left")
+        node_steps = float(180 * n_start.sum())
+        dt = (ms - prev_ms) * 1e-3
+        out["%d-%d" % (lo, hi)] = {"steps": int(s - prev_s), "node_steps": node_steps, "seconds": dt,
+                                   "node_steps_per_s": node_steps / dt if dt > 0 else None}
+        prev_s, prev_ms = s, ms
+    return out
+
+
+def run_colony(args):
+    """Config 2: one cell in a box of side 60 grown by division until 4096
+    cells, timed in launches of a few steps (CUDA events); throughput per
+    population decade.  A first pass of args.warmup steps (the step-1
+    division included) captures the step graphs; the colony then starts
+    again from one cell."""
+    import torch
+    import cellsim3d_b200 as cs
+    torch.cuda.set_device(0)
+    (p, st, cap), = build_workload("colony", args.cells)
+    topo = make_topology([(p, st, cap)])
+    sim = cs.Simulation(p, topo, cap)
+    sim.load_state(st["X"], st["Y"], st["Z"], n_cells=st["n"])
+    sim.step(max(args.warmup, 3))
+    sim.load_state(st["X"], st["Y"], st["Z"], n_cells=st["n"])
+    chunk, total, elapsed = 10, 0, 0.0
+    bounds, times = [], []
+    with ClockSampler(0) as clk:
+        while total < args.colony_max_steps and len(bounds) < len(DECADES):
+            sim.step(chunk)
+            total += chunk
+            elapsed += sim.last_step_ms()
+            n = sim.n_cells()
+            while len(bounds) < len(DECADES) and n >= DECADES[len(bounds)][1]:
+                bounds.append(total)
+                times.append(elapsed)
+    events = sim.events()
+    cells_end = sim.n_cells()
+    sim.close()
+    dec = colony_decades(events, st["n"], bounds, times)
+    # every step of the run (a run that stops short of 4096 cells included)
+    node_steps = colony_decades(events, st["n"], [total], [elapsed])["1-10"]["node_steps"]
+    return {"metric": "node-steps/s (cells x 180 x steps / s)", "value": node_steps / (elapsed * 1e-3),
+            "unit": "node-steps/s", "n_gpus": 1, "steps": total, "warmup": args.warmup,
+            "ms_per_step": elapsed / total, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (one cell, cellsim3d_b200/workloads.py config2)",
+            "config": {"workload": "colony", "cells_end": int(cells_end), "capacity": cap,
+                       "timing": "launches of %d steps, CUDA events" % chunk},
+            "decades": dec, "clocks": clk.summary()}
+
+
 def cpu_baseline(args, steps=None, cells=None):
     """The FP64 oracle stepping a bounded sample of the workload on the host."""
     import oracle
@@ -350,6 +416,8 @@ def run_reference(args):
     Without that build, the FP64 oracle port steps a bounded sample on the
     host cores instead."""
     from oracle import ref
+    if args.workload == "colony" and ref.available():
+        return run_reference_colony(args)
     line = {"impl": "reference", "metric": "node-steps/s (cells x 180 x steps / s)", "unit": "node-steps/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "data": "synthetic (seeded generator, cellsim3d_b200/workloads.py)"}
@@ -429,6 +497,37 @@ def run_reference(args):
     return line
 
 
+def run_reference_colony(args):
+    """Config 2 through the reference's own kernels: the harness stops at 4096
+    cells and reports the device time (its guard kernels excluded) at the first
+    step of each population decade."""
+    from oracle import ref
+    import cellsim3d_b200 as cs
+    (p, st, cap), = build_workload("colony", args.cells)
+    topo = make_topology([(p, st, cap)])
+    with ClockSampler(0) as clk:
+        r = ref.run(cs.make_params(p), topo, st, cap, args.colony_max_steps, decades=True)
+    bounds = [m[0] for m in r["marks"]]
+    times = [m[2] for m in r["marks"]]
+    dec = colony_decades(r["events"], st["n"], bounds, times)
+    node_steps = sum(v["node_steps"] for v in dec.values())
+    secs = times[-1] * 1e-3 if times else float("nan")
+    value = node_steps / secs
+    return {"impl": "reference", "metric": "node-steps/s (cells x 180 x steps / s)", "value": value,
+            "unit": "node-steps/s", "n_gpus": args.gpus, "steps": r["steps"], "warmup": 0,
+            "ms_per_step": times[-1] / max(r["steps"], 1) if times else None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (one cell, cellsim3d_b200/workloads.py config2)",
+            "config": {"workload": "colony", "cells_end": int(r["n"]), "capacity": cap},
+            "decades": dec,
+            "reference_build": {"status": r["status_text"], "max_bin_count": r["max_bin"],
+                                "max_cells_per_node_filter": r["max_local_nn"]},
+            "cpu_baseline": {"value": value, "unit": "node-steps/s", "cores": 0, "kind": "reference",
+                             "sample": "no CPU implementation exists: the reference's CUDA kernels on this GPU"},
+            "e2e": {"value": value, "unit": "node-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "clocks": clk.summary()}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -443,6 +542,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--skin", type=float, default=None,
                     help="neighbour-list skin (default: the library's, 0.1)")
+    ap.add_argument("--colony-max-steps", type=int, default=40000,
+                    help="colony: stop after this many steps if 4096 cells are not reached")
     ap.add_argument("--instances", type=int, default=0,
                     help="ensembles: a stratified subset of this many instances (0: all)")
     ap.add_argument("--ref-sample", type=int, default=0,
@@ -457,6 +558,10 @@ def main():
         if rank != 0:
             return
         print(json.dumps(run_reference(args)))
+        return
+    if args.workload == "colony":
+        if rank == 0:
+            print(json.dumps(run_colony(args)))
         return
     res = run_cs3d(args, world, rank, local)
     if rank == 0:

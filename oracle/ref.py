@@ -18,7 +18,9 @@ File formats (little-endian):
           pressure [n], stiffness [n], CM x, y, z [n], int32 n_init, n_first, float32 initial
           FCX..FCZ, FDX..FDZ [n_init*192] when requested, float32 FRX..FRZ [n*192]
           (random force of the last step), int32 n_far, (step, cells) [n_far] of
-          the internal-cells count.
+          the internal-cells count, int32 n_mark, (int32 step, int32 cells, float32 ms)
+          [n_mark]: colony mode (flags bit 1), the device time (guards excluded) at the
+          first step with at least 10, 100, 1000 and 4096 cells; the run ends at 4096.
 """
 import os
 import struct
@@ -60,7 +62,8 @@ def _f32(a, n):
     return a
 
 
-def run(params, topo, state, capacity, steps, dump_init=False, warmup=0, timeout=3600, workdir=None):
+def run(params, topo, state, capacity, steps, dump_init=False, warmup=0, timeout=3600, workdir=None,
+        decades=False):
     """Run the reference for `steps` steps from `state`.
 
     params, topo: ctypes structures with the layout of cs3d_params and
@@ -84,13 +87,17 @@ def run(params, topo, state, capacity, steps, dump_init=False, warmup=0, timeout
             f.write(struct.pack("<2i", C.sizeof(params), C.sizeof(topo)))
             f.write(bytes(params))
             f.write(bytes(topo))
-            f.write(struct.pack("<5i", n, int(capacity), int(steps), 1 if dump_init else 0, int(warmup)))
+            f.write(struct.pack("<5i", n, int(capacity), int(steps), (1 if dump_init else 0) | (2 if decades else 0),
+                                int(warmup)))
             for key in ("X", "Y", "Z", "VX", "VY", "VZ"):
                 a = state.get(key)
                 f.write((_f32(a, k) if a is not None else zeros).tobytes())
             f.write(_f32(press, n).tobytes())
             f.write(_f32(youngs, n).tobytes())
-        p = subprocess.run([BIN, fin, fout], capture_output=True, text=True, timeout=timeout)
+        # modules loaded before the first launch, so that no kernel's first
+        # launch carries its loading time
+        env = dict(os.environ, CUDA_MODULE_LOADING="EAGER")
+        p = subprocess.run([BIN, fin, fout], capture_output=True, text=True, timeout=timeout, env=env)
         if p.returncode != 0:
             raise RuntimeError("cs3d_ref failed (%d): %s" % (p.returncode, p.stderr[-2000:]))
         with open(fout, "rb") as f:
@@ -129,4 +136,8 @@ def run(params, topo, state, capacity, steps, dump_init=False, warmup=0, timeout
     (nfar,) = struct.unpack_from("<i", buf, off)
     off += 4
     out["far"] = np.frombuffer(buf, np.int32, 2 * nfar, off).reshape(nfar, 2).copy()
+    off += 8 * nfar
+    (nmark,) = struct.unpack_from("<i", buf, off)
+    off += 4
+    out["marks"] = [struct.unpack_from("<2if", buf, off + 12 * q) for q in range(nmark)]
     return out

@@ -455,6 +455,12 @@ int main(int argc, char **argv)
     CK(cudaEventCreate(&t1));
     int steps_done = 0;
     if (in.warmup == 0) CK(cudaEventRecord(t0));
+    // flags bit 1: colony mode, device time at the first step with N >= 10, 100,
+    // 1000 and 4096 cells (the population decades), ending at 4096
+    const int marks_at[4] = {10, 100, 1000, 4096};
+    int next_mark = 0;
+    std::vector<int> marks;
+    std::vector<float> mark_ms;
     for (int step = 1; step <= in.steps && status == ST_OK; ++step) {
         const long numNodes = (long)N * 192;
         Integrate<<<N, threadsperblock>>>(d_XP, d_YP, d_ZP, d_X, d_Y, d_Z, d_XM, d_YM, d_ZM, d_vx, d_vy, d_vz, d_time,
@@ -557,6 +563,28 @@ int main(int argc, char **argv)
             CK(cudaGetLastError());
         }
         if (status == ST_OK) steps_done = step;
+        if ((in.flags & 2) && status == ST_OK && next_mark < 4 && N >= marks_at[next_mark]) {
+            // the population reached the next decade: device time so far, guard
+            // kernels excluded; the run ends at the last one
+            cudaEvent_t em;
+            CK(cudaEventCreate(&em));
+            CK(cudaEventRecord(em));
+            CK(cudaEventSynchronize(em));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, t0, em));
+            CK(cudaEventDestroy(em));
+            double g = 0.0;
+            for (size_t q = 0; q + 1 < gev.size(); q += 2) {
+                float gm = 0.f;
+                cudaEventElapsedTime(&gm, gev[q], gev[q + 1]);
+                g += gm;
+            }
+            marks.push_back(step);
+            marks.push_back(N);
+            mark_ms.push_back((float)(ms - g));
+            ++next_mark;
+            if (next_mark == 4) break;
+        }
         if (step == in.warmup) {
             // timed region starts after the warm-up steps: drop their guard events
             CK(cudaDeviceSynchronize());
@@ -620,6 +648,12 @@ int main(int argc, char **argv)
     const int nfar = (int)(far_log.size() / 2);
     fwrite(&nfar, sizeof(int), 1, fo);
     if (nfar) fwrite(far_log.data(), sizeof(int), far_log.size(), fo);
+    const int nmark = (int)mark_ms.size();
+    fwrite(&nmark, sizeof(int), 1, fo);
+    for (int q = 0; q < nmark; ++q) {
+        fwrite(&marks[2 * q], sizeof(int), 2, fo);
+        fwrite(&mark_ms[q], sizeof(float), 1, fo);
+    }
     fclose(fo);
     for (cudaEvent_t e : gev) cudaEventDestroy(e);
     return 0;
