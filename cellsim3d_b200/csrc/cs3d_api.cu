@@ -583,8 +583,16 @@ int cs3d_set_option(cs3d_ctx *c, int option, long long value)
         int4 *p = nullptr;
         if (cudaMalloc(&p, sizeof(int4) * (size_t)value) != cudaSuccess) return CS3D_E_NOMEM;
         c->allocs.push_back(p);
+        int4 *old = c->d.pairs;
         c->d.pairs = p;
         c->d.pair_cap = value;
+        // the previous buffer is released once the work queued on it is done
+        CK(cudaStreamSynchronize(c->stream));
+        const auto it = std::find(c->allocs.begin(), c->allocs.end(), (void *)old);
+        if (it != c->allocs.end()) {
+            c->allocs.erase(it);
+            cudaFree(old);
+        }
         break;
     }
     case CS3D_OPT_SKIN: {
