@@ -344,8 +344,8 @@ int cs3d_get_stats(cs3d_ctx *ctx, long long *stats, int n);
  * receives the average time of each launch slot of a step, names a
  * comma-separated list of their names.  Slots are matched by launch order,
  * so the steps of one call should launch the same kernels: a call that
- * spans the last division step, a softening step or a change of the CoM
- * correction mixes kernels within a slot.  No counterpart in the reference. */
+ * spans the last division step or a softening step mixes kernels within a
+ * slot.  No counterpart in the reference. */
 int cs3d_profile_step(cs3d_ctx *ctx, int n_steps, float *kernel_ms, char *names, int names_len,
                       int max_kernels, int *n_kernels);
 
