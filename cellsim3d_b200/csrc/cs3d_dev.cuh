@@ -121,7 +121,7 @@ struct Dev {
     // node-level spatial hash of the neighbour-list build: cubic bins of
     // edge ~rlist hashed (with the instance) into hsize buckets
     int hsize;          // bucket capacity (>= twice the nodes of the capacity)
-    int *hsz;           // buckets in use this build (whole scan tiles, <= hsize)
+    int *hsz;           // buckets in use by the current list build (whole scan tiles, <= hsize)
     int *hcount;        // [hsize + SCAN_TILE] bucket counts, then exclusive starts
     int *hscan;         // [hsize / SCAN_TILE + 1] tile sums of the scan
     float4 *hpos;       // [cap_total*192] positions sorted by bucket, w = node id bits

@@ -202,7 +202,7 @@ const char *cs3d_strerror(int s)
     case CS3D_E_CONFIG: return "invalid parameter value";
     case CS3D_E_DEVICE_FLAGS: return "a kernel raised an error bit";
     case CS3D_E_CAPACITY: return "population exceeded the allocated capacity";
-    case CS3D_E_UNSUPPORTED: return "feature not supported by this build";
+    case CS3D_E_UNSUPPORTED: return "feature not supported by this library";
     default: return "unknown status";
     }
 }
@@ -419,7 +419,7 @@ int cs3d_config_to_params(const cs3d_config *c, cs3d_params *p)
     p->choose_random_cell_indices = c->choose_random_cell_indices ? 1 : 0;
     p->closeness_to_center = c->closeness_to_center;
     p->count_internal_radius = c->count_only_internal ? c->radius_cutoff : 0.0f;
-    // Features of the reference this build leaves out (all off in the
+    // Features of the reference this library leaves out (all off in the
     // reference's shipped inp.json and in every benchmark configuration).
     // recalc_r0: the reference's CalculateR0 (src/BondKernels.cu:3-37) stores
     // per-cell mean bond lengths into the 3x192 per-bond table d_R0

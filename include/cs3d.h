@@ -38,7 +38,7 @@ extern "C" {
 #define CS3D_E_CAPACITY       -69   /* population exceeded capacity, src/GPUbounce.cu:1265-1270; as in the
                                        reference (which exits), the run ends there: the cells that could
                                        not divide did not take the step's last half kick either */
-#define CS3D_E_UNSUPPORTED     -8   /* feature of the reference outside this build */
+#define CS3D_E_UNSUPPORTED     -8   /* feature of the reference outside this library */
 
 /* ---- device error bits (cs3d_last_error) ------------------------------ */
 #define CS3D_ERRBIT_NAN            0x001u  /* NaN position, src/propagate.cu:241-248 */
@@ -86,7 +86,7 @@ typedef struct cs3d_params {
     /* Langevin random force (rand_params.add_rands, src/propagate.cu:668-678):
      * per node and step rand_scale_factor times three standard normals, used
      * in VelocityUpdateA and the next Integrate with weight sqrt(dt).  The
-     * reference draws them from curand XORWOW states; this build draws them
+     * reference draws them from curand XORWOW states; this library draws them
      * from Philox4x32-10 keyed by rand_seed and counted by (node, step), so
      * only their distribution, not their values, matches the reference. */
     int32_t add_rands;          /* rand_params.add_rands */

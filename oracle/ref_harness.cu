@@ -139,7 +139,7 @@ struct Input {
     std::vector<float> X, Y, Z, VX, VY, VZ, press, youngs;
 };
 
-// The input file must match this build's layout exactly (sizes written by
+// The input file must match this harness's compiled layout exactly (sizes written by
 // the caller and checked here), and every value the reference kernels index
 // with or trap on is validated on the host before any launch: neighbour and
 // face indices in range, symmetric neighbour table, positive finite lengths
@@ -171,7 +171,7 @@ static bool read_input(const char *path, Input &in)
     if (!ok) { fclose(f); return fail_input("bad magic (stale writer or build)"); }
     ok = fread(sizes, sizeof(int), 2, f) == 2 && sizes[0] == (int)sizeof(cs3d_params) &&
          sizes[1] == (int)sizeof(cs3d_topology);
-    if (!ok) { fclose(f); return fail_input("parameter/topology layout differs from this build (rebuild oracle/_ref)"); }
+    if (!ok) { fclose(f); return fail_input("parameter/topology layout differs from this harness (rebuild oracle/_ref)"); }
     ok = fread(&in.p, sizeof in.p, 1, f) == 1 && fread(&in.t, sizeof in.t, 1, f) == 1;
     int hdr[5];
     ok = ok && fread(hdr, sizeof(int), 5, f) == 5;

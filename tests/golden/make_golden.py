@@ -12,7 +12,7 @@ Writes, next to this script:
   ranmar_kat.json -- RANMAR known-answer test from the comment in
                      src/marsaglia.h:66-72 (seeds 1802/9373, values after 20000
                      draws times 4096*4096).
-  traj_small.bin  -- a two-frame binary trajectory written by this build's
+  traj_small.bin  -- a two-frame binary trajectory written by this library's
   traj_small.json    writer, and the frames that scripts/celldiv.py reads back
                      from it (step, frame, cell count, coordinates checksum).
 """

@@ -1,6 +1,6 @@
 """Langevin random force (rand_params.add_rands, src/propagate.cu:668-678).
 
-The reference draws it from curand XORWOW; this build from Philox4x32-10
+The reference draws it from curand XORWOW; this library from Philox4x32-10
 keyed by rand_seed and counted by (node, step).  Only the distribution can
 match the reference: rand_scale_factor times independent standard normals.
 Checked here: the oracle's generator against an independent numpy
