@@ -111,6 +111,19 @@ def dist_env():
     return world, rank, local
 
 
+def reduce_over_ranks(dist, device, maxes, sums):
+    """The maximum of each of `maxes` and the sum of each of `sums` over all
+    ranks (one all-reduce each, the same two calls on every rank); without a
+    process group (`dist` None), the values themselves."""
+    import torch
+    mx = torch.tensor([float(v) for v in maxes], dtype=torch.float64, device=device)
+    sm = torch.tensor([float(v) for v in sums], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    return mx.tolist(), sm.tolist()
+
+
 def _subset(insts, k):
     """A stratified subset by initial cell count: every (n / k)-th instance in size order."""
     if not k or k >= len(insts):
@@ -239,13 +252,11 @@ def run_cs3d(args, world, rank, local):
         e2e = {"seconds": t1 - t0, "node_steps": n_in * 180 * args.steps,
                "h2d": (6 * 4 * n_in * 192 + 8 * n_in) / args.steps,
                "d2h": (6 * 4 * n_out * 192 + 4 * len(insts)) / args.steps + 4 * len(insts)}
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    ns = torch.tensor([node_steps], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(ns, op=dist.ReduceOp.SUM)
-    ms_max = float(t.item())
-    total_node_steps = float(ns.item())
+    # whole job: node-steps summed over ranks, times the slowest rank's; the
+    # end-to-end leg the same way, its copies summed
+    ee = e2e or {"seconds": 0.0, "node_steps": 0.0, "h2d": 0.0, "d2h": 0.0}
+    (ms_max, e2e_s), (total_node_steps, e2e_ns, e2e_h2d, e2e_d2h) = reduce_over_ranks(
+        dist, "cuda", [ms, ee["seconds"]], [node_steps, ee["node_steps"], ee["h2d"], ee["d2h"]])
     result = None
     if rank == 0:
         peak, peak_kind = _peaks()
@@ -303,10 +314,9 @@ def run_cs3d(args, world, rank, local):
                                   "instance_step_ms_p50": ms_max / args.steps,
                                   "instance_step_ms_p99": ms_max / args.steps}
         if e2e:
-            # rank 0's end-to-end rate times the ranks (replicas, or equal shares of an ensemble)
-            result["e2e"] = {"value": e2e["node_steps"] / e2e["seconds"] * world,
-                             "unit": "node-steps/s", "h2d_bytes_per_step": int(e2e["h2d"]),
-                             "d2h_bytes_per_step": int(e2e["d2h"]),
+            result["e2e"] = {"value": e2e_ns / e2e_s,
+                             "unit": "node-steps/s", "h2d_bytes_per_step": int(e2e_h2d),
+                             "d2h_bytes_per_step": int(e2e_d2h),
                              "how": "cs3d_load_state of the timed region's starting state from pinned host, "
                                     "K x cs3d_step(1) with status read-back, cs3d_get_state to host"}
     ens.close()
