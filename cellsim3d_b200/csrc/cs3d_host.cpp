@@ -395,7 +395,7 @@ int cs3d_config_to_params(const cs3d_config *c, cs3d_params *p)
     p->time_interval = c->time_interval;
     p->max_pressure = c->max_pressure;
     p->min_pressure = c->min_pressure;
-    p->growth_rate = c->do_pop_model ? c->growth_rate : c->growth_rate;
+    p->growth_rate = c->growth_rate;   // the population model (doPopModel) is refused below
     p->thresh_dist = c->thresh_dist;
     p->box_len[0] = c->box_len[0];
     p->box_len[1] = c->box_len[1];
