@@ -365,7 +365,7 @@ int cs3d_profile_step(cs3d_ctx *ctx, int n_steps, float *kernel_ms, char *names,
  * the device), or a plugin host that forbids allocation in callbacks.  The
  * caller passes device pointers to inputs and outputs it owns; everything
  * else the kernels need (the contact lists, grids and per-cell data) lives
- * in one file-scope static device array of this library (about 5 MB, held
+ * in one file-scope static device array of this library (4.2 MB, held
  * by every GPU that loads the library until the process exits).
  *
  * Inputs (device, 192-stride SoA as cs3d_load_state): X, Y, Z, VX, VY, VZ
