@@ -182,17 +182,24 @@ typedef struct cs3d_ctx cs3d_ctx;
 
 /* ---- host utilities (no GPU needed) ----------------------------------- */
 
-/* Library version (major*10000 + minor*100 + patch). */
+/* Library version (major*10000 + minor*100 + patch).  No counterpart in the
+ * reference. */
 int cs3d_version(void);
 
-/* Message for a status code. */
+/* Message for a status code.  No counterpart in the reference, which prints
+ * its message and exits. */
 const char *cs3d_strerror(int status);
 
 /* Parse inp.json (// and C comments allowed) and apply the reference's
  * validation.  Replaces read_json_params, src/GPUbounce.cu:1914-2247. */
 int cs3d_config_read_json(const char *path, cs3d_config *out, char *errbuf, int errlen);
 
-/* Hot-path parameters from a parsed config.  Seeds: cs3d_seed_map. */
+/* Hot-path parameters from a parsed config: the conversions the reference
+ * makes after reading the file (stiffness1 = stiffFactor1 x Youngs_mod,
+ * src/GPUbounce.cu:1953; stiffness2 = softStiffFactor x Youngs_mod, :2048;
+ * RANMAR seeds from rand_seed, :1796-1799, see cs3d_seed_map).  Returns
+ * CS3D_E_UNSUPPORTED for features outside this library (population model,
+ * walls, periodic box, adaptive time step, division-plane basis, recalc_r0). */
 int cs3d_config_to_params(const cs3d_config *cfg, cs3d_params *out);
 
 /* Read C180, C180NN, C180C, C180_pentahexa from a directory.  Replaces the
@@ -267,7 +274,9 @@ int cs3d_load_state(cs3d_ctx *ctx, int inst, int n_cells, const float *X, const 
                     const float *pressure, const float *youngs);
 
 /* Replace the RANMAR state of instance inst (e.g. after host-side draws
- * for random placement). */
+ * for random placement).  The reference keeps one RANMAR state per process
+ * in file-scope variables (src/marsaglia.h:50-51); an ensemble has one per
+ * instance, so it is set and read through these two calls. */
 int cs3d_set_rng(cs3d_ctx *ctx, int inst, const cs3d_rng *rng);
 /* Current RANMAR state of instance inst (the stream the divisions draw from). */
 int cs3d_get_rng(cs3d_ctx *ctx, int inst, cs3d_rng *rng);
@@ -277,12 +286,15 @@ int cs3d_get_rng(cs3d_ctx *ctx, int inst, cs3d_rng *rng);
  * error bit (see cs3d_last_error). */
 int cs3d_step(cs3d_ctx *ctx, int n_steps);
 
-/* Read back instance inst.  Any output pointer may be NULL. */
+/* Read back instance inst.  Any output pointer may be NULL.  Replaces the
+ * device-to-host copies before a trajectory frame and the force file,
+ * src/GPUbounce.cu:1447-1449 and :1458-1471. */
 int cs3d_get_state(cs3d_ctx *ctx, int inst, int *n_cells, float *X, float *Y, float *Z,
                    float *VX, float *VY, float *VZ, float *pressure, float *youngs);
 
 /* Conservative (fConList) and dissipative (fDisList) forces of the last
- * evaluation, 192-stride SoA. */
+ * evaluation, 192-stride SoA.  The conservative force is what the force
+ * file (write_cont_force, src/GPUbounce.cu:1456-1473) reads back. */
 int cs3d_get_forces(cs3d_ctx *ctx, int inst, float *FCX, float *FCY, float *FCZ,
                     float *FDX, float *FDY, float *FDZ);
 
@@ -305,15 +317,20 @@ int cs3d_get_far_counts(cs3d_ctx *ctx, int inst, int32_t *out, int max_entries, 
 int cs3d_get_random_force(cs3d_ctx *ctx, int inst, float *FRX, float *FRY, float *FRZ);
 
 /* Per-cell centre of mass (3*n), volume, area and bounding box (6*n:
- * minx maxx miny maxy minz maxz) as of the last step. */
+ * minx maxx miny maxy minz maxz) as of the last step.  The reference reads
+ * back only the volumes (src/GPUbounce.cu:1471); the rest stays on its
+ * device (CenterOfMass, src/centermass.cu:8-50; bounding_boxes,
+ * src/propagatebound.cu:10-205). */
 int cs3d_get_cells(cs3d_ctx *ctx, int inst, float *cm, float *volume, float *area,
                    float *aabb);
 
 /* The neighbour-grid extents (Minx[0..5]) and divisions used by the next
- * force evaluation. */
+ * force evaluation (the reference's minmaxpre/minmaxpost and grid set-up,
+ * src/propagatebound.cu:10-205, whose results stay on the device). */
 int cs3d_get_grid(cs3d_ctx *ctx, int inst, float minmax[6], int divs[3]);
 
-/* Options. */
+/* Options of this library's neighbour lists and pair recording.  No
+ * counterpart in the reference. */
 #define CS3D_OPT_RECORD_PAIRS  1   /* value 0/1: record the contact pairs used */
 #define CS3D_OPT_SKIN          2   /* value = skin length in units of 1e-6 */
 #define CS3D_OPT_PAIR_CAPACITY 3   /* value = max recorded pairs */
@@ -327,13 +344,18 @@ int cs3d_set_option(cs3d_ctx *ctx, int option, long long value);
 int cs3d_get_pairs(cs3d_ctx *ctx, int inst, int kind, int32_t *out, long long max_pairs,
                    long long *count);
 
-/* Division events (step, parent, daughter) since creation. */
+/* Division events (step, parent, daughter) since creation: the cells that
+ * cell_division (src/postscriptinit.cu:148-256) splits each step.  The
+ * reference does not record them. */
 int cs3d_get_events(cs3d_ctx *ctx, int inst, int32_t *out, int max_events, int *count);
 
-/* Error bits raised on the device for instance inst (OR of CS3D_ERRBIT_*). */
+/* Error bits raised on the device for instance inst (OR of CS3D_ERRBIT_*).
+ * Where the reference traps or exits (the bits' comments cite where), this
+ * library sets a bit and the step returns an error status. */
 int cs3d_last_error(cs3d_ctx *ctx, int inst, uint32_t *bits);
 
-/* Counters: [0] steps, [1] neighbour-list rebuilds, [2] max entries per node
+/* Counters of this library's neighbour lists (no counterpart in the
+ * reference): [0] steps, [1] neighbour-list rebuilds, [2] max entries per node
  * seen, [3] max candidate cells per cell seen, [4] kernel launches per step,
  * [5] max distinct contact-candidate nodes (of other cells) per cell seen,
  * [6] cell neighbour lists built (cumulative). */
@@ -388,9 +410,12 @@ int cs3d_forces_static(const cs3d_params *params, const cs3d_topology *topo, int
                        float *FCX, float *FCY, float *FCZ, float *FDX, float *FDY, float *FDZ,
                        void *stream);
 
-/* Device time of the last cs3d_step call (ms, CUDA events). */
+/* Device time of the last cs3d_step call (ms, CUDA events).  No counterpart
+ * in the reference. */
 int cs3d_last_step_ms(cs3d_ctx *ctx, float *ms);
 
+/* Release the context and its device memory.  Replaces the cudaFree block at
+ * the end of main, src/GPUbounce.cu:1549-1566. */
 int cs3d_destroy(cs3d_ctx *ctx);
 
 #ifdef __cplusplus
