@@ -77,7 +77,7 @@ void write_ascii_frame(FILE *f, int step, int interval, int n, const float *X, c
     }
 }
 
-// writeForces, src/GPUbounce.cu:2567-2598: one line per node with the total
+// writeForces, src/GPUbounce.cu:2567-2597: one line per node with the total
 // conservative force, the velocity, the position, and the cell's pressure and
 // volume (the volume of the last division test; 0 before any).
 void write_force_rows(FILE *f, int step, int n, const float *FX, const float *FY, const float *FZ, const float *VX,

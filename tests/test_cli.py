@@ -54,7 +54,7 @@ def test_cli_trajectory_matches_library(tmp_path, mesh):
     topo = cs.build_topology(cs.read_fullerene_nn(str(tmp_path)), st["X"][:192], st["Y"][:192], st["Z"][:192])
     sim = cs.Simulation(prm, topo, 256)
     sim.load_state(st["X"], st["Y"], st["Z"], n_cells=n)
-    # the force file (write_cont_force, writeForces src/GPUbounce.cu:2567-2598):
+    # the force file (write_cont_force, writeForces src/GPUbounce.cu:2567-2597):
     # a header, then one row per node at step 0 and at every frame
     lines = open(tmp_path / "forces.csv").read().splitlines()
     assert lines[0] == "step,num_cells,cell_ind,node_ind,glob_node_ind,FX,FY,FZ,F,VX,VY,VZ,V,X,Y,Z,P,Vol"
