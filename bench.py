@@ -147,8 +147,39 @@ def build_workload(name, cells, seed=123, steps=0, instances=0):
     return _WORKLOADS[key]
 
 
+def workloads():
+    """The seeded input generators (cellsim3d_b200/workloads.py, numpy only),
+    loaded from their file without running the package's __init__, so that
+    the reference arm builds its inputs without importing cellsim3d_b200 or
+    mapping libcs3d.so.  Both arms step the same generated arrays."""
+    mod = sys.modules.get("cs3d_workloads")
+    if mod is None:
+        import importlib.util
+        spec = importlib.util.spec_from_file_location(
+            "cs3d_workloads", os.path.join(ROOT, "cellsim3d_b200", "workloads.py"))
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules["cs3d_workloads"] = mod
+        spec.loader.exec_module(mod)
+    return mod
+
+
+def workload_config(name, insts):
+    """The `config` object of both arms' JSON lines: the workload as generated
+    (initial cells and nodes, instances), the same keys and values in both."""
+    cells = int(sum(st["n"] for _, st, _ in insts))
+    nodes = 180 * cells
+    return {"workload": name, "cells": cells, "nodes": nodes, "instances": len(insts),
+            "parallelism": "instances sharded" if name in ENSEMBLES else "replicas",
+            "l2": "inputs larger than L2 (no flush)" if nodes * 24 > 126e6 else "L2 resident"}
+
+
+PRECISION = ("FP32 state (positions, velocities, forces stored as float); every force term evaluated in "
+             "FP64 from the float state and rounded to float once; FP64 centre of mass, volume and division "
+             "test; float contact decisions with the reference's expressions")
+
+
 def _build_workload(name, cells, seed, steps, instances):
-    from cellsim3d_b200 import workloads as W
+    W = workloads()
     if name == "packed100k":
         c, vel, L = W.packed_fcc(cells, phi=0.5, seed=seed)
         p = W.base_params(box_len=(L, L, L), growth_rate=0.0, min_pressure=200.0, max_pressure=200.0,
@@ -175,7 +206,7 @@ def _build_workload(name, cells, seed, steps, instances):
 
 def make_topology(insts):
     import cellsim3d_b200 as cs
-    from cellsim3d_b200 import workloads as W
+    W = workloads()
     st = insts[0][1]
     return cs.build_topology(cs.mesh_from_arrays(W.load_mesh()), st["X"][:192], st["Y"][:192], st["Z"][:192])
 
@@ -191,6 +222,7 @@ def run_cs3d(args, world, rank, local):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
     insts = build_workload(args.workload, args.cells, steps=args.warmup + args.steps, instances=args.instances)
     n_total = len(insts)
+    config = workload_config(args.workload, insts)
     if args.workload in ENSEMBLES and world > 1:
         # instances shard across ranks by predicted cost, no data-path collective
         from cellsim3d_b200 import shard
@@ -279,10 +311,9 @@ def run_cs3d(args, world, rank, local):
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic (seeded generator, cellsim3d_b200/workloads.py)",
-            "config": {"workload": args.workload, "cells": cells_before, "nodes": int(n_nodes),
-                       "parallelism": "instances sharded" if args.workload in ENSEMBLES else "replicas",
-                       "l2": "inputs larger than L2 (no flush)" if n_nodes * 32 > 126e6 else "L2 resident",
-                       "precision": "FP32 forces/integration, FP64 CoM/volume/division"},
+            "config": config,
+            "precision": PRECISION,
+            "timed_cells": {"start": cells_before, "end": cells_after},
             "roofline": {"bound": "hbm", "kernel": "s1_con_dis", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak,
                          "traffic": S1_TRAFFIC_PER_NODE * n_nodes if args.workload == "packed100k" else None,
@@ -395,7 +426,7 @@ def run_colony(args):
 def cpu_baseline(args, steps=None, cells=None):
     """The FP64 oracle stepping a bounded sample of the workload on the host."""
     import oracle
-    from cellsim3d_b200 import workloads as W
+    W = workloads()
     cells = cells or args.cpu_cells
     insts = build_workload(args.workload, cells)
     # ensembles: the instance of median initial size
@@ -438,10 +469,10 @@ def run_reference(args):
                      "e2e": {"value": base["value"], "unit": "node-steps/s", "h2d_bytes_per_step": 0,
                              "d2h_bytes_per_step": 0}})
         return line
-    import cellsim3d_b200 as cs
     from concurrent.futures import ThreadPoolExecutor
     insts = build_workload(args.workload, args.cells, steps=args.warmup + args.steps)
-    topo = make_topology(insts)
+    config = workload_config(args.workload, insts)
+    mesh = workloads().load_mesh()
     n_all = len(insts)
     insts = _subset(insts, args.ref_sample)
     total_ms, node_steps, cells0 = 0.0, 0.0, 0
@@ -450,7 +481,7 @@ def run_reference(args):
 
     def one(inst):
         p, st, cap = inst
-        return st, ref.run(cs.make_params(p), topo, st, cap, args.warmup + args.steps, warmup=args.warmup)
+        return st, ref.run(p, mesh, st, cap, args.warmup + args.steps, warmup=args.warmup)
 
     with ClockSampler(0) as clk:
         # one simulation after another (device time of each timed region)
@@ -486,11 +517,12 @@ def run_reference(args):
         extra["instance_step_ms_p99"] = float(np.percentile(inst_ms, 99))
     line.update({
         "value": value, "ms_per_step": total_ms / args.steps, "dtype": "f32",
-        "config": {"workload": args.workload, "cells": cells0, "instances": len(insts), "instances_total": n_all,
-                   "instances_run": ("a stratified sample, " if len(insts) < n_all else "") +
-                                    ("one after another and %d at a time (best kept)" % args.ref_concurrency
-                                     if conc is not None else "single system"),
-                   "l2": "inputs larger than L2 (no flush)" if cells0 * 192 * 24 > 126e6 else "L2 resident"},
+        "config": config,
+        "precision": "FP32 (the reference's kernels)",
+        "instances_run": {"instances": len(insts), "cells": cells0, "of": n_all,
+                          "how": ("a stratified sample, " if len(insts) < n_all else "") +
+                                 ("one after another and %d at a time (best kept)" % args.ref_concurrency
+                                  if conc is not None else "single system")},
         "ensemble": extra,
         "reference_build": {"kernels": "src/propagate.cu, centermass.cu, volume.cu, propagatebound.cu, "
                                        "PressureKernels.cu, postscriptinit.cu compiled unmodified for sm_100a "
@@ -512,11 +544,10 @@ def run_reference_colony(args):
     cells and reports the device time (its guard kernels excluded) at the first
     step of each population decade."""
     from oracle import ref
-    import cellsim3d_b200 as cs
     (p, st, cap), = build_workload("colony", args.cells)
-    topo = make_topology([(p, st, cap)])
+    mesh = workloads().load_mesh()
     with ClockSampler(0) as clk:
-        r = ref.run(cs.make_params(p), topo, st, cap, args.colony_max_steps, decades=True)
+        r = ref.run(p, mesh, st, cap, args.colony_max_steps, decades=True)
     bounds = [m[0] for m in r["marks"]]
     times = [m[2] for m in r["marks"]]
     dec = colony_decades(r["events"], st["n"], bounds, times)

@@ -1163,7 +1163,10 @@ __global__ void k_static_store(Dev d, int n, float *FCX, float *FCY, float *FCZ,
 }
 
 // Per-device set-up: resolve the static array's device address and set the
-// kernel attributes the init sequence needs.  Runs once per device.
+// kernel attributes the init sequence needs.  Runs once per device and keeps
+// the address for the life of the process: a cudaDeviceReset (or any other
+// teardown of the device's primary context) invalidates it, and the entry
+// point must not be called on that device afterwards.
 int static_setup(int dev, StaticDevice **out)
 {
     if (dev < 0 || dev >= kMaxDevices) return CS3D_E_ARG;
@@ -1241,6 +1244,9 @@ extern "C" int cs3d_forces_static(const cs3d_params *params, const cs3d_topology
     k_build_work<<<1, 256, 0, s>>>(d);
     k_init_begin<<<1, 256, 0, s>>>(d);
     k_geom<<<sd->grid_cells, SLOTS, 0, s>>>(d, 0);
+    // correct_com at set-up, as run_init (src/GPUbounce.cu:785-805): the shift
+    // moves the positions the wall and contact forces see
+    if (params->correct_com) k_com_shift<<<1, 256, 0, s>>>(d);
     if ((rc = launch_nl_kernels(d, s, sd->grid_nodes, sd->grid_tiles))) return rc;
     k_s1<true><<<sd->grid_cells, SLOTS, sizeof(S1Smem), s>>>(d, 0);
     k_static_store<<<sd->grid_flat, 256, 0, s>>>(d, n_cells, FCX, FCY, FCZ, FDX, FDY, FDZ);

@@ -398,10 +398,14 @@ int cs3d_profile_step(cs3d_ctx *ctx, int n_steps, float *kernel_ms, char *names,
  *
  * The first call on a device resolves the static array's device address
  * (cudaGetSymbolAddress) and sets kernel attributes; make that first call
- * before any stream capture.  Every call shares the one static array, so
- * calls that overlap on the GPU (different streams or host threads) race:
- * serialise them.  The call waits for its kernels and reads back the error
- * word before returning.  Returns CS3D_E_ARG for n_cells outside
+ * before any stream capture.  The address is kept for the life of the
+ * process: after a cudaDeviceReset of that device the entry point must not
+ * be called again.  Every call shares the one static array, so calls that
+ * overlap on the GPU (different streams or host threads) race: serialise
+ * them.  Every call copies the error word back to the host and synchronises
+ * its stream before returning.  With correct_com set, the positions are
+ * shifted by the centre-of-mass correction before the forces are evaluated,
+ * as in cs3d_load_state.  Returns CS3D_E_ARG for n_cells outside
  * [1, CS3D_STATIC_MAX_CELLS] or a NULL required pointer. */
 int cs3d_forces_static(const cs3d_params *params, const cs3d_topology *topo, int n_cells,
                        const float *X, const float *Y, const float *Z,

@@ -4,7 +4,11 @@
 # Test and baseline infrastructure only; the outputs stay out of git.
 #
 #   make -f oracle/ref.mk [REF=/path/to/CellSim3D]
-REF ?= /root/reference
+#
+# REF defaults to $CELLSIM3D_REF, else to a CellSim3D checkout named
+# `reference` beside this repository.
+HERE0 := $(dir $(abspath $(lastword $(MAKEFILE_LIST))))
+REF ?= $(if $(CELLSIM3D_REF),$(CELLSIM3D_REF),$(abspath $(HERE0)../../reference))
 NVCC ?= nvcc
 HERE := $(dir $(abspath $(lastword $(MAKEFILE_LIST))))
 OUT := $(HERE)_ref

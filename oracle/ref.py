@@ -6,9 +6,17 @@ TEST AND BASELINE INFRASTRUCTURE ONLY: the parity tests use it to pin the
 restatement against the reference's own arithmetic, and the benchmark uses it
 to time the reference on the same GPU.  Nothing in the product imports it.
 
+Nothing here loads libcs3d.so or imports cellsim3d_b200: the parameter
+struct and the mesh tables are packed by the ctypes structures below (the
+layouts of cs3d_params and cs3d_topology in include/cs3d.h; the harness checks
+both sizes), and the equilibrium bond lengths and angles are computed by the
+harness itself from cell 0 of the input positions, as the reference's set-up
+does (src/GPUbounce.cu:1890-1908, :909-935).
+
 File formats (little-endian):
   input   "CS3DREF2", int32 sizeof(cs3d_params), sizeof(cs3d_topology),
-          cs3d_params, cs3d_topology (include/cs3d.h),
+          cs3d_params, cs3d_topology (include/cs3d.h; its r0 and theta0 are
+          zero here and are replaced by the harness's own),
           int32 n, capacity, steps, flags (bit 0: dump the initial forces),
           warmup (steps before the timed region),
           float32 X, Y, Z, VX, VY, VZ [n*192], pressure [n], youngs [n]
@@ -41,6 +49,51 @@ STATUS = {0: "ok", 1: "a grid bin held more than 32 cells (clamped)",
           6: "more distinct softer cells requested than exist"}
 
 
+_f, _i = C.c_float, C.c_int32
+
+
+class RefParams(C.Structure):
+    """cs3d_params (include/cs3d.h), field for field."""
+    _fields_ = [(n, _f) for n in (
+        "particle_mass", "repulsion_range", "attraction_range", "repulsion_strength",
+        "attraction_strength", "youngs_mod", "stiffness1", "internal_damping", "viscotic_damping",
+        "gamma_visc", "division_vol", "time_interval", "max_pressure", "min_pressure",
+        "growth_rate", "thresh_dist")] + [("box_len", _f * 3)] + [(n, _i) for n in (
+        "check_sphericity", "constrain_angles", "use_rigid_box", "daught_same_stiffness",
+        "div_time_steps", "rng_ij", "rng_kl", "add_rands")] + [
+        ("rand_scale_factor", _f), ("rand_seed", _i), ("correct_com", _i),
+        ("use_different_stiffnesses", _i), ("stiffness2", _f), ("phase_count", _i),
+        ("soften_after_growth", _i), ("number_of_softer_cells", _i), ("fraction_of_softer_cells", _f),
+        ("choose_random_cell_indices", _i), ("closeness_to_center", _f), ("count_internal_radius", _f)]
+
+
+class RefTopology(C.Structure):
+    """cs3d_topology (include/cs3d.h)."""
+    _fields_ = [("nn", _i * 576), ("sign", _i * 180), ("r0", _f * 576), ("theta0", _f * 576),
+                ("faces", _i * 644)]
+
+
+def pack_params(p):
+    """RefParams from a dict of cs3d_params field names (missing fields 0)."""
+    out = RefParams()
+    for name, _t in RefParams._fields_:
+        if name == "box_len":
+            for k in range(3):
+                out.box_len[k] = float(p["box_len"][k])
+        elif name in p:
+            setattr(out, name, p[name])
+    return out
+
+
+def pack_mesh(mesh):
+    """RefTopology holding the mesh connectivity (neighbours, signs, faces)."""
+    t = RefTopology()
+    C.memmove(t.nn, np.ascontiguousarray(mesh["nn"], dtype=np.int32).ctypes.data, 576 * 4)
+    C.memmove(t.sign, np.ascontiguousarray(mesh["sign"], dtype=np.int32).ctypes.data, 180 * 4)
+    C.memmove(t.faces, np.ascontiguousarray(mesh["faces"], dtype=np.int32).ctypes.data, 644 * 4)
+    return t
+
+
 def available():
     """The harness is built and not older than its sources (a stale build
     would read a different parameter layout; it rejects such input)."""
@@ -50,8 +103,9 @@ def available():
     return all(not os.path.exists(dep) or os.path.getmtime(dep) <= t for dep in _DEPS)
 
 
-def build(ref_root="/root/reference"):
-    """Compile oracle/_ref/cs3d_ref with oracle/ref.mk (needs the reference sources)."""
+def build(ref_root):
+    """Compile oracle/_ref/cs3d_ref with oracle/ref.mk from the reference
+    sources under `ref_root` (the CellSim3D checkout)."""
     subprocess.run(["make", "-s", "-f", os.path.join(HERE, "ref.mk"), "REF=" + ref_root, "-j8"], check=True)
 
 
@@ -62,15 +116,7 @@ def _f32(a, n):
     return a
 
 
-def run(params, topo, state, capacity, steps, dump_init=False, warmup=0, timeout=3600, workdir=None,
-        decades=False):
-    """Run the reference for `steps` steps from `state`.
-
-    params, topo: ctypes structures with the layout of cs3d_params and
-    cs3d_topology; state: dict with X, Y, Z (and optionally VX, VY, VZ,
-    pressure, youngs) and n.  Returns a dict of the output file."""
-    if not available():
-        raise FileNotFoundError(BIN + " not built (make -f oracle/ref.mk)")
+def _write_input(path, params, topo, state, capacity, steps, flags, warmup):
     n = int(state["n"])
     k = n * 192
     zeros = np.zeros(k, np.float32)
@@ -80,20 +126,58 @@ def run(params, topo, state, capacity, steps, dump_init=False, warmup=0, timeout
     youngs = state.get("youngs")
     if youngs is None:
         youngs = np.full(n, params.stiffness1, np.float32)
+    with open(path, "wb") as f:
+        f.write(b"CS3DREF2")
+        f.write(struct.pack("<2i", C.sizeof(params), C.sizeof(topo)))
+        f.write(bytes(params))
+        f.write(bytes(topo))
+        f.write(struct.pack("<5i", n, int(capacity), int(steps), int(flags), int(warmup)))
+        for key in ("X", "Y", "Z", "VX", "VY", "VZ"):
+            a = state.get(key)
+            f.write((_f32(a, k) if a is not None else zeros).tobytes())
+        f.write(_f32(press, n).tobytes())
+        f.write(_f32(youngs, n).tobytes())
+
+
+def tables(params, mesh, state, timeout=120):
+    """The reference's equilibrium bond lengths and angles (float32 r0[576],
+    theta0[576] in the cs3d_topology layout), computed by the harness from
+    cell 0 of `state` with the reference's own host arithmetic.  Makes no CUDA
+    call, so it runs without a GPU."""
+    if not available():
+        raise FileNotFoundError(BIN + " not built (make -f oracle/ref.mk)")
+    P = params if isinstance(params, RefParams) else pack_params(params)
+    with tempfile.TemporaryDirectory() as tmp:
+        fin, fout = os.path.join(tmp, "in.bin"), os.path.join(tmp, "out.bin")
+        _write_input(fin, P, pack_mesh(mesh), state, max(int(state["n"]), 1), 0, 0, 0)
+        p = subprocess.run([BIN, "--tables", fin, fout], capture_output=True, text=True, timeout=timeout)
+        if p.returncode != 0:
+            raise RuntimeError("cs3d_ref --tables failed (%d): %s" % (p.returncode, p.stderr[-2000:]))
+        with open(fout, "rb") as f:
+            buf = f.read()
+    if buf[:8] != b"CS3DREFT" or len(buf) != 8 + 2 * 576 * 4:
+        raise RuntimeError("cs3d_ref --tables: bad output")
+    return (np.frombuffer(buf, np.float32, 576, 8).copy(), np.frombuffer(buf, np.float32, 576, 8 + 576 * 4).copy())
+
+
+def run(params, mesh, state, capacity, steps, dump_init=False, warmup=0, timeout=3600, workdir=None,
+        decades=False):
+    """Run the reference for `steps` steps from `state`.
+
+    params: dict of cs3d_params field names (or a RefParams); mesh: dict with
+    the mesh connectivity arrays nn (3, 192), sign (180) and faces (92, 7);
+    state: dict with X, Y, Z (and optionally VX, VY, VZ, pressure, youngs)
+    and n.  The harness computes R0 and theta0 from cell 0 of the state.
+    Returns a dict of the output file."""
+    if not available():
+        raise FileNotFoundError(BIN + " not built (make -f oracle/ref.mk)")
+    params = params if isinstance(params, RefParams) else pack_params(params)
+    topo = pack_mesh(mesh)
+    n = int(state["n"])
     with tempfile.TemporaryDirectory(dir=workdir) as tmp:
         fin, fout = os.path.join(tmp, "in.bin"), os.path.join(tmp, "out.bin")
-        with open(fin, "wb") as f:
-            f.write(b"CS3DREF2")
-            f.write(struct.pack("<2i", C.sizeof(params), C.sizeof(topo)))
-            f.write(bytes(params))
-            f.write(bytes(topo))
-            f.write(struct.pack("<5i", n, int(capacity), int(steps), (1 if dump_init else 0) | (2 if decades else 0),
-                                int(warmup)))
-            for key in ("X", "Y", "Z", "VX", "VY", "VZ"):
-                a = state.get(key)
-                f.write((_f32(a, k) if a is not None else zeros).tobytes())
-            f.write(_f32(press, n).tobytes())
-            f.write(_f32(youngs, n).tobytes())
+        _write_input(fin, params, topo, state, capacity, steps, (1 if dump_init else 0) | (2 if decades else 0),
+                     warmup)
         # modules loaded before the first launch, so that no kernel's first
         # launch carries its loading time
         env = dict(os.environ, CUDA_MODULE_LOADING="EAGER")

@@ -10,11 +10,14 @@
 // reference on the same GPU; nothing in the product links or calls it.
 //
 // What differs from the reference's main(): the initial state (positions,
-// velocities, per-cell pressure and stiffness) and the mesh tables come from
-// an input file instead of initialize_C180s / the C180* files (the tables are
-// produced by the same construction, src/GPUbounce.cu:1814-1911, :909-938),
-// no trajectory or force files are written, and three host-side guards keep
-// the reference's kernels inside the memory they own:
+// velocities, per-cell pressure and stiffness) and the mesh connectivity
+// (neighbours, orientation signs, faces) come from an input file instead of
+// initialize_C180s / the C180* files.  The equilibrium bond lengths R0 and
+// angles theta0 are not taken from the input: they are computed here from
+// cell 0 of the input positions with the reference's own float3 helpers
+// (inc/VectorFunctions.hpp) and expressions, src/GPUbounce.cu:1890-1908 (R0)
+// and :909-935 (theta0).  No trajectory or force files are written, and three
+// host-side guards keep the reference's kernels inside the memory they own:
 //   * before makeNNlist (host): the grid must fit the per-step clear of the
 //     bin counts (cudaMemset of 1 MiB, src/GPUbounce.cu:1329) and the bin
 //     lists (32 * bins + cells <= MAX_NN * capacity ints); otherwise the run
@@ -41,7 +44,10 @@
 // are asynchronous (no host round trip is added to the step) and their
 // device time, measured with events, is excluded from the timing.
 //
-// Usage: cs3d_ref <in.bin> <out.bin>   (format: oracle/ref.py)
+// Usage: cs3d_ref <in.bin> <out.bin>            (format: oracle/ref.py)
+//        cs3d_ref --tables <in.bin> <out.bin>   R0 and theta0 only ("CS3DREFT",
+//                                               float32 r0[576], theta0[576]);
+//                                               makes no CUDA call
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -151,6 +157,39 @@ static bool fail_input(const char *why)
     return false;
 }
 
+// R0 and theta0 from cell 0 of the input, as the reference's set-up computes
+// them on the host: R0 = mag(a - b) per bond (src/GPUbounce.cu:1890-1908),
+// theta0 = acos of the float dot ratio per vertex angle (:909-935), with the
+// reference's float3 helpers (dot, mag, operator-) from inc/VectorFunctions.hpp,
+// compiled by the same compiler as the reference's host code.  The input's
+// r0 and theta0 are overwritten.
+static void ref_tables(Input &in)
+{
+    const float *X = in.X.data(), *Y = in.Y.data(), *Z = in.Z.data();
+    const int *nn = in.t.nn;
+    memset(in.t.r0, 0, sizeof in.t.r0);
+    memset(in.t.theta0, 0, sizeof in.t.theta0);
+    for (int i = 0; i < 180; ++i) {
+        const float3 a = make_float3(X[i], Y[i], Z[i]);
+        for (int q = 0; q < 3; ++q) {
+            const int nb = nn[q * 192 + i];
+            const float3 b = make_float3(X[nb], Y[nb], Z[nb]);
+            in.t.r0[q * 192 + i] = mag(a - b);
+        }
+    }
+    // theta0 in the angles3 layout {aij, ajk, aik} per node, written as floats
+    float *th = in.t.theta0;
+    for (int n = 0; n < 180; ++n) {
+        const float3 p = make_float3(X[n], Y[n], Z[n]);
+        const float3 ni = make_float3(X[nn[n]], Y[nn[n]], Z[nn[n]]) - p;
+        const float3 nj = make_float3(X[nn[192 + n]], Y[nn[192 + n]], Z[nn[192 + n]]) - p;
+        const float3 nk = make_float3(X[nn[384 + n]], Y[nn[384 + n]], Z[nn[384 + n]]) - p;
+        th[3 * n + 0] = acos(dot(ni, nj) / (mag(ni) * mag(nj)));
+        th[3 * n + 1] = acos(dot(nj, nk) / (mag(nj) * mag(nk)));
+        th[3 * n + 2] = acos(dot(ni, nk) / (mag(ni) * mag(nk)));
+    }
+}
+
 static bool finite_all(const std::vector<float> &v)
 {
     for (float x : v)
@@ -213,11 +252,7 @@ static bool read_input(const char *path, Input &in)
             bool back = false;
             for (int m = 0; m < 3; ++m) back = back || in.t.nn[m * 192 + nb] == i;
             if (!back) return fail_input("neighbour table not symmetric");
-            const float r0 = in.t.r0[q * 192 + i];
-            if (!(r0 > 0 && r0 < 10)) return fail_input("bond length out of range");
         }
-    for (int i = 0; i < 3 * 180; ++i)
-        if (!(in.t.theta0[i] > 0 && in.t.theta0[i] < 3.1416f)) return fail_input("angle out of range");
     for (int i = 0; i < 180; ++i)
         if (in.t.sign[i] != 1 && in.t.sign[i] != -1) return fail_input("bad orientation sign");
     for (int fc = 0; fc < 92; ++fc)
@@ -225,6 +260,15 @@ static bool read_input(const char *path, Input &in)
             const int v = in.t.faces[fc * 7 + m];
             if (v < 0 || v >= 180) return fail_input("face index out of range");
         }
+    // the reference's own equilibrium tables from cell 0 of the input
+    ref_tables(in);
+    for (int q = 0; q < 3; ++q)
+        for (int i = 0; i < 180; ++i) {
+            const float r0 = in.t.r0[q * 192 + i];
+            if (!(r0 > 0 && r0 < 10)) return fail_input("bond length out of range");
+        }
+    for (int i = 0; i < 3 * 180; ++i)
+        if (!(in.t.theta0[i] > 0 && in.t.theta0[i] < 3.1416f)) return fail_input("angle out of range");
     return true;
 }
 
@@ -238,9 +282,24 @@ template <typename T> static T *dev(size_t n)
 
 int main(int argc, char **argv)
 {
-    if (argc != 3) { fprintf(stderr, "usage: %s in.bin out.bin\n", argv[0]); return 1; }
+    const bool tables_only = argc == 4 && strcmp(argv[1], "--tables") == 0;
+    if (argc != 3 && !tables_only) {
+        fprintf(stderr, "usage: %s [--tables] in.bin out.bin\n", argv[0]);
+        return 1;
+    }
+    if (tables_only) { ++argv; }
     Input in;
     if (!read_input(argv[1], in)) { fprintf(stderr, "cs3d_ref: bad input %s\n", argv[1]); return 1; }
+    if (tables_only) {
+        // R0 and theta0 only: no CUDA call, so this runs on a host without a GPU
+        FILE *ft = fopen(argv[2], "wb");
+        if (!ft) { fprintf(stderr, "cs3d_ref: cannot write %s\n", argv[2]); return 1; }
+        fwrite("CS3DREFT", 1, 8, ft);
+        fwrite(in.t.r0, sizeof(float), 576, ft);
+        fwrite(in.t.theta0, sizeof(float), 576, ft);
+        fclose(ft);
+        return 0;
+    }
     const cs3d_params &p = in.p;
     const int cap = in.cap;
     const size_t NS = (size_t)192 * cap;

@@ -107,4 +107,6 @@ def main(root, with_traj=True):
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    main(args[0] if args else "/root/reference", with_traj="--no-traj" not in sys.argv)
+    root = args[0] if args else os.environ.get("CELLSIM3D_REF") or os.path.join(
+        os.path.dirname(os.path.dirname(os.path.dirname(HERE))), "reference")
+    main(root, with_traj="--no-traj" not in sys.argv)

@@ -14,10 +14,16 @@ TOL = 1e-5   # relative force / velocity tolerance of the parity bar
 
 
 def topo_for(st, mesh):
+    """The library's tables (cs3d_topology_build) and the oracle's, each
+    computed independently from cell 0 of the state (the oracle's by its own
+    restatement of src/GPUbounce.cu:1890-1908 and :909-935); they must agree
+    bit for bit."""
     m = cs.mesh_from_arrays(mesh)
     topo = cs.build_topology(m, st["X"][:192], st["Y"][:192], st["Z"][:192])
-    r0 = np.frombuffer(topo.r0, np.float32)
-    th = np.frombuffer(topo.theta0, np.float32)
+    r0, th = oracle.r0_theta0(st["X"][:192], st["Y"][:192], st["Z"][:192], mesh["nn"])
+    assert np.array_equal(np.frombuffer(topo.r0, np.float32).view(np.uint32), r0.view(np.uint32)), "R0 tables differ"
+    assert np.array_equal(np.frombuffer(topo.theta0, np.float32).view(np.uint32), th.view(np.uint32)), \
+        "theta0 tables differ"
     otopo = oracle.make_topo(mesh["nn"], mesh["sign"], r0, th, mesh["faces"])
     return topo, otopo
 

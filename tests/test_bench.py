@@ -68,3 +68,46 @@ def test_whole_job_figures_are_max_time_and_summed_work_over_two_gloo_ranks():
 
 def test_single_process_figures_pass_through():
     assert bench.reduce_over_ranks(None, "cpu", [3.5, 0.0], [1e12, 2.0]) == ([3.5, 0.0], [1e12, 2.0])
+
+
+_REF_INPUTS = r'''
+import os, sys, tempfile
+sys.path.insert(0, sys.argv[1])
+import bench
+from oracle import ref
+insts = bench.build_workload("small8", 100000, steps=8)
+cfg = bench.workload_config("small8", insts)
+mesh = bench.workloads().load_mesh()
+p, st, cap = insts[0]
+with tempfile.TemporaryDirectory() as d:
+    ref._write_input(os.path.join(d, "in.bin"), ref.pack_params(p), ref.pack_mesh(mesh), st, cap, 3, 0, 0)
+    assert os.path.getsize(os.path.join(d, "in.bin")) > 0
+if ref.available():
+    r0, th = ref.tables(p, mesh, st)
+    assert r0.shape == (576,) and th.shape == (576,)
+assert not any(m == "cellsim3d_b200" or m.startswith("cellsim3d_b200.") for m in sys.modules), "package imported"
+maps = open("/proc/self/maps").read()
+assert "libcs3d" not in maps, "libcs3d.so mapped"
+print("CFG", sorted(cfg.items()))
+'''
+
+
+def test_reference_arm_inputs_do_not_load_the_library():
+    """The reference arm builds its inputs (workload arrays, parameter struct,
+    mesh tables, the reference's own R0/theta0) without importing
+    cellsim3d_b200 or mapping libcs3d.so."""
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    p = subprocess.run([sys.executable, "-c", _REF_INPUTS, root], capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr[-3000:]
+    assert "CFG" in p.stdout
+
+
+def test_both_arms_print_the_same_config():
+    """Both arms take `config` from workload_config of the same generated
+    workload, before any sharding or sampling."""
+    for name in ("small8", "packed100k"):
+        a = bench.workload_config(name, bench.build_workload(name, 2000, steps=10))
+        b = bench.workload_config(name, bench.build_workload(name, 2000, steps=10))
+        assert a == b
+        assert set(a) == {"workload", "cells", "nodes", "instances", "parallelism", "l2"}

@@ -85,7 +85,7 @@ def test_population_and_volumes_against_reference_kernels(mesh):
     p, st, _ = W.config2()
     steps = 9000
     topo, _ = topo_for(st, mesh)
-    r = ref.run(cs.make_params(p), topo, st, 2048, steps)
+    r = ref.run(p, mesh, st, 2048, steps)
     assert r["status"] == 0, r["status_text"]
     sim = cs.Simulation(p, topo, 2048)
     sim.load_state(st["X"], st["Y"], st["Z"], n_cells=st["n"])

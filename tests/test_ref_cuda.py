@@ -48,7 +48,7 @@ def test_initial_forces_against_reference_kernels(mesh, case):
     sim, orc = make_pair(p, st, mesh, capacity=cap, record_pairs=False)
     got = sim.forces()
     exact = dict(zip(KEYS, [orc.FC[0], orc.FC[1], orc.FC[2], orc.FD[0], orc.FD[1], orc.FD[2]]))
-    r = ref.run(cs.make_params(p), topo, st, cap, 0, dump_init=True)
+    r = ref.run(p, mesh, st, cap, 0, dump_init=True)
     assert r["status"] == 0, r["status_text"]
     n = st["n"]
     (c_max, c_glob, _), (d_max, d_glob, _) = _errs(got, r["init"], n)
@@ -67,7 +67,7 @@ def test_division_events_against_reference_kernels(mesh):
     events of the first 2000 steps."""
     p, st, _ = W.config1()
     topo, _ = topo_for(st, mesh)
-    r = ref.run(cs.make_params(p), topo, st, 1024, 2000)
+    r = ref.run(p, mesh, st, 1024, 2000)
     assert r["status"] == 0, r["status_text"]
     sim = cs.Simulation(p, topo, 1024)
     sim.load_state(st["X"], st["Y"], st["Z"], n_cells=st["n"])
@@ -84,7 +84,7 @@ def test_first_step_velocities_against_reference_kernels(mesh):
     """Velocities and forces after one full step (8 cells, all dividing)."""
     p, st, _ = W.config1()
     topo, _ = topo_for(st, mesh)
-    r = ref.run(cs.make_params(p), topo, st, 64, 1)
+    r = ref.run(p, mesh, st, 64, 1)
     assert r["status"] == 0, r["status_text"]
     sim = cs.Simulation(p, topo, 64)
     sim.load_state(st["X"], st["Y"], st["Z"], n_cells=st["n"])
@@ -119,7 +119,7 @@ def test_stiffness_schedule_against_reference_kernels(mesh, path):
                                                                              number_of_softer_cells=3)
     p, st = _soft_config1(**over)
     topo, _ = topo_for(st, mesh)
-    r = ref.run(cs.make_params(p), topo, st, 64, 12)
+    r = ref.run(p, mesh, st, 64, 12)
     assert r["status"] == 0, r["status_text"]
     sim = cs.Simulation(p, topo, 64)
     sim.load_state(st["X"], st["Y"], st["Z"], youngs=st["youngs"], n_cells=st["n"])
@@ -156,7 +156,7 @@ def test_correct_com_against_reference_kernels(mesh):
                                        b[k][: n * 192].reshape(n, 192)[:, :180]))) for k in ("X", "Y", "Z"))
 
     for steps in (1, 20):
-        r = ref.run(cs.make_params(p), topo, st, 64, steps)
+        r = ref.run(p, mesh, st, 64, steps)
         assert r["status"] == 0, r["status_text"]
         sim, orc = make_pair(p, st, mesh, 64, record_pairs=False)
         sim.step(steps)
@@ -186,7 +186,7 @@ def test_far_counts_against_reference_kernels(mesh):
                       rng_ij=11, rng_kl=1100)
     st = W.state(c)
     topo, _ = topo_for(st, mesh)
-    r = ref.run(cs.make_params(p), topo, st, 160, 3)
+    r = ref.run(p, mesh, st, 160, 3)
     assert r["status"] == 0, r["status_text"]
     sim = cs.Simulation(p, topo, 160)
     sim.load_state(st["X"], st["Y"], st["Z"], n_cells=st["n"])
@@ -211,7 +211,7 @@ def test_langevin_statistics_against_reference_kernels(mesh):
                       add_rands=1, rand_scale_factor=1.0, rand_seed=17)
     st = W.state(c)
     topo, _ = topo_for(st, mesh)
-    r = ref.run(cs.make_params(p), topo, st, 64, 200)
+    r = ref.run(p, mesh, st, 64, 200)
     assert r["status"] == 0, r["status_text"]
     sim = cs.Simulation(p, topo, 64)
     sim.load_state(st["X"], st["Y"], st["Z"], n_cells=st["n"])
