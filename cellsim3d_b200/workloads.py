@@ -255,16 +255,30 @@ def rsa_centres(n, box, rng, min_dist=1.9, margin=1.05):
     return pts.astype(np.float32)
 
 
-def config5(n_inst=64, master_seed=2025):
+def config5_sizes(n_inst=64, master_seed=2025):
+    """The initial cell counts of config5's instances (no placement)."""
+    sm = SplitMix(master_seed)
+    out = []
+    for _ in range(n_inst):
+        out.append(256 + int(sm.uniform() * (8192 - 256 + 1)))
+        sm.uniform()
+    return out
+
+
+def config5(n_inst=64, master_seed=2025, only=None):
     """64 instances: N0 ~ U{256..8192}, random centres at packing 0.4 of the
     region the centres occupy (box side (N0 (4/3) pi / 0.4)^(1/3) + 2 x 1.05,
     centres at least 1.05 from each wall and 1.9 apart), bond stiffness
-    U[500, 2000] (stiffFactor1 = k/1000), dividing, seeds 1000..1063."""
+    U[500, 2000] (stiffFactor1 = k/1000), dividing, seeds 1000..1063.
+    only: the instance indices to generate (default all), in index order;
+    each is identical to its instance in the full ensemble."""
     sm = SplitMix(master_seed)
     inst = []
     for i in range(n_inst):
         n0 = 256 + int(sm.uniform() * (8192 - 256 + 1))
         k = 500 + 1500 * sm.uniform()
+        if only is not None and i not in only:
+            continue
         box = (n0 * (4.0 / 3.0) * math.pi / 0.4) ** (1.0 / 3.0) + 2 * 1.05
         c = rsa_centres(n0, box, np.random.default_rng([master_seed, i]))
         ij, kl = seed_pair(1000 + i)

@@ -1166,34 +1166,57 @@ void orc_run(orc_sys *s, int nsteps)
 /* (strict cut-off, src/propagate.cu:421), 1 = dissipative (:641).          */
 /* Writes (cell_a, node_i, cell_b, node_j) quadruples; returns the count.   */
 /* ------------------------------------------------------------------------ */
-long orc_pairs(orc_sys *s, int kind, int *out, long maxout)
+/* The pairs of cell a's nodes, in node order and then in the accepted-cell
+ * order of each node; at most `lim` are written to out (NULL: count only). */
+static long pairs_of_cell(const orc_sys *s, int a, int kind, int *out, long lim)
 {
     const float ra = s->P.att_range;
     const float ra2 = ra * ra;
     long cnt = 0;
     int lnn[64];
-    for (int a = 0; a < s->n; ++a)
-        for (int i = 0; i < 180; ++i) {
-            int gi = a * 192 + i;
-            float Xf = s->X[gi], Yf = s->Y[gi], Zf = s->Z[gi];
-            int nl = accepted_cells(s, a, Xf, Yf, Zf, lnn, 64);
-            if (nl > 64) nl = 64;
-            for (int q = 0; q < nl; ++q) {
-                int c = lnn[q];
-                for (int j = 0; j < 180; ++j) {
-                    int gj = c * 192 + j;
-                    float r2 = pair_r2(Xf, Yf, Zf, s->X[gj], s->Y[gj], s->Z[gj]);
-                    int keep = kind == 0 ? (r2 < ra2) : !(r2 > ra2);
-                    if (!keep) continue;
-                    if (cnt < maxout) {
-                        out[4 * cnt + 0] = a; out[4 * cnt + 1] = i;
-                        out[4 * cnt + 2] = c; out[4 * cnt + 3] = j;
-                    }
-                    cnt++;
+    for (int i = 0; i < 180; ++i) {
+        int gi = a * 192 + i;
+        float Xf = s->X[gi], Yf = s->Y[gi], Zf = s->Z[gi];
+        int nl = accepted_cells(s, a, Xf, Yf, Zf, lnn, 64);
+        if (nl > 64) nl = 64;
+        for (int q = 0; q < nl; ++q) {
+            int c = lnn[q];
+            for (int j = 0; j < 180; ++j) {
+                int gj = c * 192 + j;
+                float r2 = pair_r2(Xf, Yf, Zf, s->X[gj], s->Y[gj], s->Z[gj]);
+                int keep = kind == 0 ? (r2 < ra2) : !(r2 > ra2);
+                if (!keep) continue;
+                if (out && cnt < lim) {
+                    out[4 * cnt + 0] = a; out[4 * cnt + 1] = i;
+                    out[4 * cnt + 2] = c; out[4 * cnt + 3] = j;
                 }
+                cnt++;
             }
         }
+    }
     return cnt;
+}
+
+/* Cells are enumerated in parallel (a count pass, a prefix sum, a fill pass);
+ * the output order is the serial order: cell a ascending, then node i, then
+ * the accepted cells of the node in bin order, then node j. */
+long orc_pairs(orc_sys *s, int kind, int *out, long maxout)
+{
+    const int n = s->n;
+    long *off = (long *)malloc(sizeof(long) * ((size_t)n + 1));
+    if (!off) return -1;
+    off[0] = 0;
+    #pragma omp parallel for schedule(dynamic, 8)
+    for (int a = 0; a < n; ++a) off[a + 1] = pairs_of_cell(s, a, kind, NULL, 0);
+    for (int a = 0; a < n; ++a) off[a + 1] += off[a];
+    const long total = off[n];
+    if (out) {
+        #pragma omp parallel for schedule(dynamic, 8)
+        for (int a = 0; a < n; ++a)
+            if (off[a] < maxout) pairs_of_cell(s, a, kind, out + 4 * off[a], maxout - off[a]);
+    }
+    free(off);
+    return total;
 }
 
 /* Diagnostic: worst accepted-cell count of any node (the reference keeps at

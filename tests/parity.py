@@ -89,15 +89,26 @@ def sorted_pairs(a):
     return a[np.argsort(key, kind="stable")]
 
 
-def snapshot(sim):
-    st = sim.state()
-    st.update(sim.forces())
-    st.update(sim.random_force())
-    cells = sim.cells()
+def pair_keys(a):
+    """The pair set (cell_a, node_i, cell_b, node_j) as sorted unique int64
+    keys: equal key arrays mean equal sets (cells < 2^24, nodes < 256)."""
+    a = np.asarray(a)
+    if len(a) == 0:
+        return np.zeros(0, np.int64)
+    key = ((a[:, 0].astype(np.int64) * 256 + a[:, 1]) * (1 << 24) + a[:, 2]) * 256 + a[:, 3]
+    key.sort()
+    return key
+
+
+def snapshot(sim, inst=0):
+    st = sim.state(inst)
+    st.update(sim.forces(inst))
+    st.update(sim.random_force(inst))
+    cells = sim.cells(inst)
     st["cm"] = cells["cm"]
     st["aabb"] = cells["aabb"]
-    st["minmax"] = sim.grid()[0]
-    st["rng"] = sim.get_rng()
+    st["minmax"] = sim.grid(inst)[0]
+    st["rng"] = sim.get_rng(inst)
     st["step"] = sim.stats()["steps"]
     return st
 
@@ -125,67 +136,84 @@ def oracle_from(snap, p, otopo, capacity, record=True):
 def single_step_check(sim, tag="", tol=TOL, check_pairs=True):
     """Step the CUDA path once and the oracle once from the identical state;
     returns a dict of the measured errors after asserting the parity bar."""
-    p, otopo, cap = sim.params, sim.otopo, sim.capacity
-    before = snapshot(sim)
-    O = oracle_from(before, p, otopo, cap, record=check_pairs)
-    sim.step(1)
-    O.step(1)
-    after = snapshot(sim)
-    n = after["n"]
-    res = {"tag": tag, "n": n}
-    # discrete results: cell count, division events of this step, pair sets
-    assert n == O.n, (tag, n, O.n)
-    ev_g = sim.events()
-    ev_g = ev_g[ev_g[:, 0] == after["step"]] if len(ev_g) else ev_g
-    ev_o = O.events()
-    assert np.array_equal(ev_g, ev_o), (tag, "division events", ev_g, ev_o)
-    divided = set(ev_g[:, 1].tolist()) | set(ev_g[:, 2].tolist()) if len(ev_g) else set()
-    if check_pairs:
-        for kind in (0, 1):
-            g = sorted_pairs(sim.pairs(kind))
-            r = sorted_pairs(O.recorded_pairs(kind))
-            assert g.shape == r.shape and np.array_equal(g, r), (tag, "pair set", kind, g.shape, r.shape)
-        res["pairs"] = (len(sorted_pairs(sim.pairs(0))), len(sorted_pairs(sim.pairs(1))))
-    # positions after the drift and the division geometry: bit-exact
-    k = n * 192
-    for a, b in (("X", O.X), ("Y", O.Y), ("Z", O.Z)):
-        assert np.array_equal(after[a][:k].view(np.uint32), b[:k].view(np.uint32)), (tag, "positions", a)
-    # per-cell pressure and bond stiffness: exact
-    assert np.array_equal(after["pressure"][:n].view(np.uint32), O.press[:n].view(np.uint32)), (tag, "pressure")
-    assert np.array_equal(after["youngs"][:n].view(np.uint32), O.E[:n].view(np.uint32)), (tag, "stiffness")
-    cm_o = O.CM[:, :n].T
-    ex = [c for c in range(n)]
-    # conservative force (identical inputs)
-    ec = rel_err([after["FCX"], after["FCY"], after["FCZ"]], [O.FC[0], O.FC[1], O.FC[2]], n)
-    # velocities after the step
-    ev = rel_err([after["VX"], after["VY"], after["VZ"]], [O.VX, O.VY, O.VZ], n)
-    # dissipative force on identical inputs: the CUDA path's own v3 and x,
-    # stale grid of the previous step (cells that divided this step excluded:
-    # their positions changed after the force evaluation)
-    # (with correct_com the positions after the step were shifted after the
-    # force evaluation: the positions at the evaluation are rebuilt from the
-    # state before the step by the integrator's float arithmetic)
-    O2 = oracle_from(before, p, otopo, cap, record=False)
-    if p.get("correct_com"):
-        xs = drift_positions(before, p)
-        O2.X[:k], O2.Y[:k], O2.Z[:k] = xs[0][:k], xs[1][:k], xs[2][:k]
-    else:
-        O2.X[:k], O2.Y[:k], O2.Z[:k] = after["X"][:k], after["Y"][:k], after["Z"][:k]
-    O2.VX[:k], O2.VY[:k], O2.VZ[:k] = after["VX"][:k], after["VY"][:k], after["VZ"][:k]
-    O2._n[0] = n
-    O2.dis_force()
-    fd_ref = O2.FD
-    ed = rel_err([after["FDX"], after["FDY"], after["FDZ"]], [fd_ref[0], fd_ref[1], fd_ref[2]], n,
-                 exclude_cells=sorted(divided))
-    res.update(fc=ec, fd=ed, v=ev, cm_exact=bool(np.array_equal(after["cm"].view(np.uint32), cm_o.view(np.uint32))))
-    print("%-26s n=%5d Fc max %.2e glob %.2e | Fd max %.2e glob %.2e | V max %.2e glob %.2e"
-          % (tag, n, ec[0], ec[1], ed[0], ed[1], ev[0], ev[1]))
-    assert ec[0] < tol and ec[1] < tol, (tag, "Fc", ec)
-    assert ed[0] < tol and ed[1] < tol, (tag, "Fd", ed)
-    assert ev[0] < tol and ev[1] < tol, (tag, "V", ev)
-    O.close()
-    O2.close()
-    return res
+    return ensemble_step_check(sim, [sim.params], [sim.capacity], sim.otopo, [tag], tol, check_pairs)[0]
+
+
+def ensemble_step_check(ens, params, caps, otopo, tags, tol=TOL, check_pairs=True):
+    """One step of every instance of `ens` and of one oracle per instance
+    started from the instance's state (positions, velocities, forces, stale
+    grid, centres of mass, RANMAR state: everything the step reads).  Per
+    instance: cell count, the step's division events, both contact-pair sets,
+    positions, pressures and stiffnesses exactly; the conservative force, the
+    dissipative force and the velocities within `tol`."""
+    n_inst = len(params)
+    before = [snapshot(ens, k) for k in range(n_inst)]
+    Os = [oracle_from(before[k], params[k], otopo, caps[k], record=check_pairs) for k in range(n_inst)]
+    ens.step(1)
+    out = []
+    for k in range(n_inst):
+        p, cap, tag, O = params[k], caps[k], tags[k], Os[k]
+        O.step(1)
+        after = snapshot(ens, k)
+        n = after["n"]
+        res = {"tag": tag, "n": n}
+        # discrete results: cell count, division events of this step, pair sets
+        assert n == O.n, (tag, n, O.n)
+        ev_g = ens.events(k)
+        ev_g = ev_g[ev_g[:, 0] == after["step"]] if len(ev_g) else ev_g
+        ev_o = O.events()
+        assert np.array_equal(ev_g, ev_o), (tag, "division events", ev_g, ev_o)
+        res["events"] = len(ev_o)
+        divided = set(ev_g[:, 1].tolist()) | set(ev_g[:, 2].tolist()) if len(ev_g) else set()
+        if check_pairs:
+            npairs = []
+            for kind in (0, 1):
+                g = pair_keys(ens.pairs(kind, k))
+                r = pair_keys(O.recorded_pairs(kind))
+                assert g.shape == r.shape and np.array_equal(g, r), (tag, "pair set", kind, g.shape, r.shape)
+                npairs.append(len(g))
+            res["pairs"] = tuple(npairs)
+        # positions after the drift and the division geometry: bit-exact
+        kk = n * 192
+        for a, b in (("X", O.X), ("Y", O.Y), ("Z", O.Z)):
+            assert np.array_equal(after[a][:kk].view(np.uint32), b[:kk].view(np.uint32)), (tag, "positions", a)
+        # per-cell pressure and bond stiffness: exact
+        assert np.array_equal(after["pressure"][:n].view(np.uint32), O.press[:n].view(np.uint32)), (tag, "pressure")
+        assert np.array_equal(after["youngs"][:n].view(np.uint32), O.E[:n].view(np.uint32)), (tag, "stiffness")
+        cm_o = O.CM[:, :n].T
+        # conservative force (identical inputs)
+        ec = rel_err([after["FCX"], after["FCY"], after["FCZ"]], [O.FC[0], O.FC[1], O.FC[2]], n)
+        # velocities after the step
+        evv = rel_err([after["VX"], after["VY"], after["VZ"]], [O.VX, O.VY, O.VZ], n)
+        # dissipative force on identical inputs: the CUDA path's own v3 and x,
+        # stale grid of the previous step (cells that divided this step excluded:
+        # their positions changed after the force evaluation)
+        # (with correct_com the positions after the step were shifted after the
+        # force evaluation: the positions at the evaluation are rebuilt from the
+        # state before the step by the integrator's float arithmetic)
+        O2 = oracle_from(before[k], p, otopo, cap, record=False)
+        if p.get("correct_com"):
+            xs = drift_positions(before[k], p)
+            O2.X[:kk], O2.Y[:kk], O2.Z[:kk] = xs[0][:kk], xs[1][:kk], xs[2][:kk]
+        else:
+            O2.X[:kk], O2.Y[:kk], O2.Z[:kk] = after["X"][:kk], after["Y"][:kk], after["Z"][:kk]
+        O2.VX[:kk], O2.VY[:kk], O2.VZ[:kk] = after["VX"][:kk], after["VY"][:kk], after["VZ"][:kk]
+        O2._n[0] = n
+        O2.dis_force()
+        fd_ref = O2.FD
+        ed = rel_err([after["FDX"], after["FDY"], after["FDZ"]], [fd_ref[0], fd_ref[1], fd_ref[2]], n,
+                     exclude_cells=sorted(divided))
+        res.update(fc=ec, fd=ed, v=evv,
+                   cm_exact=bool(np.array_equal(after["cm"].view(np.uint32), cm_o.view(np.uint32))))
+        print("%-26s n=%6d Fc max %.2e glob %.2e | Fd max %.2e glob %.2e | V max %.2e glob %.2e | pairs %s"
+              % (tag, n, ec[0], ec[1], ed[0], ed[1], evv[0], evv[1], res.get("pairs")))
+        assert ec[0] < tol and ec[1] < tol, (tag, "Fc", ec)
+        assert ed[0] < tol and ed[1] < tol, (tag, "Fd", ed)
+        assert evv[0] < tol and evv[1] < tol, (tag, "V", evv)
+        O.close()
+        O2.close()
+        out.append(res)
+    return out
 
 
 def drift_positions(snap, p):

@@ -1,0 +1,166 @@
+"""Parity at the sizes the benchmark runs.
+
+The benchmark's headline workloads, through the C ABI, against the FP64
+oracle on identical float states:
+
+* packed100k: the full 100,000-cell packed system (18M nodes) of the
+  default bench line -- initial forces, and single steps 25 and 1000;
+* ensemble256: a stratified 16-instance subset of the 256-instance ensemble
+  (instances of 1..511 initial cells, as generated for the bench) -- initial
+  forces, 2000 steps with the cell counts and the division events of every
+  instance equal to those of an independently stepped oracle, then one
+  single step of every instance;
+* het64: a stratified 8-instance subset of the 64-instance heterogeneous
+  ensemble (262..8082 initial cells, own stiffness, packing 0.4) -- single
+  steps 1 (every cell divides) and 25 of every instance;
+* colony: one cell grown for 2000 steps, division events equal to the
+  independent oracle's.
+
+Every single-step check (tests/parity.py) asserts the contact-pair sets of
+both cut-offs, the positions, pressures, stiffnesses, cell counts and the
+step's division events exactly, and the conservative force, the dissipative
+force and the velocities within the 1e-5 bar."""
+import os
+import sys
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+import pytest
+
+import cellsim3d_b200 as cs
+import oracle
+from cellsim3d_b200 import workloads as W
+
+from parity import TOL, ensemble_step_check, make_pair, pair_keys, rel_err, single_step_check, topo_for
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+import bench  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def _check_init(tag, sim, orc, inst=0):
+    mm, dv = sim.grid(inst)
+    assert np.array_equal(mm.view(np.uint32), orc.minmax.view(np.uint32)), tag
+    assert tuple(dv) == orc.divs, tag
+    cells = sim.cells(inst)
+    n = orc.n
+    assert np.array_equal(cells["aabb"].view(np.uint32), orc.aabb[:n].view(np.uint32)), tag
+    assert np.array_equal(cells["cm"].view(np.uint32), orc.CM[:, :n].T.copy().view(np.uint32)), tag
+    npairs = []
+    for kind in (0, 1):
+        g = pair_keys(sim.pairs(kind, inst))
+        r = pair_keys(orc.recorded_pairs(kind))
+        assert g.shape == r.shape and np.array_equal(g, r), (tag, "pair set", kind, g.shape, r.shape)
+        npairs.append(len(g))
+    f = sim.forces(inst)
+    ec = rel_err([f["FCX"], f["FCY"], f["FCZ"]], [orc.FC[0], orc.FC[1], orc.FC[2]], n)
+    ed = rel_err([f["FDX"], f["FDY"], f["FDZ"]], [orc.FD[0], orc.FD[1], orc.FD[2]], n)
+    print("%-26s n=%6d Fc max %.2e glob %.2e | Fd max %.2e glob %.2e | pairs %s"
+          % (tag, n, ec[0], ec[1], ed[0], ed[1], tuple(npairs)))
+    assert ec[0] < TOL and ec[1] < TOL and ed[0] < TOL and ed[1] < TOL, (tag, ec, ed)
+
+
+def _advance(sim, target):
+    """Step until the next step is number `target`."""
+    cur = sim.stats()["steps"]
+    if target - 1 > cur:
+        sim.step(target - 1 - cur)
+
+
+def test_packed100k_full_size(mesh):
+    (p, st, cap), = bench.build_workload("packed100k", 100_000)
+    assert st["n"] == 100_000
+    sim, orc = make_pair(p, st, mesh, capacity=cap, pair_capacity=1 << 26)
+    assert orc.err() == 0
+    _check_init("packed100k init", sim, orc)
+    orc.close()
+    for target in (25, 1000):
+        _advance(sim, target)
+        r = single_step_check(sim, "packed100k step %d" % target)
+        assert r["n"] == 100_000 and r["pairs"][0] > 10 ** 6
+    assert sim.last_error() == 0
+    sim.close()
+
+
+def _ensemble(insts, mesh, pair_capacity):
+    topo, otopo = topo_for(insts[0][1], mesh)
+    ens = cs.Ensemble([p for p, _, _ in insts], topo, [cap for _, _, cap in insts])
+    ens.set_option(cs.OPT_PAIR_CAPACITY, pair_capacity)
+    ens.set_option(cs.OPT_RECORD_PAIRS, 1)
+    for k, (p, st, cap) in enumerate(insts):
+        ens.load_state(k, st["X"], st["Y"], st["Z"], st.get("VX"), st.get("VY"), st.get("VZ"), n_cells=st["n"])
+    return ens, otopo
+
+
+def test_ensemble256_subset_full_size(mesh):
+    """The 16-instance stratified subset of the 256-instance ensemble, with
+    the capacities of a long bench run.  The oracles step independently of
+    the CUDA path for 2000 steps (one host thread per instance)."""
+    insts = bench._subset(bench.build_workload("ensemble256", 100_000, steps=2100), 16)
+    assert len(insts) == 16 and max(st["n"] for _, st, _ in insts) >= 500
+    ens, otopo = _ensemble(insts, mesh, 1 << 24)
+    orcs = []
+    for k, (p, st, cap) in enumerate(insts):
+        o = oracle.System(cap, p, otopo)
+        o.load(st["X"], st["Y"], st["Z"], n=st["n"])
+        o.seed(p["rng_ij"], p["rng_kl"])
+        o.set_record(True)
+        o.init()
+        _check_init("ensemble256 inst %d init" % k, ens, o, inst=k)
+        o.set_record(False)
+        orcs.append(o)
+    ens.step(2000)
+    with ThreadPoolExecutor(len(orcs)) as ex:
+        list(ex.map(lambda o: o.step(2000), orcs))
+    n_events = 0
+    for k, o in enumerate(orcs):
+        assert ens.n_cells(k) == o.n, (k, ens.n_cells(k), o.n)
+        eg, eo = ens.events(k), o.events()
+        assert np.array_equal(eg, eo), (k, "division events over 2000 steps", len(eg), len(eo))
+        n_events += len(eo)
+        o.close()
+    print("ensemble256 subset: %d cells after 2000 steps, %d division events, all equal"
+          % (sum(ens.n_cells(k) for k in range(len(insts))), n_events))
+    assert n_events >= sum(st["n"] for _, st, _ in insts)   # every initial cell divides at step 1
+    ensemble_step_check(ens, [p for p, _, _ in insts], [cap for _, _, cap in insts], otopo,
+                        ["ensemble256 inst %d step 2001" % k for k in range(len(insts))])
+    for k in range(len(insts)):
+        assert ens.last_error(k) == 0, k
+    ens.close()
+
+
+def test_het64_subset_full_size(mesh):
+    """The 8-instance stratified subset of the 64-instance heterogeneous
+    ensemble (full-size instances of 262..8082 cells); single steps 1 (every
+    cell divides) and 25."""
+    sizes = W.config5_sizes()
+    picked = [q for q, _, _ in bench._subset([(q, {"n": n}, None) for q, n in enumerate(sizes)], 8)]
+    insts = [(p, st, 2 * st["n"] + 64) for p, st in W.config5(only=set(picked))]
+    assert len(insts) == 8 and max(st["n"] for _, st, _ in insts) > 8000
+    ens, otopo = _ensemble(insts, mesh, 1 << 25)
+    params, caps = [p for p, _, _ in insts], [cap for _, _, cap in insts]
+    r = ensemble_step_check(ens, params, caps, otopo, ["het64 inst %d step 1" % q for q in picked])
+    for res, (_, st, _) in zip(r, insts):
+        assert res["n"] == 2 * st["n"] and res["events"] == st["n"]
+    _advance(ens, 25)
+    ensemble_step_check(ens, params, caps, otopo, ["het64 inst %d step 25" % q for q in picked])
+    for k in range(len(insts)):
+        assert ens.last_error(k) == 0, k
+    ens.close()
+
+
+def test_colony_division_events_2000_steps(mesh):
+    """Config 2 from one cell: the division events of the first 2000 steps of
+    the CUDA path and of the independently stepped oracle."""
+    p, st, cap = W.config2(capacity=512)
+    sim, orc = make_pair(p, st, mesh, capacity=cap, record_pairs=False)
+    sim.step(2000)
+    orc.step(2000)
+    eg, eo = sim.events(), orc.events()
+    print("colony 2000 steps: %d cells, %d division events" % (sim.n_cells(), len(eg)))
+    assert sim.n_cells() == orc.n
+    assert len(eg) >= 1 and np.array_equal(eg, eo)
+    assert sim.last_error() == 0
+    sim.close()
+    orc.close()
