@@ -268,6 +268,23 @@ class Ensemble:
         a["n"] = n
         return a
 
+    def state_async(self, inst, slot, out):
+        """Start reading instance inst back into `out` (a dict of float32
+        arrays X, Y, Z, VX, VY, VZ with room for the capacity and pressure,
+        youngs per cell; any key may be missing) without waiting: the copy
+        overlaps the next steps.  Returns the cell count; the arrays are valid
+        after wait_state(slot).  Page-locked arrays (torch pin_memory, or
+        cs3d_host_alloc) make the copy asynchronous."""
+        n = C.c_int32()
+        get = lambda k: _fp(out[k]) if k in out else None
+        st = _lib.lib().cs3d_get_state_async(self.h, inst, int(slot), C.byref(n), get("X"), get("Y"), get("Z"),
+                                             get("VX"), get("VY"), get("VZ"), get("pressure"), get("youngs"))
+        _lib.check(st, "cs3d_get_state_async")
+        return n.value
+
+    def wait_state(self, slot):
+        _lib.check(_lib.lib().cs3d_wait_state(self.h, int(slot)), "cs3d_wait_state")
+
     def forces(self, inst=0):
         n = self.n_cells(inst)
         k = n * 192

@@ -84,7 +84,8 @@ EXPORTS = [
     "cs3d_create_ensemble", "cs3d_load_state", "cs3d_set_rng", "cs3d_get_rng", "cs3d_step", "cs3d_get_state",
     "cs3d_get_forces", "cs3d_get_random_force", "cs3d_get_cells", "cs3d_get_grid", "cs3d_set_option", "cs3d_get_pairs",
     "cs3d_get_events", "cs3d_get_far_counts", "cs3d_volume_histogram", "cs3d_last_error", "cs3d_get_stats", "cs3d_profile_step", "cs3d_last_step_ms",
-    "cs3d_destroy", "cs3d_forces_static",
+    "cs3d_destroy", "cs3d_forces_static", "cs3d_get_state_async", "cs3d_wait_state", "cs3d_host_alloc",
+    "cs3d_host_free",
 ]
 
 _lib = None
@@ -136,6 +137,10 @@ def lib():
     L.cs3d_get_rng.argtypes = [P, C.c_int, C.POINTER(Rng)]
     L.cs3d_step.argtypes = [P, C.c_int]
     L.cs3d_get_state.argtypes = [P, C.c_int, ip, fp, fp, fp, fp, fp, fp, fp, fp]
+    L.cs3d_get_state_async.argtypes = [P, C.c_int, C.c_int, ip, fp, fp, fp, fp, fp, fp, fp, fp]
+    L.cs3d_wait_state.argtypes = [P, C.c_int]
+    L.cs3d_host_alloc.argtypes = [C.c_size_t, C.POINTER(C.c_void_p)]
+    L.cs3d_host_free.argtypes = [C.c_void_p]
     L.cs3d_get_forces.argtypes = [P, C.c_int, fp, fp, fp, fp, fp, fp]
     L.cs3d_get_random_force.argtypes = [P, C.c_int, fp, fp, fp]
     L.cs3d_get_cells.argtypes = [P, C.c_int, fp, fp, fp, fp]

@@ -42,6 +42,12 @@ struct cs3d_ctx {
     int grid_s2 = 0;               // blocks of S2 and the integrator
     cudaGraphExec_t graph[2][2][2][2] = {};  // [parity][division][integrate first][fused S2]
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // asynchronous read-back (cs3d_get_state_async): a copy stream, two
+    // device staging slots and their events
+    cudaStream_t copy_stream = nullptr;
+    float *astage[2] = {nullptr, nullptr};
+    cudaEvent_t aready[2] = {nullptr, nullptr}, adone[2] = {nullptr, nullptr};
+    bool apending[2] = {false, false};
     float last_ms = 0.f;
     long long launches_per_step = 0;
     unsigned last_err_bits = 0;
@@ -78,6 +84,12 @@ void free_all(cs3d_ctx *c)
             for (auto &e : b)
                 for (cudaGraphExec_t g : e)
                     if (g) cudaGraphExecDestroy(g);
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+    for (int q = 0; q < 2; ++q) {
+        if (c->aready[q]) cudaEventDestroy(c->aready[q]);
+        if (c->adone[q]) cudaEventDestroy(c->adone[q]);
+    }
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     for (void *q : c->allocs) cudaFree(q);
     c->allocs.clear();
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -809,6 +821,79 @@ int cs3d_get_state(cs3d_ctx *c, int inst, int *n_cells, float *X, float *Y, floa
     if (pressure && n) CK(cudaMemcpyAsync(pressure, c->d.press + base, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
     if (youngs && n) CK(cudaMemcpyAsync(youngs, c->d.E + base, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    return CS3D_OK;
+}
+
+int cs3d_get_state_async(cs3d_ctx *c, int inst, int slot, int *n_cells, float *X, float *Y, float *Z, float *VX,
+                         float *VY, float *VZ, float *pressure, float *youngs)
+{
+    if (!c || inst < 0 || inst >= c->n_inst || slot < 0 || slot > 1) return CS3D_E_ARG;
+    cudaSetDevice(c->device);
+    int rc = ensure_init(c);
+    if (rc) return rc;
+    int n = 0;
+    if ((rc = inst_count(c, inst, &n))) return rc;
+    if (n_cells) *n_cells = n;
+    if (!c->copy_stream) CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    if (!c->astage[slot]) {
+        // six node arrays and two per-cell arrays of the whole capacity
+        const size_t words = (size_t)6 * c->cap_total * SLOTS + 2 * (size_t)c->cap_total;
+        float *p = nullptr;
+        if (cudaMalloc(&p, sizeof(float) * words) != cudaSuccess) return CS3D_E_NOMEM;
+        c->allocs.push_back(p);
+        c->astage[slot] = p;
+        CK(cudaEventCreateWithFlags(&c->aready[slot], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&c->adone[slot], cudaEventDisableTiming));
+    }
+    if (n == 0) return CS3D_OK;
+    float *stage = c->astage[slot];
+    // the slot's previous copy must have left the staging buffer
+    if (c->apending[slot]) CK(cudaStreamWaitEvent(c->stream, c->adone[slot], 0));
+    const size_t k = (size_t)n * SLOTS;
+    const size_t off = (size_t)c->hprm[inst].base * SLOTS;
+    const int base = c->hprm[inst].base;
+    const bool wx = X || Y || Z, wv = VX || VY || VZ;
+    if (wx || wv)
+        k_unpack<<<c->grid_flat, 256, 0, c->stream>>>(stage, wx ? c->d.X + off : nullptr, wv ? c->d.V + off : nullptr, k);
+    CK(cudaGetLastError());
+    float *cellv = stage + 6 * k;
+    if (pressure) CK(cudaMemcpyAsync(cellv, c->d.press + base, sizeof(float) * n, cudaMemcpyDeviceToDevice, c->stream));
+    if (youngs) CK(cudaMemcpyAsync(cellv + n, c->d.E + base, sizeof(float) * n, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaEventRecord(c->aready[slot], c->stream));
+    CK(cudaStreamWaitEvent(c->copy_stream, c->aready[slot], 0));
+    float *const out[6] = {X, Y, Z, VX, VY, VZ};
+    for (int q = 0; q < 6; ++q)
+        if (out[q]) CK(cudaMemcpyAsync(out[q], stage + (size_t)q * k, sizeof(float) * k, cudaMemcpyDeviceToHost,
+                                       c->copy_stream));
+    if (pressure) CK(cudaMemcpyAsync(pressure, cellv, sizeof(float) * n, cudaMemcpyDeviceToHost, c->copy_stream));
+    if (youngs) CK(cudaMemcpyAsync(youngs, cellv + n, sizeof(float) * n, cudaMemcpyDeviceToHost, c->copy_stream));
+    CK(cudaEventRecord(c->adone[slot], c->copy_stream));
+    c->apending[slot] = true;
+    return CS3D_OK;
+}
+
+int cs3d_wait_state(cs3d_ctx *c, int slot)
+{
+    if (!c || slot < 0 || slot > 1) return CS3D_E_ARG;
+    if (!c->apending[slot]) return CS3D_OK;
+    cudaSetDevice(c->device);
+    CK(cudaEventSynchronize(c->adone[slot]));
+    c->apending[slot] = false;
+    return CS3D_OK;
+}
+
+int cs3d_host_alloc(size_t bytes, void **ptr)
+{
+    if (!ptr) return CS3D_E_ARG;
+    *ptr = nullptr;
+    if (cudaHostAlloc(ptr, bytes ? bytes : 1, cudaHostAllocDefault) != cudaSuccess) return CS3D_E_NOMEM;
+    return CS3D_OK;
+}
+
+int cs3d_host_free(void *ptr)
+{
+    if (!ptr) return CS3D_OK;
+    CK(cudaFreeHost(ptr));
     return CS3D_OK;
 }
 

@@ -223,19 +223,53 @@ int main(int argc, char **argv)
     int frame = 1;
     int step = 0;
     int n = n0;
-    // Frames are written by a second thread from one of two host buffers
-    // while the GPU steps on (the reference writes them on the step loop's
-    // thread, src/GPUbounce.cu:1430-1470).
-    std::vector<float> WB[2][4];   // X, Y, Z, stiffness per cell
+    // Frames are read back asynchronously into one of two page-locked host
+    // buffers (cs3d_get_state_async: the device-to-host copy runs on a copy
+    // stream while the GPU steps on) and written by a second thread (the
+    // reference reads and writes them on the step loop's thread while the GPU
+    // idles, src/GPUbounce.cu:1430-1475).  Frame k is copied into buffer
+    // k % 2; when frame k + 1 is due, frame k's copy has long landed: it is
+    // handed to the writer thread, and buffer (k + 1) % 2 is free once the
+    // writer of frame k - 1 has finished.
+    float *WB[2][4] = {};   // X, Y, Z per node, stiffness per cell
     for (auto &b : WB)
-        for (auto &v : b) v.assign(cap_nodes, 0.f);
+        for (int q = 0; q < 4; ++q)
+            if ((rc = cs3d_host_alloc(sizeof(float) * (q < 3 ? cap_nodes : (size_t)cfg.max_cells), (void **)&b[q])))
+                return fail("page-locked frame buffers", rc);
+    auto free_buffers = [&]() {
+        cs3d_wait_state(ctx, 0);
+        cs3d_wait_state(ctx, 1);
+        for (auto &b : WB)
+            for (float *&p : b) { cs3d_host_free(p); p = nullptr; }
+    };
     std::thread writer;
     int wrc = 0;
-    int buf = 0;
     auto join_writer = [&]() {
         if (writer.joinable()) writer.join();
         return wrc;
     };
+    struct Pending { bool valid; int slot, step, frame, n; } pend = {false, 0, 0, 0, 0};
+    // hand the pending frame (its copy finished) to the writer thread
+    auto write_pending = [&]() -> int {
+        if (!pend.valid) return 0;
+        int r = cs3d_wait_state(ctx, pend.slot);
+        if (r) return r;
+        if (join_writer()) return wrc;
+        float *const *b = WB[pend.slot];
+        const Pending p = pend;
+        writer = std::thread([&wrc, &prm, traj, ascii, b, p, interval]() {
+            if (traj) {
+                std::vector<int32_t> types;
+                cell_types(prm, p.n, b[3], types);
+                wrc = cs3d_traj_write_frame(traj, p.step, p.frame, p.n, b[0], b[1], b[2], types.data());
+            } else {
+                write_ascii_frame(ascii, p.step, interval, p.n, b[0], b[1], b[2], prm, b[3]);
+            }
+        });
+        pend.valid = false;
+        return 0;
+    };
+    int slot = 0;
     while (step < total_steps) {
         int chunk = interval - step % interval;
         if (step + chunk > total_steps) chunk = total_steps - step;
@@ -243,6 +277,7 @@ int main(int argc, char **argv)
         step += chunk;
         if (rc) {
             join_writer();
+            free_buffers();
             uint32_t bits = 0;
             cs3d_last_error(ctx, 0, &bits);
             fprintf(stderr, "cs3d: step %d: %s (error bits 0x%x)\n", step, cs3d_strerror(rc), bits);
@@ -258,35 +293,42 @@ int main(int argc, char **argv)
         }
         if (step % interval == 0) {
             ++frame;
-            std::vector<float> *b = WB[buf];
-            if ((rc = cs3d_get_state(ctx, 0, &n, b[0].data(), b[1].data(), b[2].data(), nullptr, nullptr, nullptr,
-                                     nullptr, b[3].data()))) {
+            // the previous frame to the writer; its thread then owns that
+            // buffer, and this frame's buffer is free (its writer joined)
+            if ((rc = write_pending())) {
                 join_writer();
+                free_buffers();
+                return fail("trajectory frame", rc);
+            }
+            float *const *b = WB[slot];
+            if ((rc = cs3d_get_state_async(ctx, 0, slot, &n, b[0], b[1], b[2], nullptr, nullptr, nullptr, nullptr,
+                                           b[3]))) {
+                join_writer();
+                free_buffers();
                 return fail("reading the state", rc);
             }
-            if (join_writer()) return fail("trajectory frame", wrc);
-            writer = std::thread([&wrc, &prm, traj, ascii, b, step, frame, interval, nn = n]() {
-                if (traj) {
-                    std::vector<int32_t> types;
-                    cell_types(prm, nn, b[3].data(), types);
-                    wrc = cs3d_traj_write_frame(traj, step, frame, nn, b[0].data(), b[1].data(), b[2].data(),
-                                                types.data());
-                } else {
-                    write_ascii_frame(ascii, step, interval, nn, b[0].data(), b[1].data(), b[2].data(), prm,
-                                      b[3].data());
-                }
-            });
-            buf ^= 1;
+            pend = {true, slot, step, frame, n};
+            slot ^= 1;
             // forces at the frame, src/GPUbounce.cu:1455-1473
             if (forces && (rc = write_forces_frame(ctx, forces, step, cap_nodes, cfg.max_cells, nullptr, nullptr,
                                                    nullptr))) {
                 join_writer();
+                free_buffers();
                 return fail("forces file", rc);
             }
         }
     }
+    if ((rc = write_pending())) {
+        join_writer();
+        free_buffers();
+        return fail("trajectory frame", rc);
+    }
     if (forces) fclose(forces);
-    if (join_writer()) return fail("trajectory frame", wrc);
+    if (join_writer()) {
+        free_buffers();
+        return fail("trajectory frame", wrc);
+    }
+    free_buffers();
     cs3d_get_state(ctx, 0, &n, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
     if (traj) cs3d_traj_close(traj, n);
     if (ascii) fclose(ascii);

@@ -16,6 +16,7 @@
 #ifndef CS3D_H
 #define CS3D_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -291,6 +292,32 @@ int cs3d_step(cs3d_ctx *ctx, int n_steps);
  * src/GPUbounce.cu:1447-1449 and :1458-1471. */
 int cs3d_get_state(cs3d_ctx *ctx, int inst, int *n_cells, float *X, float *Y, float *Z,
                    float *VX, float *VY, float *VZ, float *pressure, float *youngs);
+
+/* Start reading instance inst back without waiting for it, so that the next
+ * cs3d_step overlaps the device-to-host copy (the reference reads each frame
+ * back on its step loop's thread and the GPU idles meanwhile,
+ * src/GPUbounce.cu:1443-1475, WriteBinaryTraj :2446-2477).  The cell count is
+ * read first (a short synchronous read) and stored in *n_cells; the arrays
+ * are then gathered on the context's stream into one of two device staging
+ * slots (slot 0 or 1) and copied to the caller's buffers on a separate copy
+ * stream, one cudaMemcpyAsync per array.  Output pointers may be NULL; they
+ * should be page-locked (cs3d_host_alloc) for the copy to be asynchronous.
+ * The buffers must stay valid and unread until cs3d_wait_state(ctx, slot)
+ * returns.  A later call on the same slot first waits (on the device) for
+ * that slot's previous copy.  No counterpart in the reference. */
+int cs3d_get_state_async(cs3d_ctx *ctx, int inst, int slot, int *n_cells, float *X, float *Y, float *Z,
+                         float *VX, float *VY, float *VZ, float *pressure, float *youngs);
+
+/* Wait until the copies started by cs3d_get_state_async on `slot` have
+ * landed in the caller's buffers.  Returns CS3D_OK at once if none is
+ * pending.  No counterpart in the reference. */
+int cs3d_wait_state(cs3d_ctx *ctx, int slot);
+
+/* Page-locked host memory for cs3d_get_state_async and cs3d_load_state
+ * (cudaHostAlloc / cudaFreeHost), for callers that do not link the CUDA
+ * runtime themselves.  No counterpart in the reference. */
+int cs3d_host_alloc(size_t bytes, void **ptr);
+int cs3d_host_free(void *ptr);
 
 /* Conservative (fConList) and dissipative (fDisList) forces of the last
  * evaluation, 192-stride SoA.  The conservative force is what the force

@@ -72,6 +72,8 @@ def lib():
         L.orc_set_record.argtypes = [P, C.c_int]
         L.orc_recorded_pairs.restype = C.c_long
         L.orc_recorded_pairs.argtypes = [P, C.c_int, C.POINTER(C.c_int), C.c_long]
+        L.orc_accepted.restype = C.c_long
+        L.orc_accepted.argtypes = [P, C.POINTER(C.c_int), C.c_long]
         L.orc_max_local_nn.restype = C.c_int
         L.orc_max_local_nn.argtypes = [P]
         L.orc_forces_subset.argtypes = [P, C.POINTER(C.c_int), C.c_int]
@@ -343,6 +345,24 @@ class System:
         cnt = lib().orc_recorded_pairs(self.h, kind, None, 0)
         out = np.zeros((max(cnt, 1), 4), dtype=np.int32)
         lib().orc_recorded_pairs(self.h, kind, _ip(out), cnt)
+        return out[:cnt]
+
+    def bins(self):
+        """The oracle's current grid bins (makeNNlist, src/propagatebound.cu:209-263):
+        a list of int arrays, the cells of each bin in ascending order."""
+        L = lib()
+        nb = L.orc_ptr_i(self.h, 13)[0]
+        start = np.ctypeslib.as_array(L.orc_ptr_i(self.h, 11), shape=(nb + 1,)).copy()
+        total = int(start[nb])
+        cells = np.ctypeslib.as_array(L.orc_ptr_i(self.h, 12), shape=(max(total, 1),))[:total].copy()
+        return [cells[start[b]:start[b + 1]] for b in range(nb)]
+
+    def accepted(self):
+        """(cell, node, accepted cell) triples of every node with the current
+        stale grid (src/propagate.cu:356-404)."""
+        cnt = lib().orc_accepted(self.h, None, 0)
+        out = np.zeros((max(cnt, 1), 3), dtype=np.int32)
+        lib().orc_accepted(self.h, _ip(out), cnt)
         return out[:cnt]
 
     def max_local_nn(self):

@@ -289,6 +289,7 @@ int *orc_ptr_i(orc_sys *s, int which)
     case 5: return &s->max_bin_count; case 6: return &s->max_local_nn;
     case 7: return &s->ydiv; case 8: return &s->zdiv;
     case 9: return &s->nfar; case 10: return s->far;
+    case 11: return s->bin_start; case 12: return s->bin_cells; case 13: return &s->nbins;
     default: return NULL;
     }
 }
@@ -1214,6 +1215,44 @@ long orc_pairs(orc_sys *s, int kind, int *out, long maxout)
         #pragma omp parallel for schedule(dynamic, 8)
         for (int a = 0; a < n; ++a)
             if (off[a] < maxout) pairs_of_cell(s, a, kind, out + 4 * off[a], maxout - off[a]);
+    }
+    free(off);
+    return total;
+}
+
+/* The accepted cells of every node (the cells of the node's stale bin that
+ * pass the stale box filter, src/propagate.cu:356-404, uncapped): (cell_a,
+ * node_i, cell_c) triples in cell, node, bin order; returns the count. */
+static long accepted_of_cell(const orc_sys *s, int a, int *out, long lim)
+{
+    long cnt = 0;
+    int lnn[64];
+    for (int i = 0; i < 180; ++i) {
+        int gi = a * 192 + i;
+        int nl = accepted_cells(s, a, s->X[gi], s->Y[gi], s->Z[gi], lnn, 64);
+        if (nl > 64) nl = 64;
+        for (int q = 0; q < nl; ++q) {
+            if (out && cnt < lim) { out[3 * cnt] = a; out[3 * cnt + 1] = i; out[3 * cnt + 2] = lnn[q]; }
+            cnt++;
+        }
+    }
+    return cnt;
+}
+
+long orc_accepted(orc_sys *s, int *out, long maxout)
+{
+    const int n = s->n;
+    long *off = (long *)malloc(sizeof(long) * ((size_t)n + 1));
+    if (!off) return -1;
+    off[0] = 0;
+    #pragma omp parallel for schedule(dynamic, 8)
+    for (int a = 0; a < n; ++a) off[a + 1] = accepted_of_cell(s, a, NULL, 0);
+    for (int a = 0; a < n; ++a) off[a + 1] += off[a];
+    const long total = off[n];
+    if (out) {
+        #pragma omp parallel for schedule(dynamic, 8)
+        for (int a = 0; a < n; ++a)
+            if (off[a] < maxout) accepted_of_cell(s, a, out + 3 * off[a], maxout - off[a]);
     }
     free(off);
     return total;

@@ -28,7 +28,10 @@ File formats (little-endian):
           (random force of the last step), int32 n_far, (step, cells) [n_far] of
           the internal-cells count, int32 n_mark, (int32 step, int32 cells, float32 ms)
           [n_mark]: colony mode (flags bit 1), the device time (guards excluded) at the
-          first step with at least 10, 100, 1000 and 4096 cells; the run ends at 4096.
+          first step with at least 10, 100, 1000 and 4096 cells; the run ends at 4096;
+          int32 n_grid, then when n_grid > 0 (flags bit 2) the reference's grid after
+          its first makeNNlist: float32 Minx[6], int32 Xdiv, Ydiv, Zdiv, nbins,
+          counts [nbins], lists [32*nbins], float32 bounding boxes [6*n_grid].
 """
 import os
 import struct
@@ -161,7 +164,7 @@ def tables(params, mesh, state, timeout=120):
 
 
 def run(params, mesh, state, capacity, steps, dump_init=False, warmup=0, timeout=3600, workdir=None,
-        decades=False):
+        decades=False, dump_grid=False):
     """Run the reference for `steps` steps from `state`.
 
     params: dict of cs3d_params field names (or a RefParams); mesh: dict with
@@ -176,8 +179,8 @@ def run(params, mesh, state, capacity, steps, dump_init=False, warmup=0, timeout
     n = int(state["n"])
     with tempfile.TemporaryDirectory(dir=workdir) as tmp:
         fin, fout = os.path.join(tmp, "in.bin"), os.path.join(tmp, "out.bin")
-        _write_input(fin, params, topo, state, capacity, steps, (1 if dump_init else 0) | (2 if decades else 0),
-                     warmup)
+        _write_input(fin, params, topo, state, capacity, steps,
+                     (1 if dump_init else 0) | (2 if decades else 0) | (4 if dump_grid else 0), warmup)
         # modules loaded before the first launch, so that no kernel's first
         # launch carries its loading time
         env = dict(os.environ, CUDA_MODULE_LOADING="EAGER")
@@ -224,4 +227,18 @@ def run(params, mesh, state, capacity, steps, dump_init=False, warmup=0, timeout
     (nmark,) = struct.unpack_from("<i", buf, off)
     off += 4
     out["marks"] = [struct.unpack_from("<2if", buf, off + 12 * q) for q in range(nmark)]
+    off += 12 * nmark
+    (ngrid,) = struct.unpack_from("<i", buf, off)
+    off += 4
+    if ngrid:
+        minx = np.frombuffer(buf, np.float32, 6, off).copy()
+        off += 24
+        xdiv, ydiv, zdiv, nbins = struct.unpack_from("<4i", buf, off)
+        off += 16
+        counts = np.frombuffer(buf, np.int32, nbins, off).copy()
+        off += 4 * nbins
+        lists = np.frombuffer(buf, np.int32, 32 * nbins, off).reshape(nbins, 32).copy()
+        off += 128 * nbins
+        bb = np.frombuffer(buf, np.float32, 6 * ngrid, off).reshape(ngrid, 6).copy()
+        out["grid"] = {"minx": minx, "divs": (xdiv, ydiv, zdiv), "counts": counts, "lists": lists, "bb": bb}
     return out

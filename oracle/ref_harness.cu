@@ -473,6 +473,23 @@ int main(int argc, char **argv)
     // initialisation, src/GPUbounce.cu:739-763 and :978-1004
     CenterOfMass<<<N, 256>>>(N, d_X, d_Y, d_Z, d_CMx, d_CMy, d_CMz);
     status = grid();
+    // flags bit 2: the reference's own grid after this first makeNNlist (bin
+    // counts, bin lists, bounding boxes, extents), read back as it left them
+    std::vector<int> g_counts, g_list;
+    std::vector<float> g_bb;
+    float g_minx[6] = {0, 0, 0, 0, 0, 0};
+    int g_div[4] = {0, 0, 0, 0};
+    if ((in.flags & 4) && status == ST_OK) {
+        CK(cudaDeviceSynchronize());
+        g_counts.resize(nbins);
+        g_list.resize((size_t)32 * nbins);
+        g_bb.resize((size_t)6 * N);
+        CK(cudaMemcpy(g_counts.data(), d_NoofNNlist, sizeof(int) * nbins, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(g_list.data(), d_NNlist, sizeof(int) * 32 * nbins, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(g_bb.data(), d_bb, sizeof(float) * 6 * N, cudaMemcpyDeviceToHost));
+        memcpy(g_minx, Minx, sizeof g_minx);
+        g_div[0] = Xdiv; g_div[1] = Ydiv; g_div[2] = Zdiv; g_div[3] = (int)nbins;
+    }
     if (p.correct_com) {
         // src/GPUbounce.cu:783-805
         CenterOfMass<<<N, 256>>>(N, d_X, d_Y, d_Z, d_CMx, d_CMy, d_CMz);
@@ -712,6 +729,15 @@ int main(int argc, char **argv)
     for (int q = 0; q < nmark; ++q) {
         fwrite(&marks[2 * q], sizeof(int), 2, fo);
         fwrite(&mark_ms[q], sizeof(float), 1, fo);
+    }
+    const int ngrid = (int)g_bb.size() / 6;
+    fwrite(&ngrid, sizeof(int), 1, fo);
+    if (ngrid) {
+        fwrite(g_minx, sizeof(float), 6, fo);
+        fwrite(g_div, sizeof(int), 4, fo);
+        fwrite(g_counts.data(), sizeof(int), g_counts.size(), fo);
+        fwrite(g_list.data(), sizeof(int), g_list.size(), fo);
+        fwrite(g_bb.data(), sizeof(float), g_bb.size(), fo);
     }
     fclose(fo);
     for (cudaEvent_t e : gev) cudaEventDestroy(e);

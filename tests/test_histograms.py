@@ -108,3 +108,57 @@ def test_population_and_volumes_against_reference_kernels(mesh):
     assert ks.pvalue > 1e-3
     sim.close()
     other.close()
+
+
+@pytest.mark.parametrize("config,steps", [("config1", 5000), ("config2", 8000)])
+def test_statistics_across_seeds_against_reference_kernels(mesh, config, steps):
+    """Beyond the first 2000 steps the FP32 reference and this library (FP64
+    force terms) separate chaotically, so the comparison is statistical, as
+    scripts/pop.py analyses a run: eight seeds (RANMAR (s, 100 s), s = 1..8)
+    of the same configuration run by the reference's own kernels and by the
+    CUDA path.  Two-sample KS tests on the pooled final cell volumes (every
+    cell of every seed, computed by the same device function), on the final
+    populations of the eight seeds, and on the populations at every 500th
+    step of all seeds pooled; the mean final populations agree within 15 %."""
+    from oracle import ref
+    from scipy import stats
+    if not ref.available():
+        pytest.skip("oracle/_ref/cs3d_ref not built")
+    p0, st, _ = getattr(W, config)()
+    topo, _ = topo_for(st, mesh)
+    cap = 2048
+    checkpoints = np.arange(500, steps + 1, 500)
+    pops, pops_ref, vols, vols_ref, curve, curve_ref = [], [], [], [], [], []
+    for s in range(1, 9):
+        p = dict(p0, rng_ij=s, rng_kl=100 * s)
+        r = ref.run(p, mesh, st, cap, steps)
+        assert r["status"] == 0, (s, r["status_text"])
+        sim = cs.Simulation(p, topo, cap)
+        sim.load_state(st["X"], st["Y"], st["Z"], n_cells=st["n"])
+        sim.step(steps)
+        pop = sim.population(0)
+        born = np.bincount(r["events"][:, 0], minlength=steps + 1)[: steps + 1]
+        pop_ref = st["n"] + np.cumsum(born)
+        other = cs.Simulation(p, topo, cap)
+        other.load_state(r["X"], r["Y"], r["Z"], n_cells=r["n"])
+        _, v1 = sim.volume_histogram(lo=0.0, hi=12.0, nbins=24, volumes=True)
+        _, v2 = other.volume_histogram(lo=0.0, hi=12.0, nbins=24, volumes=True)
+        pops.append(int(pop[-1]))
+        pops_ref.append(int(pop_ref[-1]))
+        curve.extend(pop[checkpoints].tolist())
+        curve_ref.extend(pop_ref[checkpoints].tolist())
+        vols.extend(v1.tolist())
+        vols_ref.extend(v2.tolist())
+        assert sim.last_error() == 0, s
+        sim.close()
+        other.close()
+    ks_v = stats.ks_2samp(vols, vols_ref)
+    ks_p = stats.ks_2samp(pops, pops_ref)
+    ks_c = stats.ks_2samp(curve, curve_ref)
+    print("%s, 8 seeds x %d steps: final populations %s (reference %s); KS p: volumes %.3f (%d / %d cells), "
+          "final populations %.3f, populations every 500 steps %.3f"
+          % (config, steps, pops, pops_ref, ks_v.pvalue, len(vols), len(vols_ref), ks_p.pvalue, ks_c.pvalue))
+    assert ks_v.pvalue > 1e-3
+    assert ks_p.pvalue > 1e-3
+    assert ks_c.pvalue > 1e-3
+    assert abs(np.mean(pops) - np.mean(pops_ref)) <= 0.15 * np.mean(pops_ref)

@@ -235,3 +235,81 @@ def test_langevin_statistics_against_reference_kernels(mesh):
         assert abs(a.mean()) < 0.05 and abs(a.std() - 1.0) < 0.03
     assert abs(v_ours.std() / v_ref.std() - 1.0) < 0.15
     sim.close()
+
+
+def _reference_accepted(st, n, g, ra):
+    """(cell, node, accepted cell) of every node from the reference's own grid
+    (bin lists, bounding boxes, extents read back after its makeNNlist), with
+    the reference's float expressions for the node's bin and the box filter
+    (src/propagate.cu:360-392), in float32 operation by operation."""
+    f32 = np.float32
+    DL = f32(2.9)
+    X = np.stack([st[k][: n * 192].reshape(n, 192)[:, :180] for k in ("X", "Y", "Z")], -1).astype(f32)
+    divs = g["divs"]
+    idx = []
+    for d in range(3):
+        s = ((X[..., d] - f32(g["minx"][2 * d])) / DL).astype(f32)
+        s = np.trunc(s).astype(np.int64)
+        idx.append(np.clip(s, 0, divs[d] - 1))
+    b = idx[2] * divs[0] * divs[1] + idx[1] * divs[0] + idx[0]
+    bb = g["bb"]
+    ra2 = f32(f32(ra) * f32(ra))
+    # every (node, cell of the node's bin) pair, vectorised
+    bflat = b.reshape(-1)
+    cnt = g["counts"][bflat]
+    node = np.repeat(np.arange(n * 180), cnt)
+    start = np.repeat(np.cumsum(cnt) - cnt, cnt)
+    slot = np.arange(len(node)) - start
+    cell = g["lists"][bflat[node], slot]
+    a = node // 180
+    keep = cell != a
+    node, cell, a = node[keep], cell[keep], a[keep]
+    Xn = X.reshape(-1, 3)[node]
+    dd = []
+    for d in range(3):
+        x = Xn[:, d]
+        u = (x - bb[cell, 2 * d + 1]).astype(f32)
+        w = (bb[cell, 2 * d] - x).astype(f32)
+        dd.append(((u > 0).astype(f32) * u + (w > 0).astype(f32) * w).astype(f32))
+    r2 = ((dd[0] * dd[0]).astype(f32) + (dd[1] * dd[1]).astype(f32)).astype(f32) + (dd[2] * dd[2]).astype(f32)
+    ok = ~(r2.astype(f32) > ra2)
+    return list(zip(a[ok].tolist(), (node[ok] % 180).tolist(), cell[ok].tolist()))
+
+
+@pytest.mark.parametrize("case", ["config1", "packed500"])
+def test_candidate_stage_against_the_reference_grid(mesh, case):
+    """The reference's own grid after its first makeNNlist
+    (src/propagatebound.cu:10-263: bounding boxes, extents, bin lists, read
+    back from its device buffers) against the oracle's and the CUDA path's:
+    boxes, extents and divisions bit for bit, every bin the same set of cells
+    (the reference fills bins in atomic order), and the per-node accepted
+    cells derived from the reference's bins (src/propagate.cu:356-404) equal
+    to the oracle's.  The CUDA path's contact pairs at this step equal the
+    oracle's (pair-set parity), so they come from the reference's
+    candidates."""
+    import oracle
+    from parity import pair_keys
+    p, st, cap = CASES[case]()
+    n = st["n"]
+    r = ref.run(p, mesh, st, cap, 0, dump_grid=True)
+    assert r["status"] == 0 and r["max_bin"] <= 32, r["status_text"]
+    g = r["grid"]
+    sim, O = make_pair(p, st, mesh, capacity=cap)
+    assert np.array_equal(g["minx"].view(np.uint32), O.minmax.view(np.uint32))
+    assert tuple(g["divs"]) == tuple(O.divs)
+    assert np.array_equal(g["bb"].view(np.uint32), O.aabb[:n].view(np.uint32))
+    mm, dv = sim.grid()
+    assert np.array_equal(mm.view(np.uint32), g["minx"].view(np.uint32)) and tuple(dv) == tuple(g["divs"])
+    assert np.array_equal(sim.cells()["aabb"].view(np.uint32), g["bb"].view(np.uint32))
+    bins = O.bins()
+    assert len(bins) == len(g["counts"])
+    for b_, cells in enumerate(bins):
+        assert sorted(g["lists"][b_, : g["counts"][b_]].tolist()) == cells.tolist(), b_
+    acc_ref = sorted(_reference_accepted(st, n, g, p["attraction_range"]))
+    acc_orc = sorted(map(tuple, O.accepted().tolist()))
+    print("%s: %d bins, %d (node, accepted cell) entries from the reference's grid" % (case, len(bins), len(acc_ref)))
+    assert acc_ref == acc_orc
+    for kind in (0, 1):
+        assert np.array_equal(pair_keys(sim.pairs(kind)), pair_keys(O.recorded_pairs(kind)))
+    sim.close()
+    O.close()
