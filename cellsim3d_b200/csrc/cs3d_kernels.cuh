@@ -155,10 +155,12 @@ __device__ __forceinline__ void sincos_small(double x, double &s, double &c)
             x2 * (1.0 / 479001600 + x2 * (-1.0 / 87178291200.0 + x2 / 20922789888000.0)))))));
 }
 
-__device__ __forceinline__ void angle_pair(float3 P, float3 Q, float th0f, double c0, double s0, double3 &Fp,
-                                           double3 &Fq)
+__device__ __forceinline__ void angle_pair(float3 Pe, float3 Qe, float3 x, float th0f, double c0, double s0,
+                                           double3 &Fp, double3 &Fq)
 {
-    const double px = P.x, py = P.y, pz = P.z, qx = Q.x, qy = Q.y, qz = Q.z;
+    // arms from the vertex x to the two end nodes: differences of floats, exact in FP64
+    const double px = (double)Pe.x - x.x, py = (double)Pe.y - x.y, pz = (double)Pe.z - x.z;
+    const double qx = (double)Qe.x - x.x, qy = (double)Qe.y - x.y, qz = (double)Qe.z - x.z;
     const double idk = px * qx + py * qy + pz * qz;
     const double rp2 = px * px + py * py + pz * pz;
     const double rq2 = qx * qx + qy * qy + qz * qz;
@@ -272,16 +274,17 @@ __device__ __forceinline__ unsigned entry_at(const uint16_t *ep, const uint32_t 
 
 // ---------------------------------------------------------------------------
 // S1 contact sweep of node i over its entries: conservative contact force
-// (strict cut-off, src/propagate.cu:406-442) added to F, tangential
-// velocity sum of the dissipative pairs (non-strict cut-off,
-// src/propagate.cu:600-656) in vt.  Returns the mask of the entries that are
-// dissipative pairs (positions do not change before S2, so S2 reuses it).
+// (strict cut-off, src/propagate.cu:406-442) added to F, sum of the velocity
+// differences v_i - v_j of the dissipative pairs (non-strict cut-off,
+// src/propagate.cu:600-656) in vsum (its tangential part is taken once, by
+// tangential()).  Lists the dissipative pairs for S2 (positions do not change
+// before S2) and returns their number.
 // Partner positions and velocities are read from global memory (L1/L2
 // resident: the partners of a cell are a few hundred nodes).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int sweep_s1(const Dev &d, const InstParams &P, const SlotData &sd, int a, int i, float3 x,
-                                        float3 v, float3 nrm, int ne, const uint32_t (&pre)[EPRE / 2], double &FX,
-                                        double &FY, double &FZ, double3 &vt)
+                                        float3 v, int ne, const uint32_t (&pre)[EPRE / 2], double &FX,
+                                        double &FY, double &FZ, double3 &vsum)
 {
     const uint16_t *ep = d.ent + (size_t)a * MAXE * SLOTS + i;
     uint16_t *dl = d.dlist + (size_t)a * MAXD * SLOTS + i;
@@ -317,16 +320,18 @@ __device__ __forceinline__ int sweep_s1(const Dev &d, const InstParams &P, const
                                               r2 < P.ra2 ? 3 : 2, 0);
             }
             if (r2 < P.ra2) {
-                // distance in FP64: (rr - R) cancels for stiff repulsion
-                const double R2 = (double)dx * dx + (double)dy * dy + (double)dz * dz;
+                // distance in FP64 from the exact difference of the float
+                // positions: (rr - R) cancels for stiff repulsion
+                const double ex = (double)x.x - xj[q].x, ey = (double)x.y - xj[q].y, ez = (double)x.z - xj[q].z;
+                const double R2 = ex * ex + ey * ey + ez * ez;
                 const double iR = rsqrt_nr(R2);
                 const double R = R2 * iR;
                 double k = 0.0;
                 if (R < (double)P.ra) k += -(double)P.asE * ((double)P.ra - R) * iR;
                 if (R <= (double)P.rr) k += (double)P.rsE * ((double)P.rr - R) * iR;
-                FX += k * dx;
-                FY += k * dy;
-                FZ += k * dz;
+                FX += k * ex;
+                FY += k * ey;
+                FZ += k * ez;
             }
         }
         float4 vj[SB];
@@ -336,19 +341,18 @@ __device__ __forceinline__ int sweep_s1(const Dev &d, const InstParams &P, const
         for (int q = 0; q < SB; ++q) {
             if (id[q] < 0) continue;
             // velocity differences of floats are exact in FP64
-            const double vx = (double)v.x - vj[q].x, vy = (double)v.y - vj[q].y, vz = (double)v.z - vj[q].z;
-            const double dn = vx * nrm.x + vy * nrm.y + vz * nrm.z;
-            vt.x += vx - dn * nrm.x;
-            vt.y += vy - dn * nrm.y;
-            vt.z += vz - dn * nrm.z;
+            vsum.x += (double)v.x - vj[q].x;
+            vsum.y += (double)v.y - vj[q].y;
+            vsum.z += (double)v.z - vj[q].z;
         }
     }
     return nd;
 }
 
-// S2 sweep: tangential velocity sum over the dissipative pairs found by S1
-// (their list, in column layout), with the velocities after the half kicks.
-__device__ __forceinline__ double3 sweep_s2(const Dev &d, const int *cell, int a, int i, float3 v, float3 nrm, int nd)
+// S2 sweep: sum of the velocity differences over the dissipative pairs found
+// by S1 (their list, in column layout), with the velocities after the half
+// kicks; tangential() takes its tangential part.
+__device__ __forceinline__ double3 sweep_s2(const Dev &d, const int *cell, int a, int i, float3 v, int nd)
 {
     const uint16_t *dl = d.dlist + (size_t)a * MAXD * SLOTS + i;
     double3 vt = make_double3(0.0, 0.0, 0.0);
@@ -364,25 +368,30 @@ __device__ __forceinline__ double3 sweep_s2(const Dev &d, const int *cell, int a
 #pragma unroll
         for (int q = 0; q < SB; ++q) {
             if (e[q] == 0xffffu) continue;
-            const double vx = (double)v.x - vj[q].x, vy = (double)v.y - vj[q].y, vz = (double)v.z - vj[q].z;
-            const double dn = vx * nrm.x + vy * nrm.y + vz * nrm.z;
-            vt.x += vx - dn * nrm.x;
-            vt.y += vy - dn * nrm.y;
-            vt.z += vz - dn * nrm.z;
+            vt.x += (double)v.x - vj[q].x;
+            vt.y += (double)v.y - vj[q].y;
+            vt.z += (double)v.z - vj[q].z;
         }
     }
     return vt;
 }
 
-// Unit surface normal of node i for the tangential friction,
-// src/propagate.cu:558-572.
-__device__ __forceinline__ float3 node_normal(const float4 *xs, int n0, int n1, int n2, float sgn)
+// Tangential part of the friction sum, src/propagate.cu:558-656: the
+// reference adds v_ij - (v_ij . n) n over the dissipative pairs of node i, with
+// n the unit normal of the surface at i, sign * unit((x_N2 - x_N1) x (x_N3 -
+// x_N1)).  The projection is linear in v_ij, so the sweeps sum the velocity
+// differences alone (S) and this applies it once: S - (S . n) n.  The normal
+// is formed in FP64 from exact differences of the float positions.
+__device__ __forceinline__ double3 tangential(const float4 *xs, int n0, int n1, int n2, float sgn, double3 S)
 {
-    float3 A = sub3(f3(xs[n1]), f3(xs[n0]));
-    float3 B = sub3(f3(xs[n2]), f3(xs[n0]));
-    float3 nrm = make_float3(A.y * B.z - A.z * B.y, A.z * B.x - A.x * B.z, A.x * B.y - A.y * B.x);
-    float nin = 1.0f / sqrtf(nrm.x * nrm.x + nrm.y * nrm.y + nrm.z * nrm.z);
-    return make_float3(sgn * (nin * nrm.x), sgn * (nin * nrm.y), sgn * (nin * nrm.z));
+    const float4 p0 = xs[n0], p1 = xs[n1], p2 = xs[n2];
+    const double ax = (double)p1.x - p0.x, ay = (double)p1.y - p0.y, az = (double)p1.z - p0.z;
+    const double bx = (double)p2.x - p0.x, by = (double)p2.y - p0.y, bz = (double)p2.z - p0.z;
+    const double cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
+    const double s = (double)sgn * rsqrt_nr(cx * cx + cy * cy + cz * cz);
+    const double nx = s * cx, ny = s * cy, nz = s * cz;
+    const double dn = S.x * nx + S.y * ny + S.z * nz;
+    return make_double3(S.x - dn * nx, S.y - dn * ny, S.z - dn * nz);
 }
 
 // Dissipative force, src/propagate.cu:546-658: bond damping with the three
@@ -742,17 +751,17 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
         const float3 v = f3(v4);
         // bond angles: thread = vertex, three angles each
         if (P.angles && i < NODES) {
-            float3 pa = sub3(f3(sm.xs[n0]), x), pb = sub3(f3(sm.xs[n1]), x), pc = sub3(f3(sm.xs[n2]), x);
+            const float3 pa = f3(sm.xs[n0]), pb = f3(sm.xs[n1]), pc = f3(sm.xs[n2]);
             const double2 *cs0 = d.topo.cs0 + 3 * i;
             const float4 th = __ldg(&d.topo.th0[i]);
             // angles (n0, n1), (n1, n2), (n0, n2); arm ends summed by destination
             double3 F01p, F01q, F12p, F12q, F02p, F02q;
             double2 t0 = __ldg(&cs0[0]);
-            angle_pair(pa, pb, th.x, t0.x, t0.y, F01p, F01q);
+            angle_pair(pa, pb, x, th.x, t0.x, t0.y, F01p, F01q);
             t0 = __ldg(&cs0[1]);
-            angle_pair(pb, pc, th.y, t0.x, t0.y, F12p, F12q);
+            angle_pair(pb, pc, x, th.y, t0.x, t0.y, F12p, F12q);
             t0 = __ldg(&cs0[2]);
-            angle_pair(pa, pc, th.z, t0.x, t0.y, F02p, F02q);
+            angle_pair(pa, pc, x, th.z, t0.x, t0.y, F02p, F02q);
             const int o = i * 3;
             sm.arm.x[o] = F01p.x + F02p.x; sm.arm.y[o] = F01p.y + F02p.y; sm.arm.z[o] = F01p.z + F02p.z;
             sm.arm.x[o + 1] = F01q.x + F12p.x; sm.arm.y[o + 1] = F01q.y + F12p.y; sm.arm.z[o + 1] = F01q.z + F12p.z;
@@ -772,18 +781,19 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
             const int nbr[3] = {n0, n1, n2};
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                const float3 dd = sub3(f3(sm.xs[nbr[k]]), x);
-                const double iR = rsqrt_nr((double)dd.x * dd.x + (double)dd.y * dd.y + (double)dd.z * dd.z);
+                // exact FP64 differences of the float positions
+                const float4 xn = sm.xs[nbr[k]];
+                const double ex = (double)xn.x - x.x, ey = (double)xn.y - x.y, ez = (double)xn.z - x.z;
+                const double iR = rsqrt_nr(ex * ex + ey * ey + ez * ez);
                 const double c = stiff * (__ldg(&d.topo.r0i[3 * i + k]) - iR);
-                FX += c * dd.x; FY += c * dd.y; FZ += c * dd.z;
+                FX += c * ex; FY += c * ey; FZ += c * ez;
             }
             // internal pressure, src/propagate.cu:318-330 (CM of the previous step)
             {
                 const float4 cm = d.CM[a];
-                const float3 r = make_float3(x.x - cm.x, x.y - cm.y, x.z - cm.z);
-                const double c = 3.0 * (double)d.press[a] *
-                                 rsqrt_nr((double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z);
-                FX += c * r.x; FY += c * r.y; FZ += c * r.z;
+                const double rx = (double)x.x - cm.x, ry = (double)x.y - cm.y, rz = (double)x.z - cm.z;
+                const double c = 3.0 * (double)d.press[a] * rsqrt_nr(rx * rx + ry * ry + rz * rz);
+                FX += c * rx; FY += c * ry; FZ += c * rz;
             }
             // bond angles, src/propagate.cu:81-181: the vertex terms (minus
             // the arm forces of the angles at i) and the arm terms (the arm
@@ -796,9 +806,9 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
                 FZ += sm.arm.z[am.x] + sm.arm.z[am.y] + sm.arm.z[am.z] - (sm.arm.z[o] + sm.arm.z[o + 1] + sm.arm.z[o + 2]);
             }
             // contacts, src/propagate.cu:356-442 and the first dissipative sweep
-            const float3 nrm = node_normal(sm.xs, n0, n1, n2, sgn);
-            double3 vt = make_double3(0.0, 0.0, 0.0);
-            const int nd = sweep_s1(d, P, sm.sd, a, i, x, v, nrm, ne, pre, FX, FY, FZ, vt);
+            double3 vsum = make_double3(0.0, 0.0, 0.0);
+            const int nd = sweep_s1(d, P, sm.sd, a, i, x, v, ne, pre, FX, FY, FZ, vsum);
+            const double3 vt = tangential(sm.xs, n0, n1, n2, sgn, vsum);
             if (nd > MAXD) atomic_or_err(&d.st[inst], CS3D_ERRBIT_ENTRY_OVERFLOW);
             // rigid box walls, src/propagate.cu:474-510 (float gap tests)
             if (P.rigid) {
@@ -931,8 +941,7 @@ __global__ void __launch_bounds__(SLOTS, 5) k_s2(Dev d, int par)
         float3 fdk = make_float3(0.f, 0.f, 0.f);
         if (i < NODES) {
             const float3 v = f3(v4);
-            const float3 nrm = node_normal(sm.xs, n0, n1, n2, sgn);
-            const double3 vt = sweep_s2(d, sm.cell, a, i, v, nrm, nd);
+            const double3 vt = tangential(sm.xs, n0, n1, n2, sgn, sweep_s2(d, sm.cell, a, i, v, nd));
             const float3 fd = dis_force(P, sm.vs, n0, n1, n2, v, vt);
             d.FD[g] = make_float4(fd.x, fd.y, fd.z, 0.f);
             fdk = fd;
