@@ -107,7 +107,7 @@ def test_ensemble256_subset_full_size(mesh):
       different floats (about one value in 1e8); in a dense dividing colony a
       one-ulp difference grows until a division happens a step earlier or
       later.  The first step at which an instance's events differ is
-      printed."""
+      printed, and must be later than step 400."""
     insts = bench._subset(bench.build_workload("ensemble256", 100_000, steps=2100), 16)
     assert len(insts) == 16 and max(st["n"] for _, st, _ in insts) >= 500
     params, caps = [p for p, _, _ in insts], [cap for _, _, cap in insts]
@@ -159,7 +159,12 @@ def test_ensemble256_subset_full_size(mesh):
           % (sum(ens.n_cells(k) for k in range(len(insts))), window_events,
              sorted(zip(n0, first_diff), key=lambda t: t[0])))
     assert window_events >= sum(n0)   # every initial cell divides at step 1
+    # Deterministic inputs and code give the same divergence steps on every
+    # run; on one B200 the earliest was step 478 (an instance of 275 initial
+    # cells) and instances of up to 5 cells never diverged.  The assertion
+    # keeps a margin below the earliest.
     for k in range(len(insts)):
+        assert first_diff[k] is None or first_diff[k] > 400, (n0[k], first_diff[k])
         orcs[k].close()
     ensemble_step_check(ens, params, caps, otopo, ["ensemble256 inst %d step 2001" % k for k in range(len(insts))])
     for k in range(len(insts)):
