@@ -349,32 +349,17 @@ __device__ __forceinline__ int sweep_s1(const Dev &d, const InstParams &P, const
     return nd;
 }
 
-// S2 sweep: sum of the velocity differences over the dissipative pairs found
-// by S1 (their list, in column layout), with the velocities after the half
-// kicks; tangential() takes its tangential part.
-__device__ __forceinline__ double3 sweep_s2(const Dev &d, const int *cell, int a, int i, float3 v, int nd)
-{
-    const uint16_t *dl = d.dlist + (size_t)a * MAXD * SLOTS + i;
-    double3 vt = make_double3(0.0, 0.0, 0.0);
-    for (int k0 = 0; k0 < nd; k0 += SB) {
-        unsigned e[SB];
-#pragma unroll
-        for (int q = 0; q < SB; ++q) e[q] = k0 + q < nd ? dl[(size_t)(k0 + q) * SLOTS] : 0xffffu;
-        float4 vj[SB];
-#pragma unroll
-        for (int q = 0; q < SB; ++q)
-            vj[q] = e[q] != 0xffffu ? __ldg(&d.Vb[cell[e[q] >> 8] * SLOTS + (int)(e[q] & 255u)])
-                                    : make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-        for (int q = 0; q < SB; ++q) {
-            if (e[q] == 0xffffu) continue;
-            vt.x += (double)v.x - vj[q].x;
-            vt.y += (double)v.y - vj[q].y;
-            vt.z += (double)v.z - vj[q].z;
-        }
-    }
-    return vt;
-}
+// S2 sweep over the dissipative pairs S1 listed, one (node, pair) item at a
+// time.  A node has 0 to ~30 pairs (about one on average), so a loop per node
+// leaves most lanes idle; instead the cell's items (every pair of every node,
+// node-major, list order within a node) are numbered by a prefix sum of the
+// pair counts and dealt out to all 192 threads, S2_IPT per thread per chunk.
+// Each item leaves v_i - v_j (velocities after the half kicks) in shared
+// memory and the node's own thread adds its items in list order, so the FP64
+// sum has a fixed order; tangential() takes its tangential part.
+constexpr int S2_IPT = 2;                    // items per thread per chunk
+constexpr int S2_CHUNK = S2_IPT * SLOTS;     // items per chunk
+constexpr int S2_MAXITEMS = NODES * MAXD;    // dissipative pairs of one cell, at most
 
 // Tangential part of the friction sum, src/propagate.cu:558-656: the
 // reference adds v_ij - (v_ij . n) n over the dissipative pairs of node i, with
@@ -866,6 +851,10 @@ struct S2Smem {
     int cell[MAXC];
     GeomScratch gs;
     int dflag;   // the cell divides (division steps)
+    double3 c[S2_CHUNK];             // v_i - v_j of each item of a chunk
+    short off[SLOTS];                // each node's first item
+    uint8_t inode[S2_MAXITEMS];      // the node of each item
+    int wsum[SLOTS / 32];
 };
 
 // Integrate + ForwardTime of the next step (src/propagate.cu:681-763) on the
@@ -932,16 +921,61 @@ __global__ void __launch_bounds__(SLOTS, 5) k_s2(Dev d, int par)
         const size_t g = (size_t)a * SLOTS + i;
         float4 x4 = make_float4(0, 0, 0, 0), v4 = make_float4(0, 0, 0, 0);
         int nd = 0;
-        if (i < NODES) { x4 = d.X[g]; v4 = d.Vb[g]; nd = d.ndis[g]; }
+        if (i < NODES) { x4 = d.X[g]; v4 = d.Vb[g]; nd = min((int)d.ndis[g], MAXD); }
         if (i < MAXC) sm.cell[i] = d.cand[(size_t)a * MAXC + i];
         sm.xs[i] = x4;
         sm.vs[i] = v4;
+        // items of the cell: warp-inclusive scan of the pair counts
+        const int lane = i & 31, wid = i >> 5;
+        int incl = nd;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) sm.wsum[wid] = incl;
         __syncthreads();
+        int off = incl - nd, n_items = 0;
+#pragma unroll
+        for (int q = 0; q < SLOTS / 32; ++q) {
+            const int ws = sm.wsum[q];
+            off += q < wid ? ws : 0;
+            n_items += ws;
+        }
+        if (i < NODES) {
+            sm.off[i] = (short)off;
+            for (int k = 0; k < nd; ++k) sm.inode[off + k] = (uint8_t)i;
+        }
+        __syncthreads();
+        double3 vsum = make_double3(0.0, 0.0, 0.0);
+        for (int base = 0; base < n_items; base += S2_CHUNK) {
+#pragma unroll
+            for (int r = 0; r < S2_IPT; ++r) {
+                const int t = r * SLOTS + i;
+                const int q = base + t;
+                if (q < n_items) {
+                    const int ii = sm.inode[q];
+                    const int k = q - sm.off[ii];
+                    const unsigned e = d.dlist[((size_t)a * MAXD + k) * SLOTS + ii];
+                    const float4 vj = __ldg(&d.Vb[sm.cell[e >> 8] * SLOTS + (int)(e & 255u)]);
+                    const float4 vi = sm.vs[ii];
+                    // velocity differences of floats are exact in FP64
+                    sm.c[t] = make_double3((double)vi.x - vj.x, (double)vi.y - vj.y, (double)vi.z - vj.z);
+                }
+            }
+            __syncthreads();
+            const int lo = max(off, base), hi = min(off + nd, base + S2_CHUNK);
+            for (int q = lo; q < hi; ++q) {
+                const double3 c = sm.c[q - base];
+                vsum.x += c.x; vsum.y += c.y; vsum.z += c.z;
+            }
+            __syncthreads();
+        }
         float disp = 0.0f;
         float3 fdk = make_float3(0.f, 0.f, 0.f);
         if (i < NODES) {
             const float3 v = f3(v4);
-            const double3 vt = tangential(sm.xs, n0, n1, n2, sgn, sweep_s2(d, sm.cell, a, i, v, nd));
+            const double3 vt = tangential(sm.xs, n0, n1, n2, sgn, vsum);
             const float3 fd = dis_force(P, sm.vs, n0, n1, n2, v, vt);
             d.FD[g] = make_float4(fd.x, fd.y, fd.z, 0.f);
             fdk = fd;
