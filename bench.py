@@ -226,7 +226,8 @@ def run_cs3d(args, world, rank, local):
     if args.workload in ENSEMBLES and world > 1:
         # instances shard across ranks by predicted cost, no data-path collective
         from cellsim3d_b200 import shard
-        mine = shard.partition([shard.predicted_cost(st) for _, st, _ in insts], world)[rank]
+        mine = shard.partition([shard.predicted_cost(st, args.warmup + args.steps, p) for p, st, _ in insts],
+                               world)[rank]
         insts = [insts[k] for k in mine]
     topo = make_topology(insts)
     ens = cs.Ensemble([p for p, _, _ in insts], topo, [cap for _, _, cap in insts], device=local)
@@ -330,7 +331,6 @@ def run_cs3d(args, world, rank, local):
             "nl_rebuilds": stats["rebuilds"],
             "max_entries": stats["max_entries"],
             "max_cand": stats["max_cand"],
-            "max_halo": stats["max_halo"],
             "clocks": clk.summary(),
         }
         if args.workload in ENSEMBLES:

@@ -21,7 +21,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import (CS3DError, Config, Mesh, Params, Rng, Topology, ERRBITS, SLOTS, NODES,
-                   OPT_RECORD_PAIRS, OPT_SKIN, OPT_PAIR_CAPACITY, OPT_REBUILD)
+                   OPT_RECORD_PAIRS, OPT_SKIN, OPT_PAIR_CAPACITY, OPT_REBUILD, OPT_HALO_STATS)
 
 __all__ = ["read_json_params", "config_to_params", "make_params", "read_fullerene_nn", "mesh_from_arrays",
            "build_topology", "Ranmar", "seed_map", "initialize_C180s", "Simulation", "Ensemble",

@@ -17,7 +17,7 @@ ERRBITS = {0x001: "NAN", 0x002: "CAPACITY", 0x004: "CAND_OVERFLOW", 0x008: "ENTR
            0x010: "NONFINITE_VOL", 0x020: "BAD_NORMAL", 0x040: "GRID_OVERFLOW", 0x080: "PAIR_OVERFLOW",
            0x100: "HALO_OVERFLOW", 0x200: "SOFT_CELLS"}
 
-OPT_RECORD_PAIRS, OPT_SKIN, OPT_PAIR_CAPACITY, OPT_REBUILD = 1, 2, 3, 4
+OPT_RECORD_PAIRS, OPT_SKIN, OPT_PAIR_CAPACITY, OPT_REBUILD, OPT_HALO_STATS = 1, 2, 3, 4, 5
 
 
 class Params(C.Structure):

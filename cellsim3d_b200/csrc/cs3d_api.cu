@@ -590,6 +590,9 @@ int cs3d_set_option(cs3d_ctx *c, int option, long long value)
     case CS3D_OPT_RECORD_PAIRS:
         c->d.record_pairs = value ? 1 : 0;
         break;
+    case CS3D_OPT_HALO_STATS:
+        c->d.halo_stats = value ? 1 : 0;
+        break;
     case CS3D_OPT_PAIR_CAPACITY: {
         if (value < 1) return CS3D_E_ARG;
         int4 *p = nullptr;

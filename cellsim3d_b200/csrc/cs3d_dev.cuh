@@ -140,6 +140,7 @@ struct Dev {
     unsigned long long *n_pairs;
     long long pair_cap;
     int record_pairs;
+    int halo_stats;     // count distinct candidate nodes per cell at list builds
 };
 
 __device__ __forceinline__ int f2o(float f)

@@ -1640,7 +1640,7 @@ __global__ void __launch_bounds__(SLOTS) k_nh_fill(Dev d)
 // once the slots are sorted.
 struct BuildSmem {
     int tkey[256];           // candidate cell of each temporary slot, -1 if free
-    uint32_t mask[256][6];   // partner nodes of each temporary slot
+    uint32_t mask[256][6];   // partner nodes of each temporary slot (CS3D_OPT_HALO_STATS)
     int comp_key[256], comp_t[256];
     short slot_of_t[256];    // final slot of a temporary slot, -1 if dropped
     int slot_t[MAXC];        // temporary slot of each final slot
@@ -1674,8 +1674,10 @@ __global__ void __launch_bounds__(SLOTS) k_nl_cell(Dev d, int phase)
         const BinGeom b = bin_geom(d, inst);
         const float rl = st->rcur + 1e-4f;
         const float rl2 = rl * rl;
+        const bool halo = d.halo_stats != 0;   // uniform
         for (int t = i; t < 256; t += SLOTS) sm.tkey[t] = -1;
-        for (int q = i; q < 256 * 6; q += SLOTS) (&sm.mask[0][0])[q] = 0u;
+        if (halo)
+            for (int q = i; q < 256 * 6; q += SLOTS) (&sm.mask[0][0])[q] = 0u;
         if (i == 0) sm.ncomp = 0;
         __syncthreads();
         const size_t g = (size_t)a * SLOTS + i;
@@ -1726,7 +1728,7 @@ __global__ void __launch_bounds__(SLOTS) k_nl_cell(Dev d, int phase)
                             last_t = t;
                         }
                         const int j = id - c * SLOTS;
-                        atomicOr(&sm.mask[t][j >> 5], 1u << (j & 31));
+                        if (halo) atomicOr(&sm.mask[t][j >> 5], 1u << (j & 31));
                         if (cnt < MAXE) ep[(size_t)cnt * SLOTS] = (uint16_t)((t << 8) | j);
                         ++cnt;
                       }
@@ -1758,15 +1760,17 @@ __global__ void __launch_bounds__(SLOTS) k_nl_cell(Dev d, int phase)
         }
         __syncthreads();
         const int nc = nct < MAXC ? nct : MAXC;
-        // distinct partner nodes of the cell (statistics only)
-        int ns = 0;
-        if (i < nc) {
-            const int t = sm.slot_t[i];
+        // distinct partner nodes of the cell (statistics, CS3D_OPT_HALO_STATS)
+        int nh = 0;
+        if (halo) {
+            int ns = 0;
+            if (i < nc) {
+                const int t = sm.slot_t[i];
 #pragma unroll
-            for (int k = 0; k < 6; ++k) ns += __popc(sm.mask[t][k]);
+                for (int k = 0; k < 6; ++k) ns += __popc(sm.mask[t][k]);
+            }
+            block_excl_scan<SLOTS>(ns, sm.wsum, nh);
         }
-        int nh;
-        block_excl_scan<SLOTS>(ns, sm.wsum, nh);
         // entries: (temporary slot, node) -> (slot, node), ascending
         if (i < NODES) {
             uint16_t ord[MAXE];
@@ -1798,7 +1802,7 @@ __global__ void __launch_bounds__(SLOTS) k_nl_cell(Dev d, int phase)
             atomicAdd(&st->built, 1);
             d.ncand[a] = nc;
             atomicMax(&st->max_cand, nct);
-            atomicMax(&st->max_halo, nh);
+            if (halo) atomicMax(&st->max_halo, nh);
         }
         int wm = cnt;
         for (int o = 16; o > 0; o >>= 1) wm = max(wm, __shfl_xor_sync(0xffffffffu, wm, o));

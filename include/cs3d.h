@@ -362,6 +362,9 @@ int cs3d_get_grid(cs3d_ctx *ctx, int inst, float minmax[6], int divs[3]);
 #define CS3D_OPT_SKIN          2   /* value = skin length in units of 1e-6 */
 #define CS3D_OPT_PAIR_CAPACITY 3   /* value = max recorded pairs */
 #define CS3D_OPT_REBUILD       4   /* value ignored: rebuild every neighbour list at the next step */
+#define CS3D_OPT_HALO_STATS    5   /* value 0/1: count the distinct contact-candidate nodes of each cell
+                                      at every list build (cs3d_get_stats [5]); off by default, as the
+                                      count costs the build a shared-memory atomic per entry */
 int cs3d_set_option(cs3d_ctx *ctx, int option, long long value);
 
 /* Contact pairs recorded during the last force evaluation (requires
@@ -384,7 +387,8 @@ int cs3d_last_error(cs3d_ctx *ctx, int inst, uint32_t *bits);
 /* Counters of this library's neighbour lists (no counterpart in the
  * reference): [0] steps, [1] neighbour-list rebuilds, [2] max entries per node
  * seen, [3] max candidate cells per cell seen, [4] kernel launches per step,
- * [5] max distinct contact-candidate nodes (of other cells) per cell seen,
+ * [5] max distinct contact-candidate nodes (of other cells) per cell seen
+ * (counted only with CS3D_OPT_HALO_STATS, else 0),
  * [6] cell neighbour lists built (cumulative). */
 int cs3d_get_stats(cs3d_ctx *ctx, long long *stats, int n);
 

@@ -33,6 +33,40 @@ def test_partition_of_the_256_instance_ensemble():
     assert loads.max() / loads.mean() < 1.05
 
 
+# Cell counts after 2000 steps of the 16-instance stratified subset of the
+# 256-instance ensemble, measured on a B200 by
+# tests/test_gpu_fullsize.py::test_ensemble256_subset_full_size (initial
+# cells -> cells after 2000 steps).
+MEASURED_2000 = {1: 9, 511: 1963, 47: 372, 275: 1428, 67: 515, 10: 77, 4: 31, 22: 166, 123: 815, 2: 15,
+                 32: 267, 398: 1753, 15: 123, 175: 1044, 5: 41}
+
+
+def test_population_model_matches_measured_growth():
+    for p, st in W.config4():
+        n0 = st["n"]
+        if n0 not in MEASURED_2000:
+            continue
+        pred = shard.predicted_population(n0, 2000, p["box_len"])[-1]
+        assert abs(pred - MEASURED_2000[n0]) <= max(2.0, 0.08 * MEASURED_2000[n0]), (n0, pred)
+
+
+def test_cost_model_uses_growth_and_steps():
+    insts = W.config4()
+    p, st = insts[0]
+    flat = dict(p, growth_rate=0.0)
+    assert shard.predicted_cost(st, 100, flat) == st["n"] * 180.0 * 100
+    assert shard.predicted_cost(st, 100) == st["n"] * 180.0 * 100
+    # dividing: every cell divides at step 1, then more
+    assert shard.predicted_cost(st, 100, p) > 2 * st["n"] * 180.0 * 99
+    # a growing ensemble: small instances grow proportionally more than large ones
+    costs = {st["n"]: shard.predicted_cost(st, 10000, p) / (st["n"] * 180.0 * 10000) for p, st in insts}
+    assert costs[min(costs)] > costs[max(costs)]
+    # 8 ranks over the 10k-step run stay balanced under the growth model
+    c = [shard.predicted_cost(st, 10000, p) for p, st in insts]
+    loads = np.array([sum(c[k] for k in part) for part in shard.partition(c, 8)])
+    assert loads.max() / loads.mean() < 1.05
+
+
 def test_partition_more_ranks_than_instances():
     parts = shard.partition([5.0, 1.0], 4)
     assert sorted(k for p in parts for k in p) == [0, 1]
