@@ -150,10 +150,13 @@ __device__ __forceinline__ int f2o(float f)
 }
 __device__ __forceinline__ float o2f(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff); }
 
-// Reference float arithmetic without FMA contraction (pair and box tests).
-__device__ __forceinline__ float r2_nc(float dx, float dy, float dz)
+// The squared distance of the reference's contact decisions (pair cut-offs,
+// box filter) as the reference's own build evaluates dx*dx + dy*dy + dz*dz:
+// nvcc's default contraction gives fma(dz, dz, fma(dx, dx, dy*dy)).  Written
+// with explicit intrinsics so that no compiler setting can change it.
+__device__ __forceinline__ float r2_ref(float dx, float dy, float dz)
 {
-    return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+    return __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
 }
 
 // Grid divisions, src/GPUbounce.cu:1332-1334.
@@ -190,7 +193,7 @@ __device__ __forceinline__ bool aabb_keep(float4 lo, float4 hi, float X, float Y
     float dy = __fadd_rn(__fmul_rn((float)(a > 0.0f), a), __fmul_rn((float)(b > 0.0f), b));
     a = __fsub_rn(Z, hi.z); b = __fsub_rn(lo.z, Z);
     float dz = __fadd_rn(__fmul_rn((float)(a > 0.0f), a), __fmul_rn((float)(b > 0.0f), b));
-    return !(r2_nc(dx, dy, dz) > ra2);
+    return !(r2_ref(dx, dy, dz) > ra2);
 }
 
 }  // namespace cs3d

@@ -114,24 +114,27 @@ __device__ __forceinline__ float3 random_force(const InstParams &P, int a, int i
     return make_float3(P.rscale * (ra * cosf(ta)), P.rscale * (ra * sinf(ta)), P.rscale * (rb * cosf(tb)));
 }
 
-// sqrt(x) and 1/x of positive doubles: float hardware seeds refined by one
-// Newton step in FP64 (relative error ~1e-14, far below what the forces need,
-// and much cheaper than the correctly rounded FP64 sequences).
-__device__ __forceinline__ double sqrt_nr(double x)
+// 1/sqrt(x), 1/x and sqrt(x) of positive doubles: the hardware's FP64
+// approximations (rsqrt.approx.ftz.f64, rcp.approx.ftz.f64; relative error
+// below 1e-6 on B200) refined by one Newton step in FP64.  Measured over
+// 1e-4..1e4 on B200: relative error below 1.3e-12, far below what the forces
+// need (their float rounding is 6e-8), with no float conversions.  The
+// arguments are never subnormal (squared lengths of at least ~1e-8).
+__device__ __forceinline__ double rsqrt_nr(double x)
 {
-    double y = (double)rsqrtf((float)x);
-    y = y * (1.5 - 0.5 * x * y * y);
-    return x * y;
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    return y * (1.5 - 0.5 * x * y * y);
 }
 __device__ __forceinline__ double rcp_nr(double x)
 {
-    double r = (double)__frcp_rn((float)x);
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
     return r * (2.0 - x * r);
 }
-__device__ __forceinline__ double rsqrt_nr(double x)
+__device__ __forceinline__ double sqrt_nr(double x)
 {
-    const double y = (double)rsqrtf((float)x);
-    return y * (1.5 - 0.5 * x * y * y);
+    return x * rsqrt_nr(x);
 }
 
 // Bond-angle term for one angle at a vertex with arms P (to the p-end node)
@@ -145,7 +148,7 @@ __device__ __forceinline__ double rsqrt_nr(double x)
 //   sin(dth / 2) = (c0 - u) / (2 sin(theta0 + dth / 2)),   dth = theta - theta0.
 // A float estimate of dth from acosf is refined by one Newton step of this
 // equation in FP64 (sin/cos of dth/2 by their Taylor series, |dth/2| < 0.4
-// for |dth/2| up to ~1.2 rad), which leaves dth accurate to ~1e-13.
+// for |dth/2| up to ~1.2 rad), which leaves dth accurate to ~1e-12.
 __device__ __forceinline__ void sincos_small(double x, double &s, double &c)
 {
     const double x2 = x * x;
@@ -155,17 +158,33 @@ __device__ __forceinline__ void sincos_small(double x, double &s, double &c)
             x2 * (1.0 / 479001600 + x2 * (-1.0 / 87178291200.0 + x2 / 20922789888000.0)))))));
 }
 
-__device__ __forceinline__ void angle_pair(float3 Pe, float3 Qe, float3 x, float th0f, double c0, double s0,
-                                           double3 &Fp, double3 &Fq)
+// One arm of a vertex: the exact FP64 difference p of two node positions,
+// its squared length, length and inverse squared length (from one rsqrt).
+struct Arm {
+    double x, y, z, r2, len, ir2;
+};
+
+__device__ __forceinline__ Arm make_arm(const double3 &to, const double3 &from)
 {
-    // arms from the vertex x to the two end nodes: differences of floats, exact in FP64
-    const double px = (double)Pe.x - x.x, py = (double)Pe.y - x.y, pz = (double)Pe.z - x.z;
-    const double qx = (double)Qe.x - x.x, qy = (double)Qe.y - x.y, qz = (double)Qe.z - x.z;
-    const double idk = px * qx + py * qy + pz * qz;
-    const double rp2 = px * px + py * py + pz * pz;
-    const double rq2 = qx * qx + qy * qy + qz * qz;
-    const double w2 = rp2 * rq2;
-    const double u = idk * rcp_nr(sqrt_nr(w2) + 1e-3);
+    Arm a;
+    a.x = to.x - from.x;
+    a.y = to.y - from.y;
+    a.z = to.z - from.z;
+    a.r2 = a.x * a.x + a.y * a.y + a.z * a.z;
+    const double r = rsqrt_nr(a.r2);
+    a.len = a.r2 * r;
+    a.ir2 = r * r;
+    return a;
+}
+
+// The angle between arms p and q: GetAngleForce(P, Q) (Fp) and
+// GetAngleForce(Q, P) (Fq).  |p||q| is the product of the two lengths, as the
+// reference forms it (sqrtf(ri_2) * sqrtf(rk_2)).
+__device__ __forceinline__ void angle_term(const Arm &p, const Arm &q, float th0f, double c0, double s0, double3 &Fp,
+                                           double3 &Fq)
+{
+    const double idk = p.x * q.x + p.y * q.y + p.z * q.z;
+    const double u = idk * rcp_nr(p.len * q.len + 1e-3);
     // float estimate, then one Newton step on g(h) = sin(h) sin(theta0 + h) - (c0 - u)/2, h = dth/2
     double h = 0.5 * (double)(acosf((float)u) - th0f);
     double sh, ch;
@@ -175,11 +194,11 @@ __device__ __forceinline__ void angle_pair(float3 Pe, float3 Qe, float3 x, float
     const double dg = ch * s1 + sh * c1t;                            // d/dh of sin(h) sin(theta0 + h)
     h -= g * rcp_nr(dg);
     const double dth = 2.0 * h;
-    const double c1 = -rsqrt_nr(w2 - idk * idk + 1e-3);
+    const double c1 = -rsqrt_nr(p.r2 * q.r2 - idk * idk + 1e-3);
     const double f = -1000.0 * c1 * dth;
-    const double cp = idk * rcp_nr(rp2), cq = idk * rcp_nr(rq2);
-    Fp = make_double3(f * (qx - cp * px), f * (qy - cp * py), f * (qz - cp * pz));
-    Fq = make_double3(f * (px - cq * qx), f * (py - cq * qy), f * (pz - cq * qz));
+    const double cp = idk * p.ir2, cq = idk * q.ir2;
+    Fp = make_double3(f * (q.x - cp * p.x), f * (q.y - cp * p.y), f * (q.z - cp * p.z));
+    Fq = make_double3(f * (p.x - cq * q.x), f * (p.y - cq * q.y), f * (p.z - cq * q.z));
 }
 
 // Shared per-CTA data of the contact sweep: candidate cells with their stale
@@ -309,7 +328,7 @@ __device__ __forceinline__ int sweep_s1(const Dev &d, const InstParams &P, const
         for (int q = 0; q < SB; ++q) {
             if (id[q] < 0) continue;
             const float dx = __fsub_rn(x.x, xj[q].x), dy = __fsub_rn(x.y, xj[q].y), dz = __fsub_rn(x.z, xj[q].z);
-            const float r2 = r2_nc(dx, dy, dz);
+            const float r2 = r2_ref(dx, dy, dz);
             if (r2 > P.ra2) { id[q] = -1; continue; }
             if (nd < MAXD) dl[(size_t)nd * SLOTS] = (uint16_t)e[q];
             ++nd;
@@ -349,17 +368,32 @@ __device__ __forceinline__ int sweep_s1(const Dev &d, const InstParams &P, const
     return nd;
 }
 
-// S2 sweep over the dissipative pairs S1 listed, one (node, pair) item at a
-// time.  A node has 0 to ~30 pairs (about one on average), so a loop per node
-// leaves most lanes idle; instead the cell's items (every pair of every node,
-// node-major, list order within a node) are numbered by a prefix sum of the
-// pair counts and dealt out to all 192 threads, S2_IPT per thread per chunk.
-// Each item leaves v_i - v_j (velocities after the half kicks) in shared
-// memory and the node's own thread adds its items in list order, so the FP64
-// sum has a fixed order; tangential() takes its tangential part.
-constexpr int S2_IPT = 2;                    // items per thread per chunk
-constexpr int S2_CHUNK = S2_IPT * SLOTS;     // items per chunk
-constexpr int S2_MAXITEMS = NODES * MAXD;    // dissipative pairs of one cell, at most
+// S2 sweep: sum of the velocity differences over the dissipative pairs found
+// by S1 (their list, in column layout), with the velocities after the half
+// kicks; tangential() takes its tangential part.
+__device__ __forceinline__ double3 sweep_s2(const Dev &d, const int *cell, int a, int i, float3 v, int nd)
+{
+    const uint16_t *dl = d.dlist + (size_t)a * MAXD * SLOTS + i;
+    double3 vt = make_double3(0.0, 0.0, 0.0);
+    for (int k0 = 0; k0 < nd; k0 += SB) {
+        unsigned e[SB];
+#pragma unroll
+        for (int q = 0; q < SB; ++q) e[q] = k0 + q < nd ? dl[(size_t)(k0 + q) * SLOTS] : 0xffffu;
+        float4 vj[SB];
+#pragma unroll
+        for (int q = 0; q < SB; ++q)
+            vj[q] = e[q] != 0xffffu ? __ldg(&d.Vb[cell[e[q] >> 8] * SLOTS + (int)(e[q] & 255u)])
+                                    : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int q = 0; q < SB; ++q) {
+            if (e[q] == 0xffffu) continue;
+            vt.x += (double)v.x - vj[q].x;
+            vt.y += (double)v.y - vj[q].y;
+            vt.z += (double)v.z - vj[q].z;
+        }
+    }
+    return vt;
+}
 
 // Tangential part of the friction sum, src/propagate.cu:558-656: the
 // reference adds v_ij - (v_ij . n) n over the dissipative pairs of node i, with
@@ -367,11 +401,11 @@ constexpr int S2_MAXITEMS = NODES * MAXD;    // dissipative pairs of one cell, a
 // x_N1)).  The projection is linear in v_ij, so the sweeps sum the velocity
 // differences alone (S) and this applies it once: S - (S . n) n.  The normal
 // is formed in FP64 from exact differences of the float positions.
-__device__ __forceinline__ double3 tangential(const float4 *xs, int n0, int n1, int n2, float sgn, double3 S)
+__device__ __forceinline__ double3 tangential(const double3 *xd, int n0, int n1, int n2, float sgn, double3 S)
 {
-    const float4 p0 = xs[n0], p1 = xs[n1], p2 = xs[n2];
-    const double ax = (double)p1.x - p0.x, ay = (double)p1.y - p0.y, az = (double)p1.z - p0.z;
-    const double bx = (double)p2.x - p0.x, by = (double)p2.y - p0.y, bz = (double)p2.z - p0.z;
+    const double3 p0 = xd[n0], p1 = xd[n1], p2 = xd[n2];
+    const double ax = p1.x - p0.x, ay = p1.y - p0.y, az = p1.z - p0.z;
+    const double bx = p2.x - p0.x, by = p2.y - p0.y, bz = p2.z - p0.z;
     const double cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
     const double s = (double)sgn * rsqrt_nr(cx * cx + cy * cy + cz * cz);
     const double nx = s * cx, ny = s * cy, nz = s * cz;
@@ -380,17 +414,19 @@ __device__ __forceinline__ double3 tangential(const float4 *xs, int n0, int n1, 
 }
 
 // Dissipative force, src/propagate.cu:546-658: bond damping with the three
-// neighbours, tangential friction sum vt, viscous drag.  FP64: the damping
-// term is a sum of velocity differences that can cancel.
-__device__ __forceinline__ float3 dis_force(const InstParams &P, const float4 *vs, int n0, int n1, int n2, float3 v,
+// neighbours, tangential friction sum vt, viscous drag, on the FP64 copies of
+// the cell's velocities (vd).  FP64: the damping term is a sum of velocity
+// differences that can cancel.
+__device__ __forceinline__ float3 dis_force(const InstParams &P, const double3 *vd, int i, int n0, int n1, int n2,
                                            double3 vt)
 {
+    const double3 v = vd[i];
     double dx = 0.0, dy = 0.0, dz = 0.0;
     const int nbr[3] = {n0, n1, n2};
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        const float4 vn = vs[nbr[k]];
-        dx += (double)v.x - vn.x; dy += (double)v.y - vn.y; dz += (double)v.z - vn.z;
+        const double3 vn = vd[nbr[k]];
+        dx += v.x - vn.x; dy += v.y - vn.y; dz += v.z - vn.z;
     }
     const double gi = P.gint, ge = P.gext, go = P.go;
     return make_float3((float)(-gi * dx - ge * vt.x - go * v.x), (float)(-gi * dy - ge * vt.y - go * v.y),
@@ -698,7 +734,8 @@ struct ArmForces {
 
 struct S1Smem {
     float4 xs[SLOTS];
-    float4 vs[SLOTS];
+    double3 xd[SLOTS];   // FP64 copies of the positions and velocities: the
+    double3 vd[SLOTS];   // FP64 terms read them without conversions
     SlotData sd;
     ArmForces arm;
 };
@@ -728,7 +765,8 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
             pre[q] = (uint32_t)d.ent[((size_t)a * MAXE + 2 * q) * SLOTS + i] |
                      ((uint32_t)d.ent[((size_t)a * MAXE + 2 * q + 1) * SLOTS + i] << 16);
         sm.xs[i] = x4;
-        sm.vs[i] = v4;
+        sm.xd[i] = make_double3(x4.x, x4.y, x4.z);
+        sm.vd[i] = make_double3(v4.x, v4.y, v4.z);
         slots_load(d, a, &d.st[inst], par, sm.sd);
         __syncthreads();
         slots_boxes(d, P, par, sm.sd, nc);
@@ -736,17 +774,18 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
         const float3 v = f3(v4);
         // bond angles: thread = vertex, three angles each
         if (P.angles && i < NODES) {
-            const float3 pa = f3(sm.xs[n0]), pb = f3(sm.xs[n1]), pc = f3(sm.xs[n2]);
+            const double3 xi = sm.xd[i];
+            const Arm pa = make_arm(sm.xd[n0], xi), pb = make_arm(sm.xd[n1], xi), pc = make_arm(sm.xd[n2], xi);
             const double2 *cs0 = d.topo.cs0 + 3 * i;
             const float4 th = __ldg(&d.topo.th0[i]);
             // angles (n0, n1), (n1, n2), (n0, n2); arm ends summed by destination
             double3 F01p, F01q, F12p, F12q, F02p, F02q;
             double2 t0 = __ldg(&cs0[0]);
-            angle_pair(pa, pb, x, th.x, t0.x, t0.y, F01p, F01q);
+            angle_term(pa, pb, th.x, t0.x, t0.y, F01p, F01q);
             t0 = __ldg(&cs0[1]);
-            angle_pair(pb, pc, x, th.y, t0.x, t0.y, F12p, F12q);
+            angle_term(pb, pc, th.y, t0.x, t0.y, F12p, F12q);
             t0 = __ldg(&cs0[2]);
-            angle_pair(pa, pc, x, th.z, t0.x, t0.y, F02p, F02q);
+            angle_term(pa, pc, th.z, t0.x, t0.y, F02p, F02q);
             const int o = i * 3;
             sm.arm.x[o] = F01p.x + F02p.x; sm.arm.y[o] = F01p.y + F02p.y; sm.arm.z[o] = F01p.z + F02p.z;
             sm.arm.x[o + 1] = F01q.x + F12p.x; sm.arm.y[o + 1] = F01q.y + F12p.y; sm.arm.z[o + 1] = F01q.z + F12p.z;
@@ -764,11 +803,12 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
             // k (R - R0) / R0 * d / R = k (1/R0 - 1/R) d
             const double stiff = d.E[a];
             const int nbr[3] = {n0, n1, n2};
+            const double3 xi = sm.xd[i];
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 // exact FP64 differences of the float positions
-                const float4 xn = sm.xs[nbr[k]];
-                const double ex = (double)xn.x - x.x, ey = (double)xn.y - x.y, ez = (double)xn.z - x.z;
+                const double3 xn = sm.xd[nbr[k]];
+                const double ex = xn.x - xi.x, ey = xn.y - xi.y, ez = xn.z - xi.z;
                 const double iR = rsqrt_nr(ex * ex + ey * ey + ez * ez);
                 const double c = stiff * (__ldg(&d.topo.r0i[3 * i + k]) - iR);
                 FX += c * ex; FY += c * ey; FZ += c * ez;
@@ -776,7 +816,7 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
             // internal pressure, src/propagate.cu:318-330 (CM of the previous step)
             {
                 const float4 cm = d.CM[a];
-                const double rx = (double)x.x - cm.x, ry = (double)x.y - cm.y, rz = (double)x.z - cm.z;
+                const double rx = xi.x - cm.x, ry = xi.y - cm.y, rz = xi.z - cm.z;
                 const double c = 3.0 * (double)d.press[a] * rsqrt_nr(rx * rx + ry * ry + rz * rz);
                 FX += c * rx; FY += c * ry; FZ += c * rz;
             }
@@ -793,7 +833,7 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
             // contacts, src/propagate.cu:356-442 and the first dissipative sweep
             double3 vsum = make_double3(0.0, 0.0, 0.0);
             const int nd = sweep_s1(d, P, sm.sd, a, i, x, v, ne, pre, FX, FY, FZ, vsum);
-            const double3 vt = tangential(sm.xs, n0, n1, n2, sgn, vsum);
+            const double3 vt = tangential(sm.xd, n0, n1, n2, sgn, vsum);
             if (nd > MAXD) atomic_or_err(&d.st[inst], CS3D_ERRBIT_ENTRY_OVERFLOW);
             // rigid box walls, src/propagate.cu:474-510 (float gap tests)
             if (P.rigid) {
@@ -808,7 +848,7 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
                 if (g1 < P.thresh) FZ += -wk * ((double)g1 - th);
                 if (g2 < P.thresh) FZ += wk * ((double)g2 - th);
             }
-            const float3 fd = dis_force(P, sm.vs, n0, n1, n2, v, vt);
+            const float3 fd = dis_force(P, sm.vd, i, n0, n1, n2, vt);
             d.FC[g] = make_float4((float)FX, (float)FY, (float)FZ, 0.f);
             d.ndis[g] = (uint8_t)(nd < MAXD ? nd : MAXD);
             if (INIT) {
@@ -847,14 +887,11 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
 // ---------------------------------------------------------------------------
 struct S2Smem {
     float4 xs[SLOTS];
-    float4 vs[SLOTS];
+    double3 xd[SLOTS];   // FP64 copies of the positions and velocities
+    double3 vd[SLOTS];
     int cell[MAXC];
     GeomScratch gs;
     int dflag;   // the cell divides (division steps)
-    double3 c[S2_CHUNK];             // v_i - v_j of each item of a chunk
-    short off[SLOTS];                // each node's first item
-    uint8_t inode[S2_MAXITEMS];      // the node of each item
-    int wsum[SLOTS / 32];
 };
 
 // Integrate + ForwardTime of the next step (src/propagate.cu:681-763) on the
@@ -921,62 +958,18 @@ __global__ void __launch_bounds__(SLOTS, 5) k_s2(Dev d, int par)
         const size_t g = (size_t)a * SLOTS + i;
         float4 x4 = make_float4(0, 0, 0, 0), v4 = make_float4(0, 0, 0, 0);
         int nd = 0;
-        if (i < NODES) { x4 = d.X[g]; v4 = d.Vb[g]; nd = min((int)d.ndis[g], MAXD); }
+        if (i < NODES) { x4 = d.X[g]; v4 = d.Vb[g]; nd = d.ndis[g]; }
         if (i < MAXC) sm.cell[i] = d.cand[(size_t)a * MAXC + i];
         sm.xs[i] = x4;
-        sm.vs[i] = v4;
-        // items of the cell: warp-inclusive scan of the pair counts
-        const int lane = i & 31, wid = i >> 5;
-        int incl = nd;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        if (lane == 31) sm.wsum[wid] = incl;
+        sm.xd[i] = make_double3(x4.x, x4.y, x4.z);
+        sm.vd[i] = make_double3(v4.x, v4.y, v4.z);
         __syncthreads();
-        int off = incl - nd, n_items = 0;
-#pragma unroll
-        for (int q = 0; q < SLOTS / 32; ++q) {
-            const int ws = sm.wsum[q];
-            off += q < wid ? ws : 0;
-            n_items += ws;
-        }
-        if (i < NODES) {
-            sm.off[i] = (short)off;
-            for (int k = 0; k < nd; ++k) sm.inode[off + k] = (uint8_t)i;
-        }
-        __syncthreads();
-        double3 vsum = make_double3(0.0, 0.0, 0.0);
-        for (int base = 0; base < n_items; base += S2_CHUNK) {
-#pragma unroll
-            for (int r = 0; r < S2_IPT; ++r) {
-                const int t = r * SLOTS + i;
-                const int q = base + t;
-                if (q < n_items) {
-                    const int ii = sm.inode[q];
-                    const int k = q - sm.off[ii];
-                    const unsigned e = d.dlist[((size_t)a * MAXD + k) * SLOTS + ii];
-                    const float4 vj = __ldg(&d.Vb[sm.cell[e >> 8] * SLOTS + (int)(e & 255u)]);
-                    const float4 vi = sm.vs[ii];
-                    // velocity differences of floats are exact in FP64
-                    sm.c[t] = make_double3((double)vi.x - vj.x, (double)vi.y - vj.y, (double)vi.z - vj.z);
-                }
-            }
-            __syncthreads();
-            const int lo = max(off, base), hi = min(off + nd, base + S2_CHUNK);
-            for (int q = lo; q < hi; ++q) {
-                const double3 c = sm.c[q - base];
-                vsum.x += c.x; vsum.y += c.y; vsum.z += c.z;
-            }
-            __syncthreads();
-        }
         float disp = 0.0f;
         float3 fdk = make_float3(0.f, 0.f, 0.f);
         if (i < NODES) {
             const float3 v = f3(v4);
-            const double3 vt = tangential(sm.xs, n0, n1, n2, sgn, vsum);
-            const float3 fd = dis_force(P, sm.vs, n0, n1, n2, v, vt);
+            const double3 vt = tangential(sm.xd, n0, n1, n2, sgn, sweep_s2(d, sm.cell, a, i, v, nd));
+            const float3 fd = dis_force(P, sm.vd, i, n0, n1, n2, vt);
             d.FD[g] = make_float4(fd.x, fd.y, fd.z, 0.f);
             fdk = fd;
             if (FUSE && !DIV) disp = next_kick(d, P, g, x4, v4, fd);

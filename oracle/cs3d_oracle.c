@@ -13,8 +13,11 @@
  *     double from the float state.
  *   - Every discrete decision that the reference makes in float (contact-pair
  *     cut-offs, bounding-box filter, bin indices, wall gaps, grid extents) is
- *     evaluated in float with the reference's expression order and no FMA
- *     contraction (built with -ffp-contract=off), so the pair sets are exact.
+ *     evaluated in float with the reference's expression order, as the
+ *     reference's own nvcc build evaluates it: no contraction of its own
+ *     (built with -ffp-contract=off) except the squared distances of the
+ *     contact decisions, which that build fuses into FMAs (r2_ref below), so
+ *     the pair sets are exact.
  *   - RANMAR and the Marsaglia sphere point are float, bit-exact.
  *
  * Reference files cited as path:line within SoftSimu/CellSim3D.
@@ -469,6 +472,23 @@ static int node_bin(const orc_sys *s, float X, float Y, float Z)
 }
 
 /* Bounding-box filter, src/propagate.cu:382-392 (float). Returns 1 if kept. */
+/* The squared distance of the reference's contact decisions as its own
+ * build evaluates it.  The source writes dx*dx + dy*dy + dz*dz in float
+ * (src/propagate.cu:386-390, :418, :614-618, :636); nvcc, with its default
+ * floating-point contraction (the reference's makefile does not turn it
+ * off), computes it as fmaf(dz, dz, fmaf(dx, dx, dy*dy)).  That association
+ * is pinned two ways: a kernel of that expression compiled with the same
+ * flags gives this value for every one of 2^20 random inputs, and a pair
+ * whose uncontracted value lies at the cut-off and whose contracted value
+ * lies above it is left out of the reference's own dissipative force
+ * (tests/golden/make_fma_case.py, tests/test_ref_cuda.py). */
+static inline float r2_ref(float dx, float dy, float dz)
+{
+    return fmaf(dz, dz, fmaf(dx, dx, dy * dy));
+}
+
+/* Bounding-box filter, src/propagate.cu:382-392.  The box deltas are exact
+ * (one of the two terms of each is zero), the sum is r2_ref. */
 static int aabb_keep(const float *bb, float X, float Y, float Z, float ra)
 {
     float dx = (X - bb[1] > 0.0f) * (X - bb[1]);
@@ -477,7 +497,7 @@ static int aabb_keep(const float *bb, float X, float Y, float Z, float ra)
     dy += (bb[2] - Y > 0.0f) * (bb[2] - Y);
     float dz = (Z - bb[5] > 0.0f) * (Z - bb[5]);
     dz += (bb[4] - Z > 0.0f) * (bb[4] - Z);
-    return !(dx * dx + dy * dy + dz * dz > ra * ra);
+    return !(r2_ref(dx, dy, dz) > ra * ra);
 }
 
 /* Accepted neighbour cells of one node (src/propagate.cu:375-404), in bin
@@ -499,7 +519,7 @@ static int accepted_cells(const orc_sys *s, int a, float X, float Y, float Z, in
 static inline float pair_r2(float xi, float yi, float zi, float xj, float yj, float zj)
 {
     float dx = xi - xj, dy = yi - yj, dz = zi - zj;
-    return dx * dx + dy * dy + dz * dz;
+    return r2_ref(dx, dy, dz);
 }
 
 /* ------------------------------------------------------------------------ */

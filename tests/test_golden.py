@@ -127,3 +127,48 @@ def test_traj_writer_matches_golden(tmp_path):
         s = float(np.stack([f["X"], f["Y"], f["Z"]], -1).astype(np.float64).sum())
         assert abs(s - g["sum"]) < 1e-9 * max(1, abs(g["sum"]))
         assert [float(f["X"][0, 0]), float(f["Y"][0, 0]), float(f["Z"][0, 0])] == g["first"]
+
+
+def _fma_case():
+    c = np.load(os.path.join(GOLD, "fma_boundary_case.npz"))
+    st = {k: c[k] for k in ("X", "Y", "Z", "VX", "VY", "VZ")}
+    st["n"] = 2
+    return c, st
+
+
+def test_fma_boundary_case_fixture():
+    """The fixture's pair lies at the cut-off in the uncontracted float
+    expression and above it in the contracted one that the reference's build
+    evaluates (fma(dz, dz, fma(dx, dx, dy*dy)))."""
+    from fractions import Fraction
+    c, st = _fma_case()
+    i, j = int(c["i"]), int(c["j"])
+    f32 = np.float32
+    d = [f32(st[k].reshape(2, 192)[0, i] - st[k].reshape(2, 192)[1, j]) for k in ("X", "Y", "Z")]
+    fma = lambda a, b, z: f32(float(Fraction(float(a)) * Fraction(float(b)) + Fraction(float(z))))
+    plain = f32(f32(f32(d[0] * d[0]) + f32(d[1] * d[1])) + f32(d[2] * d[2]))
+    contracted = fma(d[2], d[2], fma(d[0], d[0], f32(d[1] * d[1])))
+    ra2 = f32(f32(0.3) * f32(0.3))
+    assert plain == c["r2_plain"] and contracted == c["r2_fma"]
+    assert plain <= ra2 < contracted
+
+
+def test_oracle_decides_the_boundary_pair_as_the_reference_build():
+    """With the contracted squared distance the oracle leaves the pair out of
+    the dissipative set, so node i feels no friction (its neighbours and
+    itself rest); tests/test_ref_cuda.py shows the reference's own kernels
+    leave it out too."""
+    c, st = _fma_case()
+    i, j = int(c["i"]), int(c["j"])
+    mesh = W.load_mesh()
+    p = W.base_params(box_len=(30.0, 30.0, 30.0))
+    r0, th = oracle.r0_theta0(st["X"][:192], st["Y"][:192], st["Z"][:192], mesh["nn"])
+    O = oracle.System(2, p, oracle.make_topo(mesh["nn"], mesh["sign"], r0, th, mesh["faces"]))
+    O.load(st["X"], st["Y"], st["Z"], st["VX"], st["VY"], st["VZ"], n=2)
+    O.seed(1, 100)
+    O.set_record(True)
+    O.init()
+    pairs = {tuple(x) for x in O.recorded_pairs(1).tolist()}
+    assert (0, i, 1, j) not in pairs and (1, j, 0, i) not in pairs
+    assert all(float(O.FD[q][i]) == 0.0 for q in range(3))
+    O.close()

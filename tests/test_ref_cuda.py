@@ -237,6 +237,23 @@ def test_langevin_statistics_against_reference_kernels(mesh):
     sim.close()
 
 
+def fma32(a, b, c):
+    """Elementwise fmaf(a, b, c) of float32 arrays: a*b + c rounded once.  In
+    float64 a*b is exact and the sum is rounded twice only where it falls on
+    a float32 rounding tie, which the exact fractions recompute."""
+    from fractions import Fraction
+    a, b, c = (np.asarray(v, np.float32) for v in (a, b, c))
+    s = a.astype(np.float64) * b + c
+    r = s.astype(np.float32)
+    # ties of the float32 rounding of s: recompute exactly
+    lo = np.nextafter(r, np.float32(-np.inf)).astype(np.float64)
+    hi = np.nextafter(r, np.float32(np.inf)).astype(np.float64)
+    tie = (s == 0.5 * (lo + r.astype(np.float64))) | (s == 0.5 * (hi + r.astype(np.float64)))
+    for k in np.flatnonzero(tie):
+        r[k] = np.float32(float(Fraction(float(a[k])) * Fraction(float(b[k])) + Fraction(float(c[k]))))
+    return r
+
+
 def _reference_accepted(st, n, g, ra):
     """(cell, node, accepted cell) of every node from the reference's own grid
     (bin lists, bounding boxes, extents read back after its makeNNlist), with
@@ -271,8 +288,10 @@ def _reference_accepted(st, n, g, ra):
         u = (x - bb[cell, 2 * d + 1]).astype(f32)
         w = (bb[cell, 2 * d] - x).astype(f32)
         dd.append(((u > 0).astype(f32) * u + (w > 0).astype(f32) * w).astype(f32))
-    r2 = ((dd[0] * dd[0]).astype(f32) + (dd[1] * dd[1]).astype(f32)).astype(f32) + (dd[2] * dd[2]).astype(f32)
-    ok = ~(r2.astype(f32) > ra2)
+    # the reference's build evaluates dx*dx + dy*dy + dz*dz contracted:
+    # fma(dz, dz, fma(dx, dx, dy*dy)) (fma32: the exact value rounded once)
+    r2 = fma32(dd[2], dd[2], fma32(dd[0], dd[0], (dd[1] * dd[1]).astype(f32)))
+    ok = ~(r2 > ra2)
     return list(zip(a[ok].tolist(), (node[ok] % 180).tolist(), cell[ok].tolist()))
 
 
@@ -313,3 +332,37 @@ def test_candidate_stage_against_the_reference_grid(mesh, case):
         assert np.array_equal(pair_keys(sim.pairs(kind)), pair_keys(O.recorded_pairs(kind)))
     sim.close()
     O.close()
+
+
+def test_boundary_pair_decided_as_the_reference_build(mesh):
+    """The reference's own kernels, the CUDA path and the oracle on two cells
+    whose one node pair lies at the dissipative cut-off in the uncontracted
+    float expression and above it in the contracted one
+    (tests/golden/fma_boundary_case.npz, made by make_fma_case.py).  The
+    reference's build leaves the pair out (node i feels no friction), and so
+    do the CUDA path and the oracle."""
+    import os
+    import oracle
+    c = np.load(os.path.join(os.path.dirname(__file__), "golden", "fma_boundary_case.npz"))
+    i, j = int(c["i"]), int(c["j"])
+    st = {k: c[k] for k in ("X", "Y", "Z", "VX", "VY", "VZ")}
+    st["n"] = 2
+    p = W.base_params(box_len=(30.0, 30.0, 30.0))
+    r = ref.run(p, mesh, st, 2, 0, dump_init=True)
+    assert r["status"] == 0, r["status_text"]
+    fd_ref = [float(r["init"][k][i]) for k in ("FDX", "FDY", "FDZ")]
+    sim, orc = make_pair(p, st, mesh, capacity=2)
+    f = sim.forces()
+    fd_gpu = [float(f[k][i]) for k in ("FDX", "FDY", "FDZ")]
+    fd_orc = [float(orc.FD[q][i]) for q in range(3)]
+    print("boundary pair: reference Fd %s, CUDA path %s, oracle %s" % (fd_ref, fd_gpu, fd_orc))
+    assert fd_ref == [0.0, 0.0, 0.0]
+    assert fd_gpu == [0.0, 0.0, 0.0] and fd_orc == [0.0, 0.0, 0.0]
+    pairs = {tuple(x) for x in sim.pairs(1).tolist()}
+    assert (0, i, 1, j) not in pairs and (1, j, 0, i) not in pairs
+    # the pair lists of both cut-offs agree with the oracle's
+    from parity import pair_keys
+    for kind in (0, 1):
+        assert np.array_equal(pair_keys(sim.pairs(kind)), pair_keys(orc.recorded_pairs(kind)))
+    sim.close()
+    orc.close()
