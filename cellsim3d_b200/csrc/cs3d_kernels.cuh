@@ -401,9 +401,14 @@ __device__ __forceinline__ double3 sweep_s2(const Dev &d, const int *cell, int a
 // x_N1)).  The projection is linear in v_ij, so the sweeps sum the velocity
 // differences alone (S) and this applies it once: S - (S . n) n.  The normal
 // is formed in FP64 from exact differences of the float positions.
-__device__ __forceinline__ double3 tangential(const double3 *xd, int n0, int n1, int n2, float sgn, double3 S)
+__device__ __forceinline__ double3 as_d3(const double3 &a) { return a; }
+__device__ __forceinline__ double3 as_d3(const float4 &a) { return make_double3(a.x, a.y, a.z); }
+
+// xd: the cell's positions (FP64 copies, or the float4 originals).
+template <typename T>
+__device__ __forceinline__ double3 tangential(const T *xd, int n0, int n1, int n2, float sgn, double3 S)
 {
-    const double3 p0 = xd[n0], p1 = xd[n1], p2 = xd[n2];
+    const double3 p0 = as_d3(xd[n0]), p1 = as_d3(xd[n1]), p2 = as_d3(xd[n2]);
     const double ax = p1.x - p0.x, ay = p1.y - p0.y, az = p1.z - p0.z;
     const double bx = p2.x - p0.x, by = p2.y - p0.y, bz = p2.z - p0.z;
     const double cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
@@ -414,18 +419,19 @@ __device__ __forceinline__ double3 tangential(const double3 *xd, int n0, int n1,
 }
 
 // Dissipative force, src/propagate.cu:546-658: bond damping with the three
-// neighbours, tangential friction sum vt, viscous drag, on the FP64 copies of
-// the cell's velocities (vd).  FP64: the damping term is a sum of velocity
-// differences that can cancel.
-__device__ __forceinline__ float3 dis_force(const InstParams &P, const double3 *vd, int i, int n0, int n1, int n2,
+// neighbours, tangential friction sum vt, viscous drag, on the cell's
+// velocities (vd: FP64 copies or the float4 originals).  FP64: the damping
+// term is a sum of velocity differences that can cancel.
+template <typename T>
+__device__ __forceinline__ float3 dis_force(const InstParams &P, const T *vd, int i, int n0, int n1, int n2,
                                            double3 vt)
 {
-    const double3 v = vd[i];
+    const double3 v = as_d3(vd[i]);
     double dx = 0.0, dy = 0.0, dz = 0.0;
     const int nbr[3] = {n0, n1, n2};
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        const double3 vn = vd[nbr[k]];
+        const double3 vn = as_d3(vd[nbr[k]]);
         dx += v.x - vn.x; dy += v.y - vn.y; dz += v.z - vn.z;
     }
     const double gi = P.gint, ge = P.gext, go = P.go;

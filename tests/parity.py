@@ -186,17 +186,27 @@ def ensemble_step_check(ens, params, caps, otopo, tags, tol=TOL, check_pairs=Tru
         # velocities after the step
         evv = rel_err([after["VX"], after["VY"], after["VZ"]], [O.VX, O.VY, O.VZ], n)
         # dissipative force on identical inputs: the CUDA path's own v3 and x,
-        # stale grid of the previous step (cells that divided this step excluded:
-        # their positions changed after the force evaluation)
-        # (with correct_com the positions after the step were shifted after the
-        # force evaluation: the positions at the evaluation are rebuilt from the
-        # state before the step by the integrator's float arithmetic)
+        # stale grid of the previous step.  The positions are those of the
+        # force evaluation: the positions after the step, except for the cells
+        # that divided this step, whose nodes the division moved after the
+        # evaluation (their neighbours' friction saw the old ones), and except
+        # with correct_com, which shifts every node after the evaluation; both
+        # are rebuilt from the state before the step by the integrator's float
+        # arithmetic.  The two cells of each division are left out of the
+        # comparison.
         O2 = oracle_from(before[k], p, otopo, cap, record=False)
-        if p.get("correct_com"):
+        O2.X[:kk], O2.Y[:kk], O2.Z[:kk] = after["X"][:kk], after["Y"][:kk], after["Z"][:kk]
+        n_before = before[k]["n"]
+        parents = [c for c in divided if c < n_before]
+        if p.get("correct_com") or parents:
             xs = drift_positions(before[k], p)
-            O2.X[:kk], O2.Y[:kk], O2.Z[:kk] = xs[0][:kk], xs[1][:kk], xs[2][:kk]
-        else:
-            O2.X[:kk], O2.Y[:kk], O2.Z[:kk] = after["X"][:kk], after["Y"][:kk], after["Z"][:kk]
+            kb = n_before * 192
+            if p.get("correct_com"):
+                O2.X[:kb], O2.Y[:kb], O2.Z[:kb] = xs[0][:kb], xs[1][:kb], xs[2][:kb]
+            else:
+                for c in parents:
+                    sl = slice(c * 192, (c + 1) * 192)
+                    O2.X[sl], O2.Y[sl], O2.Z[sl] = xs[0][sl], xs[1][sl], xs[2][sl]
         O2.VX[:kk], O2.VY[:kk], O2.VZ[:kk] = after["VX"][:kk], after["VY"][:kk], after["VZ"][:kk]
         O2._n[0] = n
         O2.dis_force()
