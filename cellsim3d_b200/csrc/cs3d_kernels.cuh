@@ -893,9 +893,9 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
 // ---------------------------------------------------------------------------
 struct S2Smem {
     float4 xs[SLOTS];
-    double3 xd[SLOTS];   // FP64 copies of the positions and velocities
-    double3 vd[SLOTS];
+    float4 vs[SLOTS];
     int cell[MAXC];
+
     GeomScratch gs;
     int dflag;   // the cell divides (division steps)
 };
@@ -967,15 +967,16 @@ __global__ void __launch_bounds__(SLOTS, 5) k_s2(Dev d, int par)
         if (i < NODES) { x4 = d.X[g]; v4 = d.Vb[g]; nd = d.ndis[g]; }
         if (i < MAXC) sm.cell[i] = d.cand[(size_t)a * MAXC + i];
         sm.xs[i] = x4;
-        sm.xd[i] = make_double3(x4.x, x4.y, x4.z);
-        sm.vd[i] = make_double3(v4.x, v4.y, v4.z);
+        sm.vs[i] = v4;
         __syncthreads();
         float disp = 0.0f;
+
         float3 fdk = make_float3(0.f, 0.f, 0.f);
         if (i < NODES) {
             const float3 v = f3(v4);
-            const double3 vt = tangential(sm.xd, n0, n1, n2, sgn, sweep_s2(d, sm.cell, a, i, v, nd));
-            const float3 fd = dis_force(P, sm.vd, i, n0, n1, n2, vt);
+            const double3 vt = tangential(sm.xs, n0, n1, n2, sgn, sweep_s2(d, sm.cell, a, i, v, nd));
+            const float3 fd = dis_force(P, sm.vs, i, n0, n1, n2, vt);
+
             d.FD[g] = make_float4(fd.x, fd.y, fd.z, 0.f);
             fdk = fd;
             if (FUSE && !DIV) disp = next_kick(d, P, g, x4, v4, fd);
