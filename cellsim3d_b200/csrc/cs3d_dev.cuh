@@ -124,7 +124,7 @@ struct Dev {
     int *hsz;           // buckets in use by the current list build (whole scan tiles, <= hsize)
     int *hcount;        // [hsize + SCAN_TILE] bucket counts, then exclusive starts
     int *hscan;         // [hsize / SCAN_TILE + 1] tile sums of the scan
-    float4 *hpos;       // [cap_total*192] positions sorted by bucket, w = node id bits
+    float4 *hpos;       // [cap_total*192] positions sorted by bucket, w = (cell << 8 | node) bits
     int *node_rank;     // [cap_total*192] position of the node in its bucket
     DivEntry *divtab;
     int *div_total;

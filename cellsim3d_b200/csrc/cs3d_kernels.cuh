@@ -1628,7 +1628,8 @@ __global__ void __launch_bounds__(SLOTS) k_nh_fill(Dev d)
         const size_t g = (size_t)a * SLOTS + i;
         const float4 x = d.X[g];
         const unsigned k = bucket_of(b, bin_coord(x.x, b.inv), bin_coord(x.y, b.inv), bin_coord(x.z, b.inv));
-        d.hpos[d.hcount[k] + d.node_rank[g]] = make_float4(x.x, x.y, x.z, __int_as_float((int)g));
+        // w: the node as cell << 8 | node (cells < 2^23)
+        d.hpos[d.hcount[k] + d.node_rank[g]] = make_float4(x.x, x.y, x.z, __int_as_float((a << 8) | i));
     }
 }
 
@@ -1699,22 +1700,23 @@ __global__ void __launch_bounds__(SLOTS) k_nl_cell(Dev d, int phase)
                     if (nrun == 1) { kb = k0; ke = k0 + 3u; }
                     else { kb = bucket_of(b, ix - 1 + u, jy, jz); ke = kb + 1u; }
                     const int p0 = d.hcount[kb], p1 = d.hcount[ke];
-                    // candidates in batches: the loads of a batch are in flight together
+                    // candidates in batches: the loads of a batch are in flight together;
+                    // past the run a far sentinel fails the distance test
                     for (int p = p0; p < p1; p += CB) {
                       float4 yb[CB];
 #pragma unroll
                       for (int q = 0; q < CB; ++q)
-                          yb[q] = p + q < p1 ? d.hpos[p + q] : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+                          yb[q] = p + q < p1 ? d.hpos[p + q] : make_float4(1.0e30f, 1.0e30f, 1.0e30f, 0.f);
 #pragma unroll
                       for (int q = 0; q < CB; ++q) {
                         const float4 y = yb[q];
-                        const int id = __float_as_int(y.w);
-                        if (id < 0) continue;
-                        // the instance's own hash slice holds only its own nodes
-                        const int c = id / SLOTS;
-                        if (c == a) continue;
+                        // the distance first: most candidates fail it
                         const float dx = x.x - y.x, dy = x.y - y.y, dz = x.z - y.z;
                         if (!(dx * dx + dy * dy + dz * dz < rl2)) continue;
+                        // the instance's own hash slice holds only its own nodes
+                        const int id = __float_as_int(y.w);
+                        const int c = id >> 8;
+                        if (c == a) continue;
                         int t = last_t;
                         if (c != last_c) {
                             t = -1;
@@ -1727,7 +1729,7 @@ __global__ void __launch_bounds__(SLOTS) k_nl_cell(Dev d, int phase)
                             last_c = c;
                             last_t = t;
                         }
-                        const int j = id - c * SLOTS;
+                        const int j = id & 255;
                         if (halo) atomicOr(&sm.mask[t][j >> 5], 1u << (j & 31));
                         if (cnt < MAXE) ep[(size_t)cnt * SLOTS] = (uint16_t)((t << 8) | j);
                         ++cnt;
