@@ -178,6 +178,8 @@ InstParams make_inst(const cs3d_params &p, int base, int cap, float skin)
 {
     InstParams q{};
     q.mass = p.particle_mass;
+    q.mass_d = (double)p.particle_mass;
+    q.inv_m = 1.0 / (double)p.particle_mass;   // IEEE division on the host: correctly rounded
     q.rr = p.repulsion_range;
     q.ra = p.attraction_range;
     q.rs = p.repulsion_strength;

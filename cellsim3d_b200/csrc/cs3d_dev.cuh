@@ -20,6 +20,8 @@ constexpr float DL = 2.9f;             // reference grid spacing, src/GPUbounce.
 struct InstParams {
     float mass, rr, ra, rs, as, E, stiff1, gint, gext, go, divvol, dt, maxp, minp, growth, thresh;
     float box[3];
+    double mass_d;  // mass as a double
+    double inv_m;   // 1 / mass, correctly rounded (the integrator's divisions)
     float ra2;      // fl(ra*ra), the reference's float cut-off
     float asE;      // fl(as*E), attraction coefficient
     float rsE;      // fl(rs*E), repulsion coefficient
