@@ -28,6 +28,10 @@ struct cs3d_ctx {
     // device allocations to free
     std::vector<void *> allocs;
     bool need_init = true;
+    // The last step of the previous cs3d_step call ran S2 in fused mode: d.X and
+    // d.V already hold the next step's half kick and drift, and the step-end
+    // state is in d.Xe (positions) and d.Vb (velocities).
+    bool prekicked = false;
     long long host_step = 0;
     int max_div_steps = 0;
     bool any_growth = false;
@@ -40,7 +44,7 @@ struct cs3d_ctx {
     int grid_nodes = 0;            // blocks of the neighbour-list kernels
     int grid_tiles = 0;            // blocks of the bucket scan
     int grid_s2 = 0;               // blocks of S2 and the integrator
-    cudaGraphExec_t graph[2][2][2][2] = {};  // [parity][division][integrate first][fused S2]
+    cudaGraphExec_t graph[2][2][2][3] = {};  // [parity][division][integrate first][S2 mode: 0, fused 1, fused last 2]
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // asynchronous read-back (cs3d_get_state_async): a copy stream, two
     // device staging slots and their events
@@ -340,11 +344,12 @@ int run_init(cs3d_ctx *c)
 
 // One timestep, src/GPUbounce.cu:1055-1338, as a fixed launch sequence.
 // k1: the step starts with k_integrate (else the previous step's fused S2
-// did it); fuse: S2 also integrates the next step (the next step follows in
-// the same call; on division steps the two cells of each division are
-// integrated after their placement); soften: the number of this
+// did it); fuse: S2 also integrates the next step (1: the next step follows in
+// the same call; 2: the last step of a call, which also keeps the step-end
+// positions for the read-back; on division steps the two cells of each
+// division are integrated after their placement); soften: the number of this
 // step when its end softens cells (launched outside the graphs), else 0.
-int launch_step(cs3d_ctx *c, int par, bool div, bool k1 = true, bool fuse = false, const Prof &pf = Prof(),
+int launch_step(cs3d_ctx *c, int par, bool div, bool k1 = true, int fuse = 0, const Prof &pf = Prof(),
                 long long soften = 0)
 {
     const Dev &d = c->d;
@@ -356,10 +361,12 @@ int launch_step(cs3d_ctx *c, int par, bool div, bool k1 = true, bool fuse = fals
     if (rc) return rc;
     n += NL_LAUNCHES;
     k_s1<false><<<c->grid_cells, SLOTS, sizeof(S1Smem), s>>>(d, par); ++n; pf.mark(s, "s1_con_dis");
-    if (div && fuse) k_s2<true, true><<<c->grid_s2, SLOTS, 0, s>>>(d, par);
-    else if (div) k_s2<true, false><<<c->grid_s2, SLOTS, 0, s>>>(d, par);
-    else if (fuse) k_s2<false, true><<<c->grid_s2, SLOTS, 0, s>>>(d, par);
-    else k_s2<false, false><<<c->grid_s2, SLOTS, 0, s>>>(d, par);
+    if (div && fuse == 2) k_s2<true, 2><<<c->grid_s2, SLOTS, 0, s>>>(d, par);
+    else if (div && fuse) k_s2<true, 1><<<c->grid_s2, SLOTS, 0, s>>>(d, par);
+    else if (div) k_s2<true, 0><<<c->grid_s2, SLOTS, 0, s>>>(d, par);
+    else if (fuse == 2) k_s2<false, 2><<<c->grid_s2, SLOTS, 0, s>>>(d, par);
+    else if (fuse) k_s2<false, 1><<<c->grid_s2, SLOTS, 0, s>>>(d, par);
+    else k_s2<false, 0><<<c->grid_s2, SLOTS, 0, s>>>(d, par);
     ++n; pf.mark(s, fuse ? "s2_dis_geom_integrate" : "s2_dis_geom");
     if (div) {
         k_div_select<<<c->n_inst, 256, 0, s>>>(d, par); ++n; pf.mark(s, "div_select");
@@ -381,9 +388,9 @@ bool is_soften_step(const cs3d_ctx *c, long long s)
     return std::find(c->soften_steps.begin(), c->soften_steps.end(), s) != c->soften_steps.end();
 }
 
-int get_graph(cs3d_ctx *c, int par, bool div, bool k1, bool fuse, cudaGraphExec_t *out)
+int get_graph(cs3d_ctx *c, int par, bool div, bool k1, int fuse, cudaGraphExec_t *out)
 {
-    cudaGraphExec_t &g = c->graph[par][div ? 1 : 0][k1 ? 1 : 0][fuse ? 1 : 0];
+    cudaGraphExec_t &g = c->graph[par][div ? 1 : 0][k1 ? 1 : 0][fuse];
     if (!g) {
         cudaGraph_t graph;
         CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
@@ -403,6 +410,20 @@ int ensure_init(cs3d_ctx *c)
 {
     if (!c->need_init) return CS3D_OK;
     return run_init(c);
+}
+
+// After a fused last step d.X and d.V hold the next step's half kick and
+// drift; copy the kept step-end state (d.Xe, d.Vb) back for the operations
+// that read or rebuild from d.X and d.V (the forces and pressures are those of
+// the finished step either way).  The next step then runs k_integrate again.
+int settle(cs3d_ctx *c)
+{
+    if (!c->prekicked) return CS3D_OK;
+    const size_t bytes = sizeof(float4) * (size_t)c->cap_total * SLOTS;
+    CK(cudaMemcpyAsync(c->d.X, c->d.Xe, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d.V, c->d.Vb, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    c->prekicked = false;
+    return CS3D_OK;
 }
 
 int read_errors(cs3d_ctx *c, unsigned *any)
@@ -503,6 +524,7 @@ int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topol
     AL(d.prm, n_inst);
     AL(d.st, n_inst);
     AL(d.X, nodes); AL(d.V, nodes); AL(d.Vb, nodes); AL(d.FC, nodes); AL(d.FD, nodes); AL(d.FR, nodes);
+    AL(d.Xe, nodes);
     AL(d.stage, 6 * nodes);
     AL(d.CM, c->cap_total);
     AL(d.press, c->cap_total); AL(d.E, c->cap_total); AL(d.vol, c->cap_total); AL(d.area, c->cap_total);
@@ -562,7 +584,7 @@ int cs3d_create_ensemble(int n_inst, const cs3d_params *params, const cs3d_topol
     c->grid_nodes = std::max(1, std::min(c->cap_total, c->nsm * std::max(occ_nl, 1)));
     c->grid_tiles = std::max(1, std::min(d.hsize / SCAN_TILE + 1, c->nsm * 8));
     int occ_s2 = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s2, k_s2<true, false>, SLOTS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s2, k_s2<true, 0>, SLOTS, 0);
     c->grid_s2 = std::max(1, std::min(c->cap_total, c->nsm * std::max(occ_s2, 1)));
     *out = c;
     return CS3D_OK;
@@ -615,6 +637,7 @@ int cs3d_set_option(cs3d_ctx *c, int option, long long value)
     case CS3D_OPT_SKIN: {
         float s = (float)value * 1e-6f;
         if (!(s > 0.002f) || s > 1.0f) return CS3D_E_ARG;
+        if (int rc = settle(c)) return rc;   // the re-initialisation starts from the step-end state
         c->skin = s;
         for (auto &q : c->hprm) { q.skin = s; q.rlist = q.ra + s; }
         CK(cudaMemcpyAsync(c->d.prm, c->hprm.data(), sizeof(InstParams) * c->n_inst, cudaMemcpyHostToDevice, c->stream));
@@ -647,6 +670,9 @@ int cs3d_load_state(cs3d_ctx *c, int inst, int n, const float *X, const float *Y
     const InstParams &P = c->hprm[inst];
     if (n > P.cap) return CS3D_E_CAPACITY;
     cudaSetDevice(c->device);
+    // the other instances back to their step-end state: the re-initialisation
+    // that follows a load starts from it
+    if (int rc = settle(c)) return rc;
     const size_t slots = (size_t)P.cap * SLOTS;
     const size_t k = (size_t)n * SLOTS;
     const size_t off0 = (size_t)P.base * SLOTS;
@@ -723,23 +749,29 @@ int cs3d_step(cs3d_ctx *c, int n_steps)
     int rc = ensure_init(c);
     if (rc) return rc;
     CK(cudaEventRecord(c->ev0, c->stream));
-    bool k1 = true;
+    // the previous call's last S2 may already have done this step's half
+    // kick and drift
+    bool k1 = !c->prekicked;
     for (int k = 0; k < n_steps; ++k) {
         long long s = c->host_step + 1;
         int par = (int)((s - 1) & 1);
         bool div = c->any_growth && s <= c->max_div_steps;
         const bool soften = is_soften_step(c, s);
-        bool fuse = !c->any_com && !soften && k + 1 < n_steps;
+        // S2 integrates the next step unless the step shifts or softens
+        // cells after S2 (CoM correction, growth-end softening); on the last
+        // step of the call it also keeps the step-end positions
+        const int fuse = (c->any_com || soften) ? 0 : (k + 1 < n_steps ? 1 : 2);
         if (soften) {
             // the one step that softens cells runs outside the graphs
-            if ((rc = launch_step(c, par, div, k1, false, Prof(), s))) return rc;
+            if ((rc = launch_step(c, par, div, k1, 0, Prof(), s))) return rc;
         } else {
             cudaGraphExec_t g;
             if ((rc = get_graph(c, par, div, k1, fuse, &g))) return rc;
             CK(cudaGraphLaunch(g, c->stream));
         }
         c->host_step = s;
-        k1 = !fuse;
+        k1 = fuse == 0;
+        c->prekicked = fuse == 2;
     }
     CK(cudaEventRecord(c->ev1, c->stream));
     CK(cudaEventSynchronize(c->ev1));
@@ -758,6 +790,8 @@ int cs3d_profile_step(cs3d_ctx *c, int n_steps, float *kernel_ms, char *names, i
     cudaSetDevice(c->device);
     int rc = ensure_init(c);
     if (rc) return rc;
+    // every profiled step launches the same kernels, k_integrate first
+    if ((rc = settle(c))) return rc;
     std::vector<double> acc;
     std::vector<const char *> first_names;
     for (int k = 0; k < n_steps; ++k) {
@@ -772,7 +806,7 @@ int cs3d_profile_step(cs3d_ctx *c, int n_steps, float *kernel_ms, char *names, i
         cudaEvent_t e0;
         CK(cudaEventCreate(&e0));
         CK(cudaEventRecord(e0, c->stream));
-        if ((rc = launch_step(c, par, div, true, false, pf, is_soften_step(c, st) ? st : 0))) return rc;
+        if ((rc = launch_step(c, par, div, true, 0, pf, is_soften_step(c, st) ? st : 0))) return rc;
         c->host_step = st;
         CK(cudaEventSynchronize(ev.empty() ? e0 : ev.back()));
         if (acc.size() < ev.size()) { acc.resize(ev.size(), 0.0); first_names = nm; }
@@ -819,7 +853,8 @@ int cs3d_get_state(cs3d_ctx *c, int inst, int *n_cells, float *X, float *Y, floa
     if (n_cells) *n_cells = n;
     if (X || Y || Z || VX || VY || VZ) {
         float *const out[6] = {X, Y, Z, VX, VY, VZ};
-        if ((rc = fetch_soa(c, inst, n, (X || Y || Z) ? c->d.X : nullptr, (VX || VY || VZ) ? c->d.V : nullptr, out)))
+        const float4 *xs = c->prekicked ? c->d.Xe : c->d.X, *vs = c->prekicked ? c->d.Vb : c->d.V;
+        if ((rc = fetch_soa(c, inst, n, (X || Y || Z) ? xs : nullptr, (VX || VY || VZ) ? vs : nullptr, out)))
             return rc;
     }
     const int base = c->hprm[inst].base;
@@ -859,7 +894,8 @@ int cs3d_get_state_async(cs3d_ctx *c, int inst, int slot, int *n_cells, float *X
     const int base = c->hprm[inst].base;
     const bool wx = X || Y || Z, wv = VX || VY || VZ;
     if (wx || wv)
-        k_unpack<<<c->grid_flat, 256, 0, c->stream>>>(stage, wx ? c->d.X + off : nullptr, wv ? c->d.V + off : nullptr, k);
+        k_unpack<<<c->grid_flat, 256, 0, c->stream>>>(stage, wx ? (c->prekicked ? c->d.Xe : c->d.X) + off : nullptr,
+                                                      wv ? (c->prekicked ? c->d.Vb : c->d.V) + off : nullptr, k);
     CK(cudaGetLastError());
     float *cellv = stage + 6 * k;
     if (pressure) CK(cudaMemcpyAsync(cellv, c->d.press + base, sizeof(float) * n, cudaMemcpyDeviceToDevice, c->stream));
@@ -1043,6 +1079,7 @@ int cs3d_volume_histogram(cs3d_ctx *c, int inst, float lo, float hi, int nbins, 
     cudaSetDevice(c->device);
     int rc = ensure_init(c);
     if (rc) return rc;
+    if ((rc = settle(c))) return rc;   // the volumes of the step-end positions
     int n = 0;
     if ((rc = inst_count(c, inst, &n))) return rc;
     // scratch for the counts and the volumes, freed before returning

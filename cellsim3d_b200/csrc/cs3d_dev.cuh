@@ -96,6 +96,7 @@ struct Dev {
     float4 *X;          // positions (x, y, z, 0), [cell*192 + node]
     float4 *V;          // velocities (state)
     float4 *Vb;         // velocities after the half kicks (v3), read by neighbours
+    float4 *Xe;         // step-end positions kept by the last (fused) S2 of a cs3d_step call
     float4 *FC, *FD;    // forces
     float4 *FR;         // Langevin random force of the last step (zero when off)
     float *stage;       // [6 * cap_total*192] host transfer staging (SoA)

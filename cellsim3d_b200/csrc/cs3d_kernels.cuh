@@ -456,14 +456,16 @@ __device__ __forceinline__ float3 dis_force(const InstParams &P, const T *vd, in
 // PressureUpdate, src/PressureKernels.cu:4-40, for the step `step` being
 // taken: with variable stiffness, from step phase_count on a cell whose
 // stiffness is not stiffness1 has pressure 0; every other cell grows by the
-// growth rate up to maxPressure.
-__device__ __forceinline__ void pressure_update(const Dev &d, const InstParams &P, int a, int step)
+// growth rate up to maxPressure.  The reference runs it after Integrate and
+// ForwardTime and before the forces; here S1 applies it to its cell before
+// the pressure force (nothing in between reads the pressure), so that the
+// stored pressures are always those of the last finished step.
+__device__ __forceinline__ float pressure_update(const Dev &d, const InstParams &P, int a, int step)
 {
-    if (P.diffE && step >= P.phase && d.E[a] != P.stiff1) {
-        if (d.press[a] != 0.0f) d.press[a] = 0.0f;
-    } else if (d.press[a] < P.maxp) {
-        d.press[a] = d.press[a] + P.growth;
-    }
+    const float p = d.press[a];
+    if (P.diffE && step >= P.phase && d.E[a] != P.stiff1) return 0.0f;
+    if (p < P.maxp) return p + P.growth;
+    return p;
 }
 
 // ---------------------------------------------------------------------------
@@ -509,7 +511,6 @@ __device__ __forceinline__ void integrate_cell(const Dev &d, int a, float *smax)
             float m = smax[0];
             for (int q = 1; q < SLOTS / 32; ++q) m = fmaxf(m, smax[q]);
             atomicMax(&d.st[inst].disp_step, __float_as_uint(m));
-            pressure_update(d, P, a, d.st[inst].step + 1);
         }
         __syncthreads();
     }
@@ -757,6 +758,7 @@ struct S1Smem {
     double3 vd[SLOTS];   // FP64 terms read them without conversions
     SlotData sd;
     ArmForces arm;
+    float press;         // the cell's pressure of this step
 };
 
 template <bool INIT>
@@ -787,6 +789,12 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
         sm.xd[i] = make_double3(x4.x, x4.y, x4.z);
         sm.vd[i] = make_double3(v4.x, v4.y, v4.z);
         slots_load(d, a, &d.st[inst], par, sm.sd);
+        if (i == 0) {
+            // this step's PressureUpdate (none before the initial forces)
+            const float pr = INIT ? d.press[a] : pressure_update(d, P, a, d.st[inst].step);
+            if (!INIT) d.press[a] = pr;
+            sm.press = pr;
+        }
         __syncthreads();
         slots_boxes(d, P, par, sm.sd, nc);
         const float3 x = f3(x4);
@@ -836,7 +844,7 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
             {
                 const float4 cm = d.CM[a];
                 const double rx = xi.x - cm.x, ry = xi.y - cm.y, rz = xi.z - cm.z;
-                const double c = 3.0 * (double)d.press[a] * rsqrt_nr(rx * rx + ry * ry + rz * rz);
+                const double c = 3.0 * (double)sm.press * rsqrt_nr(rx * rx + ry * ry + rz * rz);
                 FX += c * rx; FY += c * ry; FZ += c * rz;
             }
             // bond angles, src/propagate.cu:81-181: the vertex terms (minus
@@ -951,10 +959,13 @@ __device__ __forceinline__ void flush_mm(Dev &d, int inst, int pn, const float *
     }
 }
 
-// FUSE (steps without division that are followed by another step of the
-// same launch sequence): the first half kick and drift of the next step
-// (k_integrate) are done here, on the force and velocity in registers.
-template <bool DIV, bool FUSE>
+// FUSE: the first half kick and drift of the next step (k_integrate) are
+// done here, on the force and velocity in registers: FUSE 1 when the next
+// step follows in the same launch sequence, FUSE 2 on the last step of a
+// cs3d_step call, which also keeps the step-end positions (Xe; the step-end
+// velocities are Vb) for the state read-back, so that the next call starts
+// without a k_integrate pass.
+template <bool DIV, int FUSE>
 __global__ void __launch_bounds__(SLOTS, 5) k_s2(Dev d, int par)
 {
     __shared__ S2Smem sm;
@@ -990,6 +1001,7 @@ __global__ void __launch_bounds__(SLOTS, 5) k_s2(Dev d, int par)
 
             d.FD[g] = make_float4(fd.x, fd.y, fd.z, 0.f);
             fdk = fd;
+            if (FUSE == 2 && !DIV) d.Xe[g] = x4;
             if (FUSE && !DIV) disp = next_kick(d, P, g, x4, v4, fd);
             else d.V[g] = v4;
         }
@@ -1026,6 +1038,7 @@ __global__ void __launch_bounds__(SLOTS, 5) k_s2(Dev d, int par)
             // a division after their placement (k_integrate_divided).
             __syncthreads();
             const bool divides = sm.dflag != 0;   // uniform
+            if (FUSE == 2 && !divides && i < NODES) d.Xe[g] = x4;
             if (!divides && i < NODES) disp = next_kick(d, P, g, x4, v4, fdk);
             for (int o = 16; o > 0; o >>= 1) disp = fmaxf(disp, __shfl_xor_sync(0xffffffffu, disp, o));
             if ((i & 31) == 0) smax[i >> 5] = disp;
@@ -1036,7 +1049,6 @@ __global__ void __launch_bounds__(SLOTS, 5) k_s2(Dev d, int par)
                 float mx = smax[0];  // visible: cell_geom (and the division decision) synchronise the block
                 for (int q = 1; q < SLOTS / 32; ++q) mx = fmaxf(mx, smax[q]);
                 atomicMax(&st->disp_step, __float_as_uint(mx));
-                pressure_update(d, P, a, st->step + 1);  // the next step's PressureUpdate
             }
             d.CM[a] = make_float4(cm.x, cm.y, cm.z, 0.f);
             d.aabb[pn][2 * a] = lo;
@@ -1260,6 +1272,9 @@ __global__ void __launch_bounds__(SLOTS) k_div_apply(Dev d, int par)
             d.X[gb] = xb;
             d.Xb[ga] = xa;   // new anchors of the displacement test
             d.Xb[gb] = xb;
+            d.Xe[ga] = xa;   // step-end state of the two cells (read back after a fused last step)
+            d.Xe[gb] = xb;
+            d.Vb[gb] = d.Vb[ga];
             d.V[gb] = d.V[ga];
             d.FC[gb] = make_float4(0, 0, 0, 0);
             d.FD[gb] = make_float4(0, 0, 0, 0);
