@@ -470,7 +470,7 @@ __device__ __forceinline__ float pressure_update(const Dev &d, const InstParams 
 
 // ---------------------------------------------------------------------------
 // K1: first half kick + drift of a step (Integrate + ForwardTime,
-// src/propagate.cu:681-763) and PressureUpdate (src/PressureKernels.cu:4-40).
+// src/propagate.cu:681-763).  The step's PressureUpdate is S1's.
 // ---------------------------------------------------------------------------
 // One cell, called by the whole block (it synchronises).
 __device__ __forceinline__ void integrate_cell(const Dev &d, int a, float *smax)
