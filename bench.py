@@ -60,25 +60,37 @@ class ClockSampler:
     def __init__(self, device_index=0):
         self.idx = device_index
         self.proc = None
-        self.lines = []
+        self.lines = []   # (arrival time, line)
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # the timed region starts once nvidia-smi is sampling
+            t = time.perf_counter()
+            while not self.lines and time.perf_counter() - t < 5.0 and self.proc.poll() is None:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
+        self.t0 = time.perf_counter()
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
 
     def __exit__(self, *a):
+        self.t1 = time.perf_counter()
         if self.proc:
+            # one more sample after the region (a short region may hold none)
+            n = len(self.lines)
+            t = time.perf_counter()
+            while len(self.lines) == n and time.perf_counter() - t < 0.5 and self.proc.poll() is None:
+                time.sleep(0.01)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -88,7 +100,11 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        # samples taken during the timed region, plus the first one after it
+        # (nvidia-smi reports the state at the sample time)
+        inside = [ln for t, ln in self.lines if self.t0 is not None and self.t0 <= t <= self.t1]
+        after = [ln for t, ln in self.lines if self.t1 is not None and t > self.t1][:1]
+        for ln in inside + after:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
