@@ -507,7 +507,12 @@ def run_reference(args):
                 raise RuntimeError("reference stopped in the warm-up: " + r["status_text"])
             total_ms += r["total_ms"] - r["guard_ms"]
             inst_ms.append((r["total_ms"] - r["guard_ms"]) / timed)
-            node_steps += 0.5 * (st["n"] + r["n"]) * 180 * timed   # cell count grows by division
+            # cell count grows by division: the trapezoid between the counts at
+            # the start of the timed steps (after the warm-up's divisions) and
+            # at the end, as the CUDA arm counts
+            ev = np.asarray(r["events"]).reshape(-1, 3)
+            n_t0 = st["n"] + int(np.count_nonzero(ev[:, 0] <= args.warmup))
+            node_steps += 0.5 * (n_t0 + r["n"]) * 180 * timed
             cells0 += st["n"]
             statuses.add(r["status_text"])
             max_bin, max_nn = max(max_bin, r["max_bin"]), max(max_nn, r["max_local_nn"])
@@ -522,11 +527,15 @@ def run_reference(args):
             conc = time.perf_counter() - t0
     value = node_steps / (total_ms * 1e-3)
     extra = {}
+    if args.workload in ENSEMBLES:
+        # whole simulations per hour, the timed steps standing for the run of
+        # warmup + steps steps (as the CUDA arm reports it)
+        run_s = total_ms * 1e-3 * (args.warmup + args.steps) / args.steps
+        extra = {"steps_per_sim": args.warmup + args.steps, "sims_per_hour_sequential": len(insts) * 3600.0 / run_s}
     if conc is not None:
-        extra = {"sequential_node_steps_per_s": value, "concurrent_node_steps_per_s": node_steps / conc,
-                 "concurrent_processes": args.ref_concurrency,
-                 "sims_per_hour_sequential": len(insts) * 3600.0 / (total_ms * 1e-3),
-                 "sims_per_hour_concurrent": len(insts) * 3600.0 / conc}
+        extra.update({"sequential_node_steps_per_s": value, "concurrent_node_steps_per_s": node_steps / conc,
+                      "concurrent_processes": args.ref_concurrency,
+                      "sims_per_hour_concurrent": len(insts) * 3600.0 / conc})
         value = max(value, node_steps / conc)
     if len(inst_ms) > 1:
         extra["instance_step_ms_p50"] = float(np.percentile(inst_ms, 50))

@@ -5,6 +5,7 @@ import os
 import sys
 
 import numpy as np
+import pytest
 
 sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 import bench  # noqa: E402
@@ -111,3 +112,30 @@ def test_both_arms_print_the_same_config():
         b = bench.workload_config(name, bench.build_workload(name, 2000, steps=10))
         assert a == b
         assert set(a) == {"workload", "cells", "nodes", "instances", "parallelism", "l2"}
+
+
+def test_reference_arm_counts_node_steps_from_the_cells_after_the_warmup(monkeypatch):
+    """The reference arm's node-steps start from the cells present after the
+    warm-up (initial cells plus the warm-up's divisions), as the CUDA arm's
+    do, and its sims/hr cover warmup + steps steps.  The harness run is
+    stubbed: 8 initial cells, all dividing at step 1 of a 3-step warm-up,
+    then 2 more divisions; 10 timed steps of 1 ms each."""
+    from oracle import ref
+    monkeypatch.setattr(ref, "available", lambda: True)
+
+    def fake_run(p, mesh, st, cap, steps, warmup=0, **kw):
+        ev = [(1, c, 8 + c) for c in range(st["n"])] + [(6, 0, 2 * st["n"]), (9, 1, 2 * st["n"] + 1)]
+        return {"steps": steps, "n": 2 * st["n"] + 2, "total_ms": 10.0, "guard_ms": 0.0, "events": np.array(ev),
+                "status_text": "ok", "max_bin": 1, "max_local_nn": 1}
+    monkeypatch.setattr(ref, "run", fake_run)
+    monkeypatch.setattr(bench.workloads(), "load_mesh", lambda: None)
+    args = bench.argparse.Namespace(workload="small8", cells=8, warmup=3, steps=10, ref_sample=0,
+                                    ref_concurrency=1, gpus=1, cpu_cells=8, cpu_steps=1)
+    monkeypatch.setattr(bench, "build_workload",
+                        lambda *a, **k: [({}, {"n": 8}, 64)])
+    line = bench.run_reference(args)
+    # 16 cells after the warm-up, 18 at the end: 17 on average over 10 steps in 10 ms
+    assert line["value"] == pytest.approx(17 * 180 * 10 / 10e-3)
+    args.workload = "het64"
+    line = bench.run_reference(args)
+    assert line["ensemble"]["sims_per_hour_sequential"] == pytest.approx(3600.0 / (10e-3 * 13 / 10))
