@@ -36,7 +36,7 @@ NODE_BYTES = 48  # algorithmic bytes per node-step: float32 x and v, read and wr
 # DRAM bytes (read + write) per node of one k_s1 launch: ncu's dram__bytes_read.sum
 # and dram__bytes_write.sum of one launch on 30k packed cells (5.4M nodes: 387.5 MB
 # + 213.7 MB), scaled by the nodes of the launch
-S1_TRAFFIC_PER_NODE = 111.3
+S1_TRAFFIC_PER_NODE = 111.8
 ENSEMBLES = ("ensemble256", "het64")
 _WORKLOADS = {}
 
@@ -291,13 +291,18 @@ def run_cs3d(args, world, rank, local):
         t0 = time.perf_counter()
         for k, (n, h, pr, yg) in enumerate(host):
             ens.load_state(k, h["X"], h["Y"], h["Z"], h["VX"], h["VY"], h["VZ"], pressure=pr, youngs=yg, n_cells=n)
+        t_load = time.perf_counter()
         for _ in range(args.steps):
             ens.step(1)
+        t_steps = time.perf_counter()
         outs = [ens.state(k, out=res[k]) for k in range(len(insts))]
         t1 = time.perf_counter()
         n_in = sum(h[0] for h in host)
         n_out = sum(o["n"] for o in outs)
         # node-steps at the starting cell counts (divisions during the K steps not counted)
+        # wall-clock split (rank 0's): the upload, the K calls (the first
+        # one re-initialises: list build and initial forces), the read-back
+        split_ms = {"load": 1e3 * (t_load - t0), "steps": 1e3 * (t_steps - t_load), "read": 1e3 * (t1 - t_steps)}
         e2e = {"seconds": t1 - t0, "node_steps": n_in * 180 * args.steps,
                "h2d": (6 * 4 * n_in * 192 + 8 * n_in) / args.steps,
                "d2h": (6 * 4 * n_out * 192 + 4 * len(insts)) / args.steps + 4 * len(insts)}
@@ -365,7 +370,8 @@ def run_cs3d(args, world, rank, local):
                              "unit": "node-steps/s", "h2d_bytes_per_step": int(e2e_h2d),
                              "d2h_bytes_per_step": int(e2e_d2h),
                              "how": "cs3d_load_state of the timed region's starting state from pinned host, "
-                                    "K x cs3d_step(1) with status read-back, cs3d_get_state to host"}
+                                    "K x cs3d_step(1) with status read-back, cs3d_get_state to host",
+                             "split_ms_rank0": {k: round(v, 3) for k, v in split_ms.items()}}
     ens.close()
     if dist:
         dist.barrier()

@@ -656,6 +656,7 @@ struct GeomScratch {
     double sum[SLOTS / 32][3];
     float mn[SLOTS / 32][3], mx[SLOTS / 32][3];
     double vol[SLOTS / 32], area[SLOTS / 32];
+    double fc[CS3D_FACES][3];   // face centres relative to the cell's centre of mass
 };
 
 // Centre of mass (FP64 sum, src/centermass.cu:8-50) and bounding box
@@ -697,38 +698,50 @@ __device__ __forceinline__ void cell_geom(const float4 *xs, GeomScratch &gs, flo
     hi = make_float4(b0, b1, b2, 0.0f);
 }
 
-// Volume, area and the division test, src/volume.cu:5-163, in FP64.
+// Volume, area and the division test, src/volume.cu:5-163, in FP64.  Each
+// face (12 pentagons, 80 hexagons, vertices relative to the cell's centre of
+// mass) is cut into triangles at its vertex average; the volume is the sum
+// of |det| / 6 of the tetrahedra (centre of mass, triangle) and the area the
+// sum of the triangle areas.  The face centres first (one thread per face),
+// then the 552 triangles dealt out to all threads.
 __device__ __noinline__ void cell_volume(const Dev &d, const float4 *xs, float3 cm, GeomScratch &gs, bool sph,
                                          double &vol, double &area)
 {
-    int t = threadIdx.x, w = t >> 5, l = t & 31;
-    double tv = 0, fa = 0;
+    const int t = threadIdx.x, w = t >> 5, l = t & 31;
+    const double cx = cm.x, cy = cm.y, cz = cm.z;
     if (t < CS3D_FACES) {
         const uint8_t *F = d.topo.faces + 7 * t;
-        double lx[7], ly[7], lz[7];
-        for (int q = 0; q < 7; ++q) {
-            float4 p = xs[F[q]];
-            lx[q] = (double)p.x - (double)cm.x;
-            ly[q] = (double)p.y - (double)cm.y;
-            lz[q] = (double)p.z - (double)cm.z;
-        }
         double ax = 0, ay = 0, az = 0;
-        for (int q = 0; q < 5; ++q) { ax += lx[q]; ay += ly[q]; az += lz[q]; }
+        for (int q = 0; q < 5; ++q) {
+            const float4 p = xs[F[q]];
+            ax += (double)p.x - cx; ay += (double)p.y - cy; az += (double)p.z - cz;
+        }
         double fac = (double)0.166666667f;
         if (t < 12) fac = (double)0.2f;
-        else { ax += lx[5]; ay += ly[5]; az += lz[5]; }
-        ax *= fac; ay *= fac; az *= fac;
-        for (int q = 0; q < 6; ++q) {
-            double n1 = (ly[q + 1] * az - ay * lz[q + 1]) * lx[q];
-            double n2 = (lz[q + 1] * ax - az * lx[q + 1]) * ly[q];
-            double n3 = (lx[q + 1] * ay - ax * ly[q + 1]) * lz[q];
-            tv += fabs(n1 + n2 + n3);
-            if (sph) {
-                double x1 = lx[q] - ax, y1 = ly[q] - ay, z1 = lz[q] - az;
-                double x2 = lx[q + 1] - ax, y2 = ly[q + 1] - ay, z2 = lz[q + 1] - az;
-                double xx = y1 * z2 - z1 * y2, yy = z1 * x2 - x1 * z2, zz = x1 * y2 - y1 * x2;
-                fa += 0.5 * sqrt(xx * xx + yy * yy + zz * zz);
-            }
+        else {
+            const float4 p = xs[F[5]];
+            ax += (double)p.x - cx; ay += (double)p.y - cy; az += (double)p.z - cz;
+        }
+        gs.fc[t][0] = ax * fac; gs.fc[t][1] = ay * fac; gs.fc[t][2] = az * fac;
+    }
+    __syncthreads();
+    double tv = 0, fa = 0;
+    for (int k = t; k < CS3D_FACES * 6; k += SLOTS) {
+        const int f = k / 6, q = k - 6 * f;
+        const uint8_t *F = d.topo.faces + 7 * f;
+        const float4 p0 = xs[F[q]], p1 = xs[F[q + 1]];
+        const double x0 = (double)p0.x - cx, y0 = (double)p0.y - cy, z0 = (double)p0.z - cz;
+        const double x1 = (double)p1.x - cx, y1 = (double)p1.y - cy, z1 = (double)p1.z - cz;
+        const double ax = gs.fc[f][0], ay = gs.fc[f][1], az = gs.fc[f][2];
+        const double n1 = (y1 * az - ay * z1) * x0;
+        const double n2 = (z1 * ax - az * x1) * y0;
+        const double n3 = (x1 * ay - ax * y1) * z0;
+        tv += fabs(n1 + n2 + n3);
+        if (sph) {
+            const double u1 = x0 - ax, v1 = y0 - ay, w1 = z0 - az;
+            const double u2 = x1 - ax, v2 = y1 - ay, w2 = z1 - az;
+            const double xx = v1 * w2 - w1 * v2, yy = w1 * u2 - u1 * w2, zz = u1 * v2 - v1 * u2;
+            fa += 0.5 * sqrt(xx * xx + yy * yy + zz * zz);
         }
     }
     tv = warp_sum(tv);
