@@ -120,6 +120,25 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def apply_skin_schedule(ens, args):
+    """--skin-schedule FILE: the neighbour-list skin by population range
+    (a schedule written by `python -m cellsim3d_b200.autotune`).  It changes
+    the time only, not the results."""
+    if args.skin_schedule:
+        from cellsim3d_b200 import autotune
+        ens.set_skin_schedule(*autotune.load_schedule(args.skin_schedule))
+
+
+def skin_info(args):
+    """The neighbour-list skin of the run, for the JSON line."""
+    out = {"skin": args.skin if args.skin is not None else 0.1}
+    if args.skin_schedule:
+        from cellsim3d_b200 import autotune
+        mc, sk = autotune.load_schedule(args.skin_schedule)
+        out["schedule"] = {"min_cells": mc, "skins": sk, "file": os.path.basename(args.skin_schedule)}
+    return out
+
+
 def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -249,6 +268,7 @@ def run_cs3d(args, world, rank, local):
     ens = cs.Ensemble([p for p, _, _ in insts], topo, [cap for _, _, cap in insts], device=local)
     if args.skin is not None:
         ens.set_option(cs.OPT_SKIN, int(round(args.skin * 1e6)))
+    apply_skin_schedule(ens, args)
     for k, (p, st, cap) in enumerate(insts):
         ens.load_state(k, st["X"], st["Y"], st["Z"], st.get("VX"), st.get("VY"), st.get("VZ"), n_cells=st["n"])
     n_nodes0 = sum(st["n"] for _, st, _ in insts) * 180
@@ -352,6 +372,7 @@ def run_cs3d(args, world, rank, local):
             "nl_rebuilds": stats["rebuilds"],
             "max_entries": stats["max_entries"],
             "max_cand": stats["max_cand"],
+            "list_skin": skin_info(args),
             "clocks": clk.summary(),
         }
         if args.workload in ENSEMBLES:
@@ -416,6 +437,9 @@ def run_colony(args):
     (p, st, cap), = build_workload("colony", args.cells)
     topo = make_topology([(p, st, cap)])
     sim = cs.Simulation(p, topo, cap)
+    if args.skin is not None:
+        sim.set_option(cs.OPT_SKIN, int(round(args.skin * 1e6)))
+    apply_skin_schedule(sim, args)
     sim.load_state(st["X"], st["Y"], st["Z"], n_cells=st["n"])
     sim.step(max(args.warmup, 3))
     sim.load_state(st["X"], st["Y"], st["Z"], n_cells=st["n"])
@@ -440,6 +464,7 @@ def run_colony(args):
             "unit": "node-steps/s", "n_gpus": 1, "steps": total, "warmup": args.warmup,
             "ms_per_step": elapsed / total, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (one cell, cellsim3d_b200/workloads.py config2)",
+            "list_skin": skin_info(args),
             "config": {"workload": "colony", "cells_end": int(cells_end), "capacity": cap,
                        "timing": "launches of %d steps, CUDA events" % chunk},
             "decades": dec, "clocks": clk.summary()}
@@ -614,6 +639,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--skin", type=float, default=None,
                     help="neighbour-list skin (default: the library's, 0.1)")
+    ap.add_argument("--skin-schedule", default=None,
+                    help="skin by population range, a file written by python -m cellsim3d_b200.autotune")
     ap.add_argument("--colony-max-steps", type=int, default=40000,
                     help="colony: stop after this many steps if 4096 cells are not reached")
     ap.add_argument("--instances", type=int, default=0,

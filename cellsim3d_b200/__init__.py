@@ -214,6 +214,18 @@ class Ensemble:
     def set_option(self, option, value):
         _lib.check(_lib.lib().cs3d_set_option(self.h, option, int(value)), "cs3d_set_option")
 
+    def set_skin_schedule(self, min_cells=(), skins=()):
+        """Neighbour-list skin by population range (cs3d_set_skin_schedule):
+        an instance with at least min_cells[k] cells steps with skins[k];
+        empty sequences clear the schedule.  Changes the time, not the
+        results."""
+        mc = np.ascontiguousarray(min_cells, dtype=np.int32)
+        sk = np.ascontiguousarray(skins, dtype=np.float32)
+        if mc.shape != sk.shape or mc.ndim != 1:
+            raise ValueError("min_cells and skins must be 1-D sequences of one length")
+        _lib.check(_lib.lib().cs3d_set_skin_schedule(self.h, int(mc.size), _ip(mc), _fp(sk)),
+                   "cs3d_set_skin_schedule")
+
     # -- stepping
     def step(self, n=1, raise_on_error=True):
         st = _lib.lib().cs3d_step(self.h, int(n))

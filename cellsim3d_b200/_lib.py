@@ -85,7 +85,7 @@ EXPORTS = [
     "cs3d_get_forces", "cs3d_get_random_force", "cs3d_get_cells", "cs3d_get_grid", "cs3d_set_option", "cs3d_get_pairs",
     "cs3d_get_events", "cs3d_get_far_counts", "cs3d_volume_histogram", "cs3d_last_error", "cs3d_get_stats", "cs3d_profile_step", "cs3d_last_step_ms",
     "cs3d_destroy", "cs3d_forces_static", "cs3d_get_state_async", "cs3d_wait_state", "cs3d_host_alloc",
-    "cs3d_host_free",
+    "cs3d_host_free", "cs3d_set_skin_schedule",
 ]
 
 _lib = None
@@ -146,6 +146,7 @@ def lib():
     L.cs3d_get_cells.argtypes = [P, C.c_int, fp, fp, fp, fp]
     L.cs3d_get_grid.argtypes = [P, C.c_int, fp, ip]
     L.cs3d_set_option.argtypes = [P, C.c_int, C.c_longlong]
+    L.cs3d_set_skin_schedule.argtypes = [P, C.c_int, ip, fp]
     L.cs3d_get_pairs.argtypes = [P, C.c_int, C.c_int, ip, C.c_longlong, C.POINTER(C.c_longlong)]
     L.cs3d_get_events.argtypes = [P, C.c_int, ip, C.c_int, ip]
     L.cs3d_get_far_counts.argtypes = [P, C.c_int, ip, C.c_int, ip]

@@ -207,6 +207,7 @@ InstParams make_inst(const cs3d_params &p, int base, int cap, float skin)
     q.rsE = rs * E;
     q.wallk = 100.0f * E;
     q.skin = skin;
+    q.skin_base = skin;
     q.rlist = p.attraction_range + skin;
     q.check_sph = p.check_sphericity;
     q.angles = p.constrain_angles;
@@ -606,6 +607,34 @@ int cs3d_destroy(cs3d_ctx *c)
     return CS3D_OK;
 }
 
+int cs3d_set_skin_schedule(cs3d_ctx *c, int n, const int *min_cells, const float *skins)
+{
+    if (!c || n < 0 || n > CS3D_SKIN_RANGES || (n > 0 && (!min_cells || !skins))) return CS3D_E_ARG;
+    for (int k = 0; k < n; ++k) {
+        if (min_cells[k] < 1 || (k > 0 && min_cells[k] <= min_cells[k - 1])) return CS3D_E_ARG;
+        if (!(skins[k] > 0.002f) || skins[k] > 1.0f) return CS3D_E_ARG;
+    }
+    cudaSetDevice(c->device);
+    for (auto &q : c->hprm) {
+        q.sk_n = n;
+        for (int k = 0; k < CS3D_SKIN_RANGES; ++k) {
+            q.sk_min[k] = k < n ? min_cells[k] : 0;
+            q.sk_val[k] = k < n ? skins[k] : 0.0f;
+        }
+    }
+    // only the schedule fields: the device keeps the skin in use (and so
+    // its lists) until the next step compares it with the schedule
+    for (int k = 0; k < c->n_inst; ++k) {
+        InstParams *dp = c->d.prm + k;
+        const InstParams &hp = c->hprm[k];
+        CK(cudaMemcpyAsync(&dp->sk_n, &hp.sk_n, sizeof hp.sk_n, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(dp->sk_min, hp.sk_min, sizeof hp.sk_min, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(dp->sk_val, hp.sk_val, sizeof hp.sk_val, cudaMemcpyHostToDevice, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return CS3D_OK;
+}
+
 int cs3d_set_option(cs3d_ctx *c, int option, long long value)
 {
     if (!c) return CS3D_E_ARG;
@@ -639,7 +668,7 @@ int cs3d_set_option(cs3d_ctx *c, int option, long long value)
         if (!(s > 0.002f) || s > 1.0f) return CS3D_E_ARG;
         if (int rc = settle(c)) return rc;   // the re-initialisation starts from the step-end state
         c->skin = s;
-        for (auto &q : c->hprm) { q.skin = s; q.rlist = q.ra + s; }
+        for (auto &q : c->hprm) { q.skin = s; q.skin_base = s; q.rlist = q.ra + s; }
         CK(cudaMemcpyAsync(c->d.prm, c->hprm.data(), sizeof(InstParams) * c->n_inst, cudaMemcpyHostToDevice, c->stream));
         c->need_init = true;
         break;

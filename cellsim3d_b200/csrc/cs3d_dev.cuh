@@ -27,7 +27,11 @@ struct InstParams {
     float rsE;      // fl(rs*E), repulsion coefficient
     float wallk;    // fl(100*E), rigid-box wall stiffness, src/propagate.cu:481
     float rlist;    // neighbour-list radius (ra + skin)
-    float skin;
+    float skin;     // skin in use (set by the device from the schedule)
+    float skin_base;            // the context's skin (CS3D_OPT_SKIN)
+    int sk_n;                   // skin schedule by population: ranges in use
+    int sk_min[CS3D_SKIN_RANGES];    // lowest cell count of each range, ascending
+    float sk_val[CS3D_SKIN_RANGES];  // skin of each range
     int check_sph, angles, rigid, daught_same, div_steps;
     int base, cap;
     int rands;      // Langevin random force on

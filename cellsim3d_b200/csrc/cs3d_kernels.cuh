@@ -293,17 +293,7 @@ __device__ __forceinline__ bool pred_ok(SlotPred &sp, const SlotData &sd, const 
 
 constexpr int EPRE = 8;  // entries prefetched per node at the start of a cell
 constexpr int SB = 4;    // entries whose partner loads are in flight together
-
-// Entry k of a node: from the prefetched words (two entries each) or global.
-__device__ __forceinline__ unsigned entry_at(const uint16_t *ep, const uint32_t (&pre)[EPRE / 2], int k)
-{
-    if (k >= EPRE) return ep[(size_t)k * SLOTS];
-    uint32_t w = 0;
-#pragma unroll
-    for (int r = 0; r < EPRE / 2; ++r)
-        if ((k >> 1) == r) w = pre[r];
-    return (k & 1) ? (w >> 16) : (w & 0xffffu);
-}
+static_assert(EPRE == 2 * SB && SB == 4, "the sweep's entry window is two batches of four entries");
 
 // ---------------------------------------------------------------------------
 // S1 contact sweep of node i over its entries: conservative contact force
@@ -324,10 +314,25 @@ __device__ __forceinline__ int sweep_s1(const Dev &d, const InstParams &P, const
     SlotPred sp;
     pred_init(sp, sd, x);
     int nd = 0;
+    // a window of two batches of entries in registers (two per word): the
+    // current batch, and the next one, loaded a batch ahead
+    uint32_t w0 = pre[0], w1 = pre[1], w2 = pre[2], w3 = pre[3];
     for (int k0 = 0; k0 < ne; k0 += SB) {
         unsigned e[SB];
+        e[0] = w0 & 0xffffu;
+        e[1] = k0 + 1 < ne ? (w0 >> 16) : 0xffffu;
+        e[2] = k0 + 2 < ne ? (w1 & 0xffffu) : 0xffffu;
+        e[3] = k0 + 3 < ne ? (w1 >> 16) : 0xffffu;
+        w0 = w2;
+        w1 = w3;
+        {
+            const int kn = k0 + 2 * SB;
+            unsigned f[SB];
 #pragma unroll
-        for (int q = 0; q < SB; ++q) e[q] = (k0 + q < ne) ? entry_at(ep, pre, k0 + q) : 0xffffu;
+            for (int q = 0; q < SB; ++q) f[q] = kn + q < ne ? ep[(size_t)(kn + q) * SLOTS] : 0xffffu;
+            w2 = f[0] | (f[1] << 16);
+            w3 = f[2] | (f[3] << 16);
+        }
         int id[SB];
 #pragma unroll
         for (int q = 0; q < SB; ++q) {
@@ -595,6 +600,19 @@ __global__ void __launch_bounds__(256) k_step_begin(Dev d, int par_next)
         // already large.
         const float ds = __uint_as_float(st->disp_step);
         st->disp_step = 0u;
+        if (P.sk_n > 0) {
+            // the skin of the instance's population range; a change is a
+            // whole-instance rebuild with the new list radius
+            float want = P.skin_base;
+            for (int q = 0; q < P.sk_n; ++q)
+                if (st->n >= P.sk_min[q]) want = P.sk_val[q];
+            if (want != P.skin) {
+                InstParams *Pw = &d.prm[k];
+                Pw->skin = want;
+                Pw->rlist = Pw->ra + want;
+                st->force_rebuild = 1;
+            }
+        }
         const bool full = st->force_rebuild || !(2.0f * ds + 1e-3f < P.skin) ||
                           (st->div_count > 0 && ds > 0.25f * P.skin);
         const bool part = !full && st->div_count > 0;

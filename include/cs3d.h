@@ -282,6 +282,23 @@ int cs3d_set_rng(cs3d_ctx *ctx, int inst, const cs3d_rng *rng);
 /* Current RANMAR state of instance inst (the stream the divisions draw from). */
 int cs3d_get_rng(cs3d_ctx *ctx, int inst, cs3d_rng *rng);
 
+/* Neighbour-list skin by population range, for every instance: an instance
+ * with at least min_cells[k] cells (ascending bounds) steps with skins[k],
+ * below min_cells[0] with the context's skin (CS3D_OPT_SKIN).  The device
+ * applies it at the start of each step from the instance's current cell
+ * count; a change takes effect with a whole-instance list rebuild in that
+ * step.  The skin changes no result -- the contact-pair sets and the order
+ * in which the force sums run do not depend on it -- only the time (longer
+ * lists against fewer rebuilds), so a schedule picked by timing
+ * (cellsim3d_b200.autotune) is safe to apply.  n = 0 clears it.  No
+ * counterpart in the reference, whose contact grid has a fixed spacing
+ * (src/GPUbounce.cu:756) and whose launch shapes are fixed (one block per
+ * cell, src/GPUbounce.cu:1059-1151).  CS3D_E_ARG for n < 0, n >
+ * CS3D_SKIN_RANGES, bounds not strictly ascending or below 1, or a skin
+ * outside (0.002, 1]. */
+#define CS3D_SKIN_RANGES 8
+int cs3d_set_skin_schedule(cs3d_ctx *ctx, int n, const int *min_cells, const float *skins);
+
 /* Advance every instance by n_steps timesteps of src/GPUbounce.cu:1055-1338.
  * Returns CS3D_E_DEVICE_FLAGS or CS3D_E_CAPACITY if a kernel raised an
  * error bit (see cs3d_last_error). */
