@@ -120,22 +120,41 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+SCHEDULES = os.path.join(ROOT, "cellsim3d_b200", "schedules")
+
+
+def schedule_path(args):
+    """The skin schedule of the run: --skin-schedule FILE, or with "auto"
+    the autotuner's schedule for the workload (cellsim3d_b200/schedules/,
+    tuned on a B200) when one exists and no fixed --skin is given; "none"
+    for the library's fixed skin."""
+    s = args.skin_schedule
+    if not s or s == "none":
+        return None
+    if s == "auto":
+        p = os.path.join(SCHEDULES, args.workload + ".json")
+        return p if args.skin is None and os.path.exists(p) else None
+    return s
+
+
 def apply_skin_schedule(ens, args):
-    """--skin-schedule FILE: the neighbour-list skin by population range
-    (a schedule written by `python -m cellsim3d_b200.autotune`).  It changes
-    the time only, not the results."""
-    if args.skin_schedule:
+    """The neighbour-list skin by population range (a schedule written by
+    `python -m cellsim3d_b200.autotune`).  It changes the time only, not
+    the results."""
+    p = schedule_path(args)
+    if p:
         from cellsim3d_b200 import autotune
-        ens.set_skin_schedule(*autotune.load_schedule(args.skin_schedule))
+        ens.set_skin_schedule(*autotune.load_schedule(p))
 
 
 def skin_info(args):
     """The neighbour-list skin of the run, for the JSON line."""
     out = {"skin": args.skin if args.skin is not None else 0.1}
-    if args.skin_schedule:
+    p = schedule_path(args)
+    if p:
         from cellsim3d_b200 import autotune
-        mc, sk = autotune.load_schedule(args.skin_schedule)
-        out["schedule"] = {"min_cells": mc, "skins": sk, "file": os.path.basename(args.skin_schedule)}
+        mc, sk = autotune.load_schedule(p)
+        out["schedule"] = {"min_cells": mc, "skins": sk, "file": os.path.relpath(p, ROOT)}
     return out
 
 
@@ -639,8 +658,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--skin", type=float, default=None,
                     help="neighbour-list skin (default: the library's, 0.1)")
-    ap.add_argument("--skin-schedule", default=None,
-                    help="skin by population range, a file written by python -m cellsim3d_b200.autotune")
+    ap.add_argument("--skin-schedule", default="none",
+                    help="skin by population range: a file written by python -m cellsim3d_b200.autotune, "
+                         "'auto' (the tuned schedule of the workload in cellsim3d_b200/schedules/) or 'none'")
     ap.add_argument("--colony-max-steps", type=int, default=40000,
                     help="colony: stop after this many steps if 4096 cells are not reached")
     ap.add_argument("--instances", type=int, default=0,

@@ -15,8 +15,10 @@ same populations at the same steps.
     sched = tune(make_sim, steps=4000)          # e.g. a colony from one cell
     sim.set_skin_schedule(*sched.schedule())    # applied per instance by the device
 
-Ensembles take the schedule of a colony run: each instance switches by its
-own cell count.
+The device applies a schedule to each instance of an ensemble by the
+instance's own cell count.  An ensemble's step times cannot be split by
+instance, so an ensemble is tuned as one range (`--workload ensemble256` or
+`het64`): one skin for all its instances, picked on its own trajectory.
 """
 import json
 
@@ -145,7 +147,8 @@ def main(argv=None):
     import sys
     sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
     ap = argparse.ArgumentParser(description=main.__doc__)
-    ap.add_argument("--workload", default="colony", choices=["colony", "packed100k"])
+    ap.add_argument("--workload", default="colony", choices=["colony", "packed100k", "ensemble256", "het64"])
+    ap.add_argument("--instances", type=int, default=0, help="ensembles: a stratified subset of this many")
     ap.add_argument("--steps", type=int, default=28000)
     ap.add_argument("--cells", type=int, default=100_000)
     ap.add_argument("--chunk", type=int, default=50)
@@ -153,16 +156,26 @@ def main(argv=None):
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     import bench
-    from . import Simulation
-    (p, st, cap), = bench.build_workload(a.workload, a.cells)
-    topo = bench.make_topology([(p, st, cap)])
+    from . import Ensemble
+    insts = bench.build_workload(a.workload, a.cells, steps=a.steps, instances=a.instances)
+    topo = bench.make_topology(insts)
+    ensemble = a.workload in bench.ENSEMBLES
 
     def make():
-        sim = Simulation(p, topo, cap)
-        sim.load_state(st["X"], st["Y"], st["Z"], st.get("VX"), st.get("VY"), st.get("VZ"), n_cells=st["n"])
-        return sim
+        ens = Ensemble([p for p, _, _ in insts], topo, [cap for _, _, cap in insts])
+        for k, (p, st, cap) in enumerate(insts):
+            ens.load_state(k, st["X"], st["Y"], st["Z"], st.get("VX"), st.get("VY"), st.get("VZ"), n_cells=st["n"])
+        return ens
 
-    res = tune(make, a.steps, skins=[float(x) for x in a.skins.split(",")], chunk=a.chunk)
+    def total(ens):
+        return sum(ens.n_cells(k) for k in range(len(insts)))
+
+    skins = [float(x) for x in a.skins.split(",")]
+    if ensemble:
+        # one range; the same-trajectory check on the total cell count
+        res = tune(make, a.steps, skins=skins, bounds=(1,), chunk=a.chunk, population=total)
+    else:
+        res = tune(make, a.steps, skins=skins, chunk=a.chunk, population=total)
     text = res.to_json()
     if a.out:
         with open(a.out, "w") as f:

@@ -139,3 +139,22 @@ def test_reference_arm_counts_node_steps_from_the_cells_after_the_warmup(monkeyp
     args.workload = "het64"
     line = bench.run_reference(args)
     assert line["ensemble"]["sims_per_hour_sequential"] == pytest.approx(3600.0 / (10e-3 * 13 / 10))
+
+
+def test_skin_schedule_selection(tmp_path):
+    """--skin-schedule: 'none' (the default) and 'auto' without a tuned file
+    or with a fixed --skin give no schedule; 'auto' picks the workload's
+    tuned file; a path is taken as given."""
+    ns = bench.argparse.Namespace
+    assert bench.schedule_path(ns(skin_schedule="none", skin=None, workload="packed100k")) is None
+    assert bench.schedule_path(ns(skin_schedule="auto", skin=None, workload="no_such_workload")) is None
+    tuned = os.path.join(bench.SCHEDULES, "colony.json")
+    assert bench.schedule_path(ns(skin_schedule="auto", skin=None, workload="colony")) == tuned
+    assert bench.schedule_path(ns(skin_schedule="auto", skin=0.08, workload="colony")) is None
+    p = str(tmp_path / "s.json")
+    assert bench.schedule_path(ns(skin_schedule=p, skin=None, workload="colony")) == p
+    from cellsim3d_b200 import autotune
+    mc, sk = autotune.load_schedule(tuned)
+    assert mc and len(mc) == len(sk) and all(0.002 < s <= 1.0 for s in sk)
+    info = bench.skin_info(ns(skin_schedule="auto", skin=None, workload="colony"))
+    assert info["schedule"]["min_cells"] == mc and info["schedule"]["file"] == "cellsim3d_b200/schedules/colony.json"
