@@ -658,7 +658,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--skin", type=float, default=None,
                     help="neighbour-list skin (default: the library's, 0.1)")
-    ap.add_argument("--skin-schedule", default="none",
+    ap.add_argument("--skin-schedule", default="auto",
                     help="skin by population range: a file written by python -m cellsim3d_b200.autotune, "
                          "'auto' (the tuned schedule of the workload in cellsim3d_b200/schedules/) or 'none'")
     ap.add_argument("--colony-max-steps", type=int, default=40000,

@@ -784,7 +784,6 @@ struct ArmForces {
 };
 
 struct S1Smem {
-    float4 xs[SLOTS];
     double3 xd[SLOTS];   // FP64 copies of the positions and velocities: the
     double3 vd[SLOTS];   // FP64 terms read them without conversions
     SlotData sd;
@@ -816,7 +815,6 @@ __global__ void __launch_bounds__(SLOTS, 4) k_s1(Dev d, int par)
         for (int q = 0; q < EPRE / 2; ++q)
             pre[q] = (uint32_t)d.ent[((size_t)a * MAXE + 2 * q) * SLOTS + i] |
                      ((uint32_t)d.ent[((size_t)a * MAXE + 2 * q + 1) * SLOTS + i] << 16);
-        sm.xs[i] = x4;
         sm.xd[i] = make_double3(x4.x, x4.y, x4.z);
         sm.vd[i] = make_double3(v4.x, v4.y, v4.z);
         slots_load(d, a, &d.st[inst], par, sm.sd);

@@ -142,12 +142,15 @@ def test_reference_arm_counts_node_steps_from_the_cells_after_the_warmup(monkeyp
 
 
 def test_skin_schedule_selection(tmp_path):
-    """--skin-schedule: 'none' (the default) and 'auto' without a tuned file
-    or with a fixed --skin give no schedule; 'auto' picks the workload's
-    tuned file; a path is taken as given."""
+    """--skin-schedule: 'none', and 'auto' (the default) without a tuned
+    file or with a fixed --skin, give no schedule; 'auto' picks the
+    workload's tuned file; a path is taken as given.  The default packed
+    workload has no tuned file (its pick did not carry over between
+    windows)."""
     ns = bench.argparse.Namespace
     assert bench.schedule_path(ns(skin_schedule="none", skin=None, workload="packed100k")) is None
     assert bench.schedule_path(ns(skin_schedule="auto", skin=None, workload="no_such_workload")) is None
+    assert bench.schedule_path(ns(skin_schedule="auto", skin=None, workload="packed100k")) is None
     tuned = os.path.join(bench.SCHEDULES, "colony.json")
     assert bench.schedule_path(ns(skin_schedule="auto", skin=None, workload="colony")) == tuned
     assert bench.schedule_path(ns(skin_schedule="auto", skin=0.08, workload="colony")) is None
