@@ -36,7 +36,7 @@ NODE_BYTES = 48  # algorithmic bytes per node-step: float32 x and v, read and wr
 # DRAM bytes (read + write) per node of one k_s1 launch: ncu's dram__bytes_read.sum
 # and dram__bytes_write.sum of one launch on 30k packed cells (5.4M nodes: 387.5 MB
 # + 213.7 MB), scaled by the nodes of the launch
-S1_TRAFFIC_PER_NODE = 111.8
+S1_TRAFFIC_PER_NODE = 112.0
 ENSEMBLES = ("ensemble256", "het64")
 _WORKLOADS = {}
 
