@@ -139,7 +139,7 @@ def schedule_path(args):
 
 def apply_skin_schedule(ens, args):
     """The neighbour-list skin by population range (a schedule written by
-    `python -m cellsim3d_b200.autotune`).  It changes the time only, not
+    `bench.py --autotune`).  It changes the time only, not
     the results."""
     p = schedule_path(args)
     if p:
@@ -156,6 +156,35 @@ def skin_info(args):
         mc, sk = autotune.load_schedule(p)
         out["schedule"] = {"min_cells": mc, "skins": sk, "file": os.path.relpath(p, ROOT)}
     return out
+
+
+def run_autotune(args):
+    """--autotune FILE: the skin autotuner (cellsim3d_b200/autotune.py) on
+    this workload: `--steps` steps per candidate skin (`--tune-skins`) in
+    cs3d_step calls of `--tune-chunk` steps, by population range for a
+    single system, as one range for an ensemble.  Writes the schedule with
+    its timing table to FILE (the format of cellsim3d_b200/schedules/)."""
+    import cellsim3d_b200 as cs
+    from cellsim3d_b200 import autotune
+    insts = build_workload(args.workload, args.cells, steps=args.steps, instances=args.instances)
+    topo = make_topology(insts)
+
+    def make():
+        ens = cs.Ensemble([p for p, _, _ in insts], topo, [cap for _, _, cap in insts])
+        for k, (p, st, cap) in enumerate(insts):
+            ens.load_state(k, st["X"], st["Y"], st["Z"], st.get("VX"), st.get("VY"), st.get("VZ"), n_cells=st["n"])
+        return ens
+
+    def total(ens):
+        return sum(ens.n_cells(k) for k in range(len(insts)))
+
+    skins = [float(x) for x in args.tune_skins.split(",")]
+    bounds = (1,) if args.workload in ENSEMBLES else autotune.DEFAULT_BOUNDS
+    res = autotune.tune(make, args.steps, skins=skins, bounds=bounds, chunk=args.tune_chunk, population=total)
+    text = res.to_json()
+    with open(args.autotune, "w") as f:
+        f.write(text + "\n")
+    return text
 
 
 def dist_env():
@@ -658,8 +687,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--skin", type=float, default=None,
                     help="neighbour-list skin (default: the library's, 0.1)")
+    ap.add_argument("--autotune", default=None, metavar="FILE",
+                    help="tune the list skin on this workload (--steps steps per candidate) and write the schedule")
+    ap.add_argument("--tune-skins", default="0.05,0.07,0.1,0.13")
+    ap.add_argument("--tune-chunk", type=int, default=50)
     ap.add_argument("--skin-schedule", default="auto",
-                    help="skin by population range: a file written by python -m cellsim3d_b200.autotune, "
+                    help="skin by population range: a file written by --autotune, "
                          "'auto' (the tuned schedule of the workload in cellsim3d_b200/schedules/) or 'none'")
     ap.add_argument("--colony-max-steps", type=int, default=40000,
                     help="colony: stop after this many steps if 4096 cells are not reached")
@@ -677,6 +710,10 @@ def main():
         if rank != 0:
             return
         print(json.dumps(run_reference(args)))
+        return
+    if args.autotune:
+        if rank == 0:
+            print(run_autotune(args))
         return
     if args.workload == "colony":
         if rank == 0:

@@ -15,10 +15,13 @@ same populations at the same steps.
     sched = tune(make_sim, steps=4000)          # e.g. a colony from one cell
     sim.set_skin_schedule(*sched.schedule())    # applied per instance by the device
 
+`python bench.py --workload colony --steps 28000 --autotune FILE` tunes a
+benchmark workload and writes the schedule with its timing table.
+
 The device applies a schedule to each instance of an ensemble by the
 instance's own cell count.  An ensemble's step times cannot be split by
-instance, so an ensemble is tuned as one range (`--workload ensemble256` or
-`het64`): one skin for all its instances, picked on its own trajectory.
+instance, so an ensemble is tuned as one range (bounds=(1,)): one skin for
+all its instances, picked on its own trajectory.
 """
 import json
 
@@ -138,50 +141,3 @@ def load_schedule(path):
     with open(path) as f:
         d = json.load(f)
     return list(d["min_cells"]), [float(x) for x in d["skins"]]
-
-
-def main(argv=None):
-    """python -m cellsim3d_b200.autotune --workload colony --steps 28000 --out FILE"""
-    import argparse
-    import os
-    import sys
-    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
-    ap = argparse.ArgumentParser(description=main.__doc__)
-    ap.add_argument("--workload", default="colony", choices=["colony", "packed100k", "ensemble256", "het64"])
-    ap.add_argument("--instances", type=int, default=0, help="ensembles: a stratified subset of this many")
-    ap.add_argument("--steps", type=int, default=28000)
-    ap.add_argument("--cells", type=int, default=100_000)
-    ap.add_argument("--chunk", type=int, default=50)
-    ap.add_argument("--skins", default=",".join(str(s) for s in DEFAULT_SKINS))
-    ap.add_argument("--out", default=None)
-    a = ap.parse_args(argv)
-    import bench
-    from . import Ensemble
-    insts = bench.build_workload(a.workload, a.cells, steps=a.steps, instances=a.instances)
-    topo = bench.make_topology(insts)
-    ensemble = a.workload in bench.ENSEMBLES
-
-    def make():
-        ens = Ensemble([p for p, _, _ in insts], topo, [cap for _, _, cap in insts])
-        for k, (p, st, cap) in enumerate(insts):
-            ens.load_state(k, st["X"], st["Y"], st["Z"], st.get("VX"), st.get("VY"), st.get("VZ"), n_cells=st["n"])
-        return ens
-
-    def total(ens):
-        return sum(ens.n_cells(k) for k in range(len(insts)))
-
-    skins = [float(x) for x in a.skins.split(",")]
-    if ensemble:
-        # one range; the same-trajectory check on the total cell count
-        res = tune(make, a.steps, skins=skins, bounds=(1,), chunk=a.chunk, population=total)
-    else:
-        res = tune(make, a.steps, skins=skins, chunk=a.chunk, population=total)
-    text = res.to_json()
-    if a.out:
-        with open(a.out, "w") as f:
-            f.write(text + "\n")
-    print(text)
-
-
-if __name__ == "__main__":
-    main()

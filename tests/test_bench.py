@@ -1,6 +1,7 @@
 """bench.py's accounting, on the CPU: node-steps and time per population
 decade of a colony run, from its division events; and the whole-job figures
 under several ranks (slowest rank's time, work summed), with two gloo ranks."""
+import json
 import os
 import sys
 
@@ -161,3 +162,44 @@ def test_skin_schedule_selection(tmp_path):
     assert mc and len(mc) == len(sk) and all(0.002 < s <= 1.0 for s in sk)
     info = bench.skin_info(ns(skin_schedule="auto", skin=None, workload="colony"))
     assert info["schedule"]["min_cells"] == mc and info["schedule"]["file"] == "cellsim3d_b200/schedules/colony.json"
+
+
+def test_autotune_mode_writes_a_schedule(monkeypatch, tmp_path):
+    """bench.py --autotune: one range for an ensemble, a schedule file in the
+    format of cellsim3d_b200/schedules/ (stand-in ensemble, no GPU)."""
+    import cellsim3d_b200 as cs
+    from cellsim3d_b200 import autotune
+
+    class FakeEns:
+        def __init__(self, params, topo, caps):
+            self.n, self.skin, self.last = [2] * len(params), None, 0.0
+
+        def load_state(self, *a, **k):
+            pass
+
+        def set_option(self, opt, v):
+            self.skin = v * 1e-6
+
+        def n_cells(self, k):
+            return self.n[k]
+
+        def step(self, m, raise_on_error=True):
+            self.last = m * (1.0 + abs(self.skin - 0.07))
+            return 0
+
+        def last_step_ms(self):
+            return self.last
+
+        def close(self):
+            pass
+
+    monkeypatch.setattr(cs, "Ensemble", FakeEns)
+    monkeypatch.setattr(bench, "make_topology", lambda insts: None)
+    st = {"X": None, "Y": None, "Z": None, "n": 2}
+    monkeypatch.setattr(bench, "build_workload", lambda *a, **k: [({}, st, 8), ({}, st, 8)])
+    out = str(tmp_path / "ens.json")
+    args = bench.argparse.Namespace(workload="ensemble256", cells=0, steps=100, instances=0, autotune=out,
+                                    tune_skins="0.05,0.07,0.1", tune_chunk=25)
+    text = bench.run_autotune(args)
+    assert autotune.load_schedule(out) == ([1], [0.07])
+    assert json.loads(text)["bounds"] == [1]
