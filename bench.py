@@ -418,6 +418,7 @@ def run_cs3d(args, world, rank, local):
             # every rank launches the same kernel sequence: the whole job's count
             "gpu_launches": int(stats["launches_per_step"]) * args.steps * world,
             "nl_rebuilds": stats["rebuilds"],
+            "nl_rebuilds_div_rule": stats["rebuilds_div_rule"],
             "max_entries": stats["max_entries"],
             "max_cand": stats["max_cand"],
             "list_skin": skin_info(args),

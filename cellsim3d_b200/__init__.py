@@ -384,7 +384,7 @@ class Ensemble:
         s = (C.c_longlong * 8)()
         _lib.check(_lib.lib().cs3d_get_stats(self.h, s, 8), "cs3d_get_stats")
         return {"steps": s[0], "rebuilds": s[1], "max_entries": s[2], "max_cand": s[3], "launches_per_step": s[4],
-                "max_halo": s[5], "lists_built": s[6]}
+                "max_halo": s[5], "lists_built": s[6], "rebuilds_div_rule": s[7]}
 
 
 class Simulation(Ensemble):

@@ -1185,6 +1185,7 @@ int cs3d_get_stats(cs3d_ctx *c, long long *stats, int n)
         v[2] = std::max<long long>(v[2], q.max_entries);
         v[3] = std::max<long long>(v[3], q.max_cand);
         v[6] += q.built;
+        v[7] += q.rebuilds_div;
     }
     for (int k = 0; k < n && k < 8; ++k) stats[k] = v[k];
     return CS3D_OK;

@@ -66,6 +66,7 @@ struct InstState {
     int hbits;             // log2 of the slice size (0: not rebuilding)
     int built;             // cells whose lists were built (cumulative)
     int rebuilds;
+    int rebuilds_div;      // of those, the ones only the rule for dividing instances called for
     float syscm[3];        // the reference's system centre of mass as of its last
                            // calc_sys_CM call, (1, 1, 1) before the first one
     // RANMAR, src/marsaglia.h:50-52

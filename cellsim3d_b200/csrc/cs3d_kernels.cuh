@@ -613,8 +613,10 @@ __global__ void __launch_bounds__(256) k_step_begin(Dev d, int par_next)
                 st->force_rebuild = 1;
             }
         }
-        const bool full = st->force_rebuild || !(2.0f * ds + 1e-3f < P.skin) ||
-                          (st->div_count > 0 && ds > 0.25f * P.skin);
+        const bool by_disp = st->force_rebuild || !(2.0f * ds + 1e-3f < P.skin);
+        const bool by_div = st->div_count > 0 && ds > 0.25f * P.skin;
+        const bool full = by_disp || by_div;
+        if (by_div && !by_disp) st->rebuilds_div += 1;
         const bool part = !full && st->div_count > 0;
         st->rebuild = full ? 2 : part ? 1 : 0;
         st->rcur = full ? P.rlist : P.rlist + 2.0f * ds + 1e-3f;

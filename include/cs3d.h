@@ -406,7 +406,10 @@ int cs3d_last_error(cs3d_ctx *ctx, int inst, uint32_t *bits);
  * seen, [3] max candidate cells per cell seen, [4] kernel launches per step,
  * [5] max distinct contact-candidate nodes (of other cells) per cell seen
  * (counted only with CS3D_OPT_HALO_STATS, else 0),
- * [6] cell neighbour lists built (cumulative). */
+ * [6] cell neighbour lists built (cumulative), [7] of the rebuilds [1], those
+ * that only the rule for dividing instances called for (a division in the
+ * step and a node more than a quarter of the skin from its anchor, with no
+ * node past half the skin). */
 int cs3d_get_stats(cs3d_ctx *ctx, long long *stats, int n);
 
 /* Profiling pass: n_steps steps launched kernel by kernel (not as a graph)
