@@ -4,9 +4,10 @@ real-time loop that must not call cudaMalloc/cudaFree, a plugin host that
 forbids allocation in callbacks).  It takes device pointers the caller owns
 and keeps its scratch in a static device array of the library.
 
-Checked through the C ABI against the existing entry point (cs3d_load_state
-followed by cs3d_get_forces) on the same inputs, on two calls in a row, with
-the tolerance of the parity tests.  This file is collected last on purpose.
+Checked through the C ABI against the FP64 oracle's initial forces and
+against the existing entry point (cs3d_load_state followed by
+cs3d_get_forces) on the same inputs, on two calls in a row, with the
+tolerance of the parity tests.  This file is collected last on purpose.
 """
 import ctypes as C
 
@@ -17,7 +18,8 @@ import cellsim3d_b200 as cs
 from cellsim3d_b200 import _lib
 from cellsim3d_b200 import workloads as W
 
-from parity import TOL, rel_err
+import oracle
+from parity import TOL, rel_err, topo_for
 
 pytestmark = pytest.mark.gpu
 
@@ -40,6 +42,22 @@ def _reference_forces(p, st, topo):
     return f
 
 
+def _oracle_forces(p, st, mesh):
+    """The oracle's initial forces (src/GPUbounce.cu:978-1004) on the same
+    state, with the oracle's own R0/theta0 tables (equal to the library's,
+    which topo_for asserts)."""
+    _, otopo = topo_for(st, mesh)
+    n = st["n"]
+    o = oracle.System(n, p, otopo)
+    o.load(st["X"], st["Y"], st["Z"], st.get("VX"), st.get("VY"), st.get("VZ"), n=n)
+    o.seed(p["rng_ij"], p["rng_kl"])
+    o.init()
+    f = {"FCX": o.FC[0].copy(), "FCY": o.FC[1].copy(), "FCZ": o.FC[2].copy(),
+         "FDX": o.FD[0].copy(), "FDY": o.FD[1].copy(), "FDZ": o.FD[2].copy()}
+    o.close()
+    return f
+
+
 def _static_forces(p, st, topo, torch):
     n = st["n"]
     dev = torch.device("cuda", 0)
@@ -59,19 +77,22 @@ def _static_forces(p, st, topo, torch):
 
 
 def test_static_forces_match_existing_entry_point(mesh):
-    """Two calls in a row per state, each against the existing entry point
-    (cs3d_load_state + cs3d_get_forces) within the parity tolerance."""
+    """Two calls in a row per state, each against the FP64 oracle and
+    against the existing entry point (cs3d_load_state + cs3d_get_forces)
+    within the parity tolerance."""
     import torch
     m = cs.mesh_from_arrays(mesh)
     for p, st in _states():
         topo = cs.build_topology(m, st["X"][:192], st["Y"][:192], st["Z"][:192])
         ref = _reference_forces(p, st, topo)
+        orc = _oracle_forces(p, st, mesh)
         n = st["n"]
         for call in range(2):
             got = _static_forces(p, st, topo, torch)
-            ec = rel_err([got["FCX"], got["FCY"], got["FCZ"]], [ref["FCX"], ref["FCY"], ref["FCZ"]], n)
-            ed = rel_err([got["FDX"], got["FDY"], got["FDZ"]], [ref["FDX"], ref["FDY"], ref["FDZ"]], n)
-            assert ec[0] < TOL and ed[0] < TOL, (n, call, p.get("correct_com"), ec, ed)
+            for tag, want in (("oracle", orc), ("entry point", ref)):
+                ec = rel_err([got["FCX"], got["FCY"], got["FCZ"]], [want["FCX"], want["FCY"], want["FCZ"]], n)
+                ed = rel_err([got["FDX"], got["FDY"], got["FDZ"]], [want["FDX"], want["FDY"], want["FDZ"]], n)
+                assert ec[0] < TOL and ed[0] < TOL, (tag, n, call, p.get("correct_com"), ec, ed)
             # padding slots 180..191 are zero in all six outputs
             for k in ("FCX", "FCY", "FCZ", "FDX", "FDY", "FDZ"):
                 assert np.all(got[k].reshape(n, 192)[:, 180:] == 0), (k, call)
